@@ -1,0 +1,116 @@
+"""ctypes binding of the bclx C ABI (include/bclx.h).
+
+The shared library is built in place by ``bcl_b200.build`` (nvcc, sm_100a).
+There is no fallback: if the library cannot be loaded, every entry point
+raises, so nothing silently runs on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbclx.so")
+
+# status codes (bclx_status_t)
+OK, ERR_INVALID, ERR_DTYPE, ERR_CUDA, ERR_NO_MEMORY, ERR_INDEX_OVERFLOW, ERR_DEVICE_TIMEOUT, ERR_NO_DEVICE = range(8)
+STATUS_NAMES = {
+    OK: "BCLX_OK", ERR_INVALID: "BCLX_ERR_INVALID", ERR_DTYPE: "BCLX_ERR_DTYPE", ERR_CUDA: "BCLX_ERR_CUDA",
+    ERR_NO_MEMORY: "BCLX_ERR_NO_MEMORY", ERR_INDEX_OVERFLOW: "BCLX_ERR_INDEX_OVERFLOW",
+    ERR_DEVICE_TIMEOUT: "BCLX_ERR_DEVICE_TIMEOUT", ERR_NO_DEVICE: "BCLX_ERR_NO_DEVICE",
+}
+
+# value types (bclx_dtype_t)
+F32, I32, BF16 = 0, 1, 2
+
+i64, i32, vp = ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p
+
+
+class CSRDesc(ctypes.Structure):
+    """bclx_csr_t"""
+    _fields_ = [("m", i64), ("n", i64), ("nnz", i64), ("row_ptr", vp), ("col_ind", vp), ("vals", vp),
+                ("dtype", i32), ("pad_", i32)]
+
+
+class SpGrid(ctypes.Structure):
+    """bclx_spgrid_t"""
+    _fields_ = [("m", i64), ("n", i64), ("tile_m", i64), ("tile_n", i64), ("grid_m", i64), ("grid_n", i64),
+                ("tiles", vp), ("dtype", i32), ("pad_", i32)]
+
+
+class SpGridOut(ctypes.Structure):
+    """bclx_spgrid_out_t"""
+    _fields_ = [("m", i64), ("n", i64), ("tile_m", i64), ("tile_n", i64), ("grid_m", i64), ("grid_n", i64),
+                ("tile_row_ptr", vp), ("tile_offset", vp), ("col_ind", vp), ("vals", vp), ("dtype", i32),
+                ("pad_", i32)]
+
+
+class DGrid(ctypes.Structure):
+    """bclx_dgrid_t"""
+    _fields_ = [("m", i64), ("n", i64), ("tile_m", i64), ("tile_n", i64), ("grid_m", i64), ("grid_n", i64),
+                ("tiles", vp), ("dtype", i32), ("pad_", i32)]
+
+
+assert ctypes.sizeof(CSRDesc) == 56
+
+# name -> (argtypes); every function returns int (status) unless listed in _RESTYPES
+SIGNATURES = {
+    "bclx_context_create": [ctypes.c_int, ctypes.POINTER(vp)],
+    "bclx_context_destroy": [vp],
+    "bclx_context_set_stream": [vp, vp],
+    "bclx_context_synchronize": [vp],
+    "bclx_last_error": [],
+    "bclx_version": [],
+    "bclx_spgemm_symbolic": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
+                             ctypes.POINTER(vp), ctypes.POINTER(i64)],
+    "bclx_spgemm_numeric": [vp, vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
+                            i32, i32],
+    "bclx_spgemm_plan_destroy": [vp],
+    "bclx_spgemm_plan_stats": [vp, ctypes.POINTER(i64)],
+    "bclx_tile_accumulate_symbolic": [vp, vp, i32, i64, i64, i32, vp, ctypes.POINTER(vp), ctypes.POINTER(i64)],
+    "bclx_tile_accumulate_numeric": [vp, vp, vp, i32, ctypes.POINTER(CSRDesc)],
+    "bclx_spmm_tile": [vp, i64, i64, i64, i64, vp, vp, vp, vp, vp, i64, i64, i32],
+    "bclx_spmm_grid": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid)],
+}
+_RESTYPES = {"bclx_last_error": ctypes.c_char_p}
+
+
+class BclxError(RuntimeError):
+    def __init__(self, fn: str, status: int, detail: str):
+        super().__init__(f"{fn} failed: {STATUS_NAMES.get(status, status)}" + (f" ({detail})" if detail else ""))
+        self.status = status
+
+
+_lib = None
+
+
+def load(build_if_missing: bool = True):
+    """Load libbclx.so (building it with nvcc first if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH) and build_if_missing:
+        from . import build as _build
+        _build.build()
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"bclx CUDA library not found at {LIB_PATH}; run `python -m bcl_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = _RESTYPES.get(name, ctypes.c_int)
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args) -> None:
+    """Call an entry point and raise BclxError on a non-zero status."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != OK:
+        detail = lib.bclx_last_error()
+        raise BclxError(name, rc, detail.decode() if detail else "")
+
+
+def exported_symbols():
+    return list(SIGNATURES)

@@ -1,0 +1,608 @@
+"""Device-resident tile containers and the gemm calls of BCL's matrix path,
+over the bclx C ABI.
+
+Python mirror of the reference's interface for this path
+(bcl/containers/SPMatrix.hpp, DMatrix.hpp, algorithms/spgemm.hpp): the same
+names and argument meaning — ``SPMatrix`` / ``DMatrix`` with a tile grid
+chosen by a ``BlockCustom`` policy, ``grid_shape`` / ``tile_shape`` /
+``tile_nnz`` / ``tile_rank`` / ``get_tile`` / ``assign_tile`` / ``get`` /
+``dot``, and ``gemm(a, b, c)`` for sparse x sparse and sparse x dense.  Every
+tile lives on one GPU (rank 0); torch supplies device memory and the current
+stream, and all arithmetic runs in the CUDA kernels behind the C ABI.
+
+Storage.  An SPMatrix keeps its CSR tiles packed in four device arrays, tile
+t = i*grid_n + j owning ``col_ind/vals[tile_offset[t]:tile_offset[t+1]]`` and
+``tile_row_ptr[t]`` (tile_m+1 local offsets), plus a device array of
+``bclx_csr_t`` descriptors, one per tile, that the kernels read.  This is the
+format the sparse product writes, so a product is again an SPMatrix without a
+copy.  A DMatrix keeps ``grid_m*grid_n`` padded row-major tiles of
+tile_m x tile_n in one allocation, as DMatrix does (DMatrix.hpp:55-95).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import CSRDesc, DGrid, SpGrid, SpGridOut, call
+from .gen import CSR
+
+_NP_TO_DT = {np.dtype(np.float32): _lib.F32, np.dtype(np.int32): _lib.I32}
+_TORCH_OF = {_lib.F32: torch.float32, _lib.I32: torch.int32, _lib.BF16: torch.bfloat16}
+
+
+def _ceil_div(a: int, b: int) -> int:
+    return (a + b - 1) // b
+
+
+# ---- context ------------------------------------------------------------------
+
+
+class Context:
+    """A bclx context on one device; every call runs on torch's current stream."""
+
+    def __init__(self, device: int = 0):
+        if not torch.cuda.is_available():
+            raise RuntimeError("bcl_b200 needs a CUDA device (B200, sm_100a); none is visible")
+        self.device = device
+        h = ctypes.c_void_p()
+        call("bclx_context_create", device, ctypes.byref(h))
+        self.h = h
+
+    def use_current_stream(self):
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        call("bclx_context_set_stream", self.h, ctypes.c_void_p(s))
+        return self.h
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                _lib.load().bclx_context_destroy(self.h)
+        except Exception:
+            pass
+
+
+_contexts = {}
+
+
+def context(device: Optional[int] = None) -> Context:
+    d = torch.cuda.current_device() if device is None else int(device)
+    if d not in _contexts:
+        _contexts[d] = Context(d)
+    return _contexts[d]
+
+
+# ---- blocking ------------------------------------------------------------------
+
+
+@dataclasses.dataclass
+class BlockCustom:
+    """Tile-grid policy (bcl/containers/detail/Blocking.hpp:215-245): a tile
+    shape and a processor grid.  On one GPU the processor grid is {1, 1}, so
+    every tile is owned by rank 0.  A tile dimension of 0 (``Tile::div``)
+    divides that dimension evenly over the processor grid."""
+
+    tile_shape: Tuple[int, int]
+    grid_shape: Tuple[int, int] = (1, 1)
+
+    def seed(self, m: int, n: int) -> Tuple[int, int]:
+        tm, tn = self.tile_shape
+        if tm == 0:
+            tm = _ceil_div(m, self.grid_shape[0])
+        if tn == 0:
+            tn = _ceil_div(n, self.grid_shape[1])
+        if tm <= 0 or tn <= 0:
+            raise ValueError("tile shape must be positive")
+        return int(tm), int(tn)
+
+
+# ---- host-side tiling ------------------------------------------------------------
+
+
+def split_tiles(a: CSR, tm: int, tn: int):
+    """Cut a host CSR into a tm x tn tile grid, packed (the result of
+    SPMatrix::init_ / get_slice_impl_, SPMatrix.hpp:211-271, CSRMatrix.hpp:238-276):
+    returns (tile_row_ptr [ntiles, tm+1] int32 local offsets, tile_offset
+    [ntiles+1] int64, col_ind int32 tile-local, vals)."""
+    gm, gn = _ceil_div(a.m, tm), _ceil_div(a.n, tn)
+    ntiles = gm * gn
+    rp = a.row_ptr.astype(np.int64)
+    rows = np.repeat(np.arange(a.m, dtype=np.int64), np.diff(rp))
+    cols = a.col_ind.astype(np.int64)
+    ti, tj = rows // tm, cols // tn
+    t = ti * gn + tj
+    order = np.argsort(t, kind="stable")  # keeps (row, col) order inside every tile
+    t_sorted = t[order]
+    lrow = rows[order] - ti[order] * tm
+    counts = np.bincount(t, minlength=ntiles)
+    tile_offset = np.zeros(ntiles + 1, dtype=np.int64)
+    np.cumsum(counts, out=tile_offset[1:])
+    per_row = np.bincount(t_sorted * tm + lrow, minlength=ntiles * tm).reshape(ntiles, tm)
+    tile_rp = np.zeros((ntiles, tm + 1), dtype=np.int64)
+    np.cumsum(per_row, axis=1, out=tile_rp[:, 1:])
+    if counts.size and counts.max(initial=0) >= 2**31:
+        raise OverflowError("a tile has more than 2**31-1 nonzeros")
+    col_local = (cols[order] - tj[order] * tn).astype(np.int32)
+    return tile_rp.astype(np.int32), tile_offset, col_local, a.vals[order]
+
+
+def _nonempty(t: torch.Tensor) -> torch.Tensor:
+    return t if t.numel() > 0 else torch.zeros(1, dtype=t.dtype, device=t.device)
+
+
+# ---- SPMatrix ----------------------------------------------------------------------
+
+
+class SPMatrix:
+    """Distributed sparse matrix with every tile on this GPU
+    (BCL::SPMatrix<T, int>, bcl/containers/SPMatrix.hpp:69-659)."""
+
+    def __init__(self, m: int, n: int, tile_m: int, tile_n: int, dtype, device: int,
+                 tile_row_ptr: torch.Tensor, tile_offset: torch.Tensor, col_ind: torch.Tensor,
+                 vals: torch.Tensor):
+        self.m, self.n = int(m), int(n)
+        self.tm, self.tn = int(tile_m), int(tile_n)
+        self.gm, self.gn = _ceil_div(self.m, self.tm), _ceil_div(self.n, self.tn)
+        self.dtype = np.dtype(dtype)
+        self.device = device
+        self.tile_row_ptr = tile_row_ptr
+        self.tile_offset = tile_offset
+        self.col_ind = _nonempty(col_ind)
+        self.vals = _nonempty(vals)
+        self._offsets_host = None
+        self._build_desc()
+
+    # -- construction
+    @classmethod
+    def from_csr(cls, a: CSR, blocking: BlockCustom, device: Optional[int] = None) -> "SPMatrix":
+        """Tile a host matrix and upload it (the SPMatrix(fname, blocking)
+        constructor's slicing, SPMatrix.hpp:211-271, from an in-memory CSR)."""
+        dev = torch.cuda.current_device() if device is None else device
+        tm, tn = blocking.seed(a.m, a.n)
+        trp, toff, ci, v = split_tiles(a, tm, tn)
+        td = torch.device("cuda", dev)
+        return cls(a.m, a.n, tm, tn, a.vals.dtype, dev,
+                   torch.from_numpy(trp).to(td), torch.from_numpy(toff).to(td),
+                   torch.from_numpy(ci).to(td), torch.from_numpy(np.ascontiguousarray(v)).to(td))
+
+    @classmethod
+    def zeros(cls, shape: Tuple[int, int], blocking: BlockCustom, dtype=np.float32,
+              device: Optional[int] = None) -> "SPMatrix":
+        """An all-zero matrix (SPMatrix(dim, blocking), init_with_zero)."""
+        dev = torch.cuda.current_device() if device is None else device
+        m, n = shape
+        tm, tn = blocking.seed(m, n)
+        ntiles = _ceil_div(m, tm) * _ceil_div(n, tn)
+        td = torch.device("cuda", dev)
+        return cls(m, n, tm, tn, dtype, dev, torch.zeros((ntiles, tm + 1), dtype=torch.int32, device=td),
+                   torch.zeros(ntiles + 1, dtype=torch.int64, device=td),
+                   torch.zeros(0, dtype=torch.int32, device=td),
+                   torch.zeros(0, dtype=_TORCH_OF[_NP_TO_DT[np.dtype(dtype)]], device=td))
+
+    def _build_desc(self):
+        """Device array of bclx_csr_t, one per tile, computed on the device."""
+        ntiles = self.gm * self.gn
+        td = self.tile_row_ptr.device
+        ti = torch.arange(self.gm, device=td).repeat_interleave(self.gn)
+        tj = torch.arange(self.gn, device=td).repeat(self.gm)
+        d = torch.empty((ntiles, 6), dtype=torch.int64, device=td)
+        d[:, 0] = torch.clamp(self.m - ti * self.tm, max=self.tm)
+        d[:, 1] = torch.clamp(self.n - tj * self.tn, max=self.tn)
+        d[:, 2] = self.tile_offset[1:] - self.tile_offset[:-1]
+        d[:, 3] = self.tile_row_ptr.data_ptr() + torch.arange(ntiles, device=td) * (self.tm + 1) * 4
+        d[:, 4] = self.col_ind.data_ptr() + self.tile_offset[:-1] * 4
+        d[:, 5] = self.vals.data_ptr() + self.tile_offset[:-1] * self.vals.element_size()
+        self.desc = torch.empty((ntiles, 7), dtype=torch.int64, device=td)
+        self.desc[:, :6] = d
+        self.desc[:, 6] = _NP_TO_DT[self.dtype]  # dtype (low 32 bits) and pad
+        self.desc = self.desc.contiguous()
+        self._offsets_host = None
+
+    # -- the reference's accessors
+    def shape(self):
+        return (self.m, self.n)
+
+    def grid_shape(self):
+        return (self.gm, self.gn)
+
+    def tile_shape(self, index=None):
+        if index is None:
+            return (self.tm, self.tn)
+        i, j = index
+        return (min(self.tm, self.m - i * self.tm), min(self.tn, self.n - j * self.tn))
+
+    def tile_rank(self, index) -> int:
+        return 0
+
+    def _offsets(self) -> np.ndarray:
+        if self._offsets_host is None:
+            self._offsets_host = self.tile_offset.cpu().numpy()
+        return self._offsets_host
+
+    def tile_nnz(self, index) -> int:
+        t = index[0] * self.gn + index[1]
+        o = self._offsets()
+        return int(o[t + 1] - o[t])
+
+    def nnz(self) -> int:
+        return int(self._offsets()[-1])
+
+    def spgrid(self) -> SpGrid:
+        return SpGrid(self.m, self.n, self.tm, self.tn, self.gm, self.gn, self.desc.data_ptr(),
+                      _NP_TO_DT[self.dtype], 0)
+
+    def tile_desc_ptr(self, index) -> int:
+        """Device address of one tile's bclx_csr_t (a 1x1 grid view of it)."""
+        return self.desc.data_ptr() + (index[0] * self.gn + index[1]) * 56
+
+    def get_tile(self, index) -> CSR:
+        """Copy one tile to the host (SPMatrix::get_tile, SPMatrix.hpp:476-494)."""
+        t = index[0] * self.gn + index[1]
+        o = self._offsets()
+        m, n = self.tile_shape(index)
+        rp = self.tile_row_ptr[t, : m + 1].cpu().numpy()
+        ci = self.col_ind[o[t]:o[t + 1]].cpu().numpy() if o[t + 1] > o[t] else np.zeros(0, np.int32)
+        v = self.vals[o[t]:o[t + 1]].cpu().numpy() if o[t + 1] > o[t] else np.zeros(0, self.dtype)
+        return CSR(m, n, rp, ci, v)
+
+    def get(self) -> CSR:
+        """Gather the whole matrix to the host in global coordinates
+        (SPMatrix::get, SPMatrix.hpp:516-546)."""
+        o = self._offsets()
+        nnz = int(o[-1])
+        trp = self.tile_row_ptr.cpu().numpy().astype(np.int64)
+        ci = self.col_ind.cpu().numpy()[:nnz].astype(np.int64)
+        v = self.vals.cpu().numpy()[:nnz]
+        t_of = np.repeat(np.arange(self.gm * self.gn), np.diff(o))
+        ti, tj = t_of // self.gn, t_of % self.gn
+        # local row of each entry
+        lrow = np.empty(nnz, dtype=np.int64)
+        for t in range(self.gm * self.gn):
+            if o[t + 1] > o[t]:
+                cnt = np.diff(trp[t])
+                lrow[o[t]:o[t + 1]] = np.repeat(np.arange(self.tm), cnt)
+        grow = ti * self.tm + lrow
+        gcol = tj * self.tn + ci
+        key = grow * self.n + gcol
+        order = np.argsort(key, kind="stable")
+        counts = np.bincount(grow, minlength=self.m)
+        rp = np.zeros(self.m + 1, dtype=np.int64)
+        np.cumsum(counts, out=rp[1:])
+        return CSR(self.m, self.n, rp.astype(np.int32), gcol[order].astype(np.int32), v[order])
+
+    def assign_tile(self, index, tile: CSR) -> None:
+        """Replace one tile (SPMatrix::assign_tile, SPMatrix.hpp:277-308)."""
+        if tile.m != self.tile_shape(index)[0] or tile.n != self.tile_shape(index)[1]:
+            raise RuntimeError("BCL::SpMatrix::assign_tile: tile shape mismatch")
+        t = index[0] * self.gn + index[1]
+        o = self._offsets()
+        td = self.tile_row_ptr.device
+        nnz = int(o[-1])
+        old_n = int(o[t + 1] - o[t])
+        new_n = tile.nnz
+        ci = torch.cat([self.col_ind[: o[t]], torch.from_numpy(tile.col_ind.astype(np.int32)).to(td),
+                        self.col_ind[o[t + 1]:nnz]])
+        v = torch.cat([self.vals[: o[t]], torch.from_numpy(np.ascontiguousarray(tile.vals, self.dtype)).to(td),
+                       self.vals[o[t + 1]:nnz]])
+        rp = self.tile_row_ptr.clone()
+        rp[t].zero_()
+        rp[t, : tile.m + 1] = torch.from_numpy(tile.row_ptr.astype(np.int32)).to(td)
+        rp[t, tile.m + 1:] = new_n
+        toff = self.tile_offset.clone()
+        toff[t + 1:] += new_n - old_n
+        self.tile_row_ptr, self.tile_offset = rp, toff
+        self.col_ind, self.vals = _nonempty(ci), _nonempty(v)
+        self._build_desc()
+
+    def dot(self, other):
+        """C = self * other (SPMatrix::dot -> gemm)."""
+        if isinstance(other, SPMatrix):
+            return spgemm(self, other)
+        if isinstance(other, DMatrix):
+            c = DMatrix.zeros((self.m, other.n), BlockCustom((self.tm, other.tn)), dtype=other.torch_dtype,
+                              device=self.device)
+            gemm(self, other, c)
+            return c
+        raise TypeError("dot: unsupported operand")
+
+
+# ---- DMatrix -------------------------------------------------------------------------
+
+
+class DMatrix:
+    """Distributed dense matrix with every tile on this GPU (BCL::DMatrix<T>,
+    bcl/containers/DMatrix.hpp:27-587): grid_m*grid_n tiles of tile_m x tile_n,
+    row-major, padded to full size at the edges.  FP32, or bfloat16 storage."""
+
+    def __init__(self, m: int, n: int, tile_m: int, tile_n: int, tiles: torch.Tensor):
+        self.m, self.n, self.tm, self.tn = int(m), int(n), int(tile_m), int(tile_n)
+        self.gm, self.gn = _ceil_div(self.m, self.tm), _ceil_div(self.n, self.tn)
+        assert tiles.shape == (self.gm * self.gn, self.tm, self.tn) and tiles.is_contiguous()
+        self.tiles = tiles
+        self.torch_dtype = tiles.dtype
+        self.device = tiles.device.index
+        nt = self.gm * self.gn
+        self.ptrs = (tiles.data_ptr() + torch.arange(nt, dtype=torch.int64, device=tiles.device)
+                     * (self.tm * self.tn * tiles.element_size())).contiguous()
+
+    @classmethod
+    def zeros(cls, shape, blocking: BlockCustom, dtype=torch.float32, device=None) -> "DMatrix":
+        dev = torch.cuda.current_device() if device is None else device
+        m, n = shape
+        tm, tn = blocking.seed(m, n)
+        nt = _ceil_div(m, tm) * _ceil_div(n, tn)
+        return cls(m, n, tm, tn, torch.zeros((nt, tm, tn), dtype=dtype, device=torch.device("cuda", dev)))
+
+    @classmethod
+    def from_array(cls, arr, blocking: BlockCustom, dtype=torch.float32, device=None) -> "DMatrix":
+        """Tile a full row-major array (host numpy or torch)."""
+        dev = torch.cuda.current_device() if device is None else device
+        full = torch.as_tensor(arr)
+        m, n = full.shape
+        d = cls.zeros((m, n), blocking, dtype=dtype, device=dev)
+        d.set_matrix(full)
+        return d
+
+    def set_matrix(self, full: torch.Tensor) -> None:
+        src = full.to(device=self.tiles.device, dtype=self.torch_dtype)
+        mp, np_ = self.gm * self.tm, self.gn * self.tn
+        pad = torch.zeros((mp, np_), dtype=self.torch_dtype, device=self.tiles.device)
+        pad[: self.m, : self.n] = src
+        self.tiles.copy_(pad.view(self.gm, self.tm, self.gn, self.tn).permute(0, 2, 1, 3)
+                         .reshape(self.gm * self.gn, self.tm, self.tn))
+
+    def get_matrix(self) -> torch.Tensor:
+        """The whole matrix as one row-major tensor (DMatrix::get_matrix)."""
+        full = (self.tiles.view(self.gm, self.gn, self.tm, self.tn).permute(0, 2, 1, 3)
+                .reshape(self.gm * self.tm, self.gn * self.tn))
+        return full[: self.m, : self.n]
+
+    def fill_(self, value) -> "DMatrix":
+        """DMatrix::operator=(value) (DMatrix.hpp:226-242)."""
+        self.tiles.fill_(value)
+        return self
+
+    def shape(self):
+        return (self.m, self.n)
+
+    def grid_shape(self):
+        return (self.gm, self.gn)
+
+    def tile_shape(self, index=None):
+        if index is None:
+            return (self.tm, self.tn)
+        i, j = index
+        return (min(self.tm, self.m - i * self.tm), min(self.tn, self.n - j * self.tn))
+
+    def tile_rank(self, index) -> int:
+        return 0
+
+    def tile_ptr(self, index) -> int:
+        return int(self.tiles[index[0] * self.gn + index[1]].data_ptr())
+
+    @property
+    def bclx_dtype(self) -> int:
+        if self.torch_dtype == torch.float32:
+            return _lib.F32
+        if self.torch_dtype == torch.bfloat16:
+            return _lib.BF16
+        raise TypeError("DMatrix tiles must be float32 or bfloat16")
+
+    def dgrid(self) -> DGrid:
+        return DGrid(self.m, self.n, self.tm, self.tn, self.gm, self.gn, self.ptrs.data_ptr(), self.bclx_dtype, 0)
+
+
+# ---- products -----------------------------------------------------------------------
+
+
+def _out_grid(a: SPMatrix, b: SPMatrix):
+    td = a.tile_row_ptr.device
+    gm, gn = a.gm, b.gn
+    trp = torch.empty((gm * gn, a.tm + 1), dtype=torch.int32, device=td)
+    toff = torch.empty(gm * gn + 1, dtype=torch.int64, device=td)
+    out = SpGridOut(a.m, b.n, a.tm, b.tn, gm, gn, trp.data_ptr(), toff.data_ptr(), None, None,
+                    _NP_TO_DT[a.dtype], 0)
+    return out, trp, toff
+
+
+class SpgemmPlan:
+    """Holds a symbolic-phase plan (work decomposition and row offsets)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def stats(self) -> dict:
+        arr = (ctypes.c_int64 * 6)()
+        call("bclx_spgemm_plan_stats", self.h, arr)
+        keys = ["products", "row_items", "work_items", "big_items", "stages", "nnz"]
+        return dict(zip(keys, [int(x) for x in arr]))
+
+    def close(self):
+        if self.h:
+            _lib.load().bclx_spgemm_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def _check_grids(a: SPMatrix, b: SPMatrix):
+    if a.n != b.m:
+        raise RuntimeError("BCL::gemm: inner dimensions differ")
+    if a.tn != b.tm:
+        raise RuntimeError("BCL::gemm: A's tile width must equal B's tile height")
+    if a.dtype != b.dtype:
+        raise TypeError("BCL::gemm: A and B value types differ")
+
+
+def spgemm_symbolic(a: SPMatrix, b: SPMatrix):
+    """Symbolic phase: returns (plan, out descriptor, tile_row_ptr, tile_offset, nnz)."""
+    _check_grids(a, b)
+    ctx = context(a.device)
+    h = ctx.use_current_stream()
+    out, trp, toff = _out_grid(a, b)
+    plan = ctypes.c_void_p()
+    nnz = ctypes.c_int64()
+    ag, bg = a.spgrid(), b.spgrid()
+    call("bclx_spgemm_symbolic", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), ctypes.byref(plan),
+         ctypes.byref(nnz))
+    return SpgemmPlan(plan), out, trp, toff, int(nnz.value)
+
+
+def spgemm(a: SPMatrix, b: SPMatrix, stages: str = "fused", keep_plan: bool = False):
+    """C = A * B over the tile grids (BCL::gemm(SPMatrix, SPMatrix, SPMatrix&),
+    spgemm.hpp:182-242).  ``stages="fused"`` runs every SUMMA stage in one
+    numeric launch; ``"per_stage"`` runs one launch per stage (all G*G tile
+    products of that stage), adding into C between them; the results are
+    bit-identical."""
+    plan, out, trp, toff, nnz = spgemm_symbolic(a, b)
+    td = a.tile_row_ptr.device
+    ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=td)
+    v = torch.empty(max(nnz, 1), dtype=_TORCH_OF[_NP_TO_DT[a.dtype]], device=td)
+    out.col_ind, out.vals = ci.data_ptr(), v.data_ptr()
+    spgemm_numeric(plan, a, b, out, stages)
+    c = SPMatrix(a.m, b.n, a.tm, b.tn, a.dtype, a.device, trp, toff, ci, v)
+    if keep_plan:
+        return c, plan
+    plan.close()
+    return c
+
+
+def spgemm_numeric(plan: SpgemmPlan, a: SPMatrix, b: SPMatrix, out: SpGridOut, stages: str = "fused"):
+    h = context(a.device).use_current_stream()
+    ag, bg = a.spgrid(), b.spgrid()
+    if stages == "fused":
+        call("bclx_spgemm_numeric", h, plan.h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), 0, 0)
+    elif stages == "per_stage":
+        for s in range(a.gn):
+            call("bclx_spgemm_numeric", h, plan.h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), s, s + 1)
+    else:
+        raise ValueError(stages)
+
+
+def tile_accumulate(parts: Sequence[SPMatrix]) -> SPMatrix:
+    """Sum 1x1-grid partial tiles in list order (SparseHashAccumulator::
+    accumulate + get_matrix, SparseHashAccumulator.hpp:86-183)."""
+    p0 = parts[0]
+    m, n = p0.m, p0.n
+    td = p0.tile_row_ptr.device
+    descs = torch.cat([p.desc[0:1] for p in parts]).contiguous()
+    h = context(p0.device).use_current_stream()
+    rp = torch.empty((1, m + 1), dtype=torch.int32, device=td)
+    plan = ctypes.c_void_p()
+    nnz = ctypes.c_int64()
+    dt = _NP_TO_DT[p0.dtype]
+    call("bclx_tile_accumulate_symbolic", h, ctypes.c_void_p(descs.data_ptr()), len(parts), m, n, dt,
+         ctypes.c_void_p(rp.data_ptr()), ctypes.byref(plan), ctypes.byref(nnz))
+    pl = SpgemmPlan(plan)
+    k = int(nnz.value)
+    ci = torch.empty(max(k, 1), dtype=torch.int32, device=td)
+    v = torch.empty(max(k, 1), dtype=_TORCH_OF[dt], device=td)
+    out = CSRDesc(m, n, k, rp.data_ptr(), ci.data_ptr(), v.data_ptr(), dt, 0)
+    call("bclx_tile_accumulate_numeric", h, pl.h, ctypes.c_void_p(descs.data_ptr()), len(parts), ctypes.byref(out))
+    pl.close()
+    toff = torch.tensor([0, k], dtype=torch.int64, device=td)
+    return SPMatrix(m, n, m, n, p0.dtype, p0.device, rp, toff, ci, v)
+
+
+def _tile_view(a: SPMatrix, index) -> SPMatrix:
+    """A 1x1-grid SPMatrix sharing one tile's storage (no copy)."""
+    t = index[0] * a.gn + index[1]
+    o = a._offsets()
+    m, n = a.tile_shape(index)
+    lo, hi = int(o[t]), int(o[t + 1])
+    td = a.tile_row_ptr.device
+    rp = a.tile_row_ptr[t:t + 1, : m + 1].contiguous() if m + 1 != a.tm + 1 else a.tile_row_ptr[t:t + 1]
+    toff = torch.tensor([0, hi - lo], dtype=torch.int64, device=td)
+    return SPMatrix(m, n, m, n, a.dtype, a.device, rp, toff, a.col_ind[lo:hi] if hi > lo else a.col_ind[:0],
+                    a.vals[lo:hi] if hi > lo else a.vals[:0])
+
+
+def spgemm_plain(a: SPMatrix, b: SPMatrix) -> SPMatrix:
+    """The reference's loop structure, one call per tile product: for every C
+    tile (i, j), the partials A_ik * B_kj for k = (k_ + i + j) mod G each by a
+    two-phase product, then their tile accumulation (spgemm.hpp:200-235)."""
+    _check_grids(a, b)
+    G = a.gn
+    td = a.tile_row_ptr.device
+    tiles = []
+    for i in range(a.gm):
+        for j in range(b.gn):
+            parts = []
+            for k_ in range(G):
+                k = (k_ + i + j) % G
+                parts.append(spgemm(_tile_view(a, (i, k)), _tile_view(b, (k, j))))
+            tiles.append(tile_accumulate(parts))
+    # pack the per-tile results into one SPMatrix
+    tm, tn = a.tm, b.tn
+    counts = [t.nnz() for t in tiles]
+    toff = np.zeros(len(tiles) + 1, dtype=np.int64)
+    np.cumsum(counts, out=toff[1:])
+    trp = torch.empty((len(tiles), tm + 1), dtype=torch.int32, device=td)
+    for t, tile in enumerate(tiles):
+        mt = tile.m
+        trp[t, : mt + 1] = tile.tile_row_ptr[0, : mt + 1]
+        trp[t, mt + 1:] = counts[t]
+    ci = torch.cat([t.col_ind[: c] for t, c in zip(tiles, counts)])
+    v = torch.cat([t.vals[: c] for t, c in zip(tiles, counts)])
+    return SPMatrix(a.m, b.n, tm, tn, a.dtype, a.device, trp, torch.from_numpy(toff).to(td), ci, v)
+
+
+def spmm(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:
+    """C += A * B over tile grids in one launch (BCL::gemm(SPMatrix, DMatrix,
+    DMatrix&), spgemm.hpp:153-179)."""
+    if a.n != b.m or a.m != c.m or b.n != c.n:
+        raise RuntimeError("BCL::gemm: shape mismatch")
+    if a.dtype != np.float32:
+        raise TypeError("SpMM needs FP32 sparse values")
+    h = context(a.device).use_current_stream()
+    ag, bg, cg = a.spgrid(), b.dgrid(), c.dgrid()
+    call("bclx_spmm_grid", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(cg))
+
+
+def spmm_plain(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:
+    """The reference's loop, one spmm_wrapper call per tile product
+    (spgemm.hpp:153-179)."""
+    if a.n != b.m or a.m != c.m or b.n != c.n:
+        raise RuntimeError("BCL::gemm: shape mismatch")
+    h = context(a.device).use_current_stream()
+    o = a._offsets()
+    G = a.gn
+    es = b.tiles.element_size()
+    for i in range(c.gm):
+        for j in range(c.gn):
+            for k_ in range(G):
+                k = (k_ + i + j) % G
+                t = i * a.gn + k
+                m, n = c.tile_shape((i, j))
+                call("bclx_spmm_tile", h, m, n, a.tile_shape((i, k))[1], int(o[t + 1] - o[t]),
+                     ctypes.c_void_p(c.tile_ptr((i, j))), ctypes.c_void_p(b.tile_ptr((k, j))),
+                     ctypes.c_void_p(a.vals.data_ptr() + int(o[t]) * 4),
+                     ctypes.c_void_p(a.tile_row_ptr[t].data_ptr()),
+                     ctypes.c_void_p(a.col_ind.data_ptr() + int(o[t]) * 4), b.tn, c.tn, c.bclx_dtype)
+    del es
+
+
+def gemm(a, b, c=None):
+    """BCL::gemm(a, b, c): sparse x sparse returns the product SPMatrix (c, if
+    given, is replaced tile by tile, as assign_tile does); sparse x dense
+    accumulates into the DMatrix c in place."""
+    if isinstance(a, SPMatrix) and isinstance(b, SPMatrix):
+        res = spgemm(a, b)
+        if c is not None:
+            if (c.m, c.n, c.tm, c.tn) != (res.m, res.n, res.tm, res.tn):
+                raise RuntimeError("BCL::gemm: C has a different tile grid")
+            c.tile_row_ptr, c.tile_offset, c.col_ind, c.vals = res.tile_row_ptr, res.tile_offset, res.col_ind, res.vals
+            c._build_desc()
+            return c
+        return res
+    if isinstance(a, SPMatrix) and isinstance(b, DMatrix):
+        if c is None:
+            raise TypeError("sparse x dense gemm needs the output DMatrix")
+        spmm(a, b, c)
+        return c
+    raise TypeError("BCL::gemm: unsupported operand types")

@@ -1,0 +1,155 @@
+// Shared pieces of the bclx CUDA library: status handling, the context
+// (device, stream, stream-ordered scratch pool, pinned readback slot), tile
+// grid views read by the kernels, and warp/block primitives.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/bclx.h"
+
+namespace bclx {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarp = 32;
+
+// ---- status ---------------------------------------------------------------
+
+void set_last_error(const std::string& msg);
+
+#define BCLX_CK(call)                                                              \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      ::bclx::set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+      return e_ == cudaErrorMemoryAllocation ? BCLX_ERR_NO_MEMORY : BCLX_ERR_CUDA; \
+    }                                                                             \
+  } while (0)
+
+#define BCLX_CK_LAUNCH() BCLX_CK(cudaGetLastError())
+
+#define BCLX_TRY(expr)            \
+  do {                            \
+    int s_ = (expr);              \
+    if (s_ != BCLX_OK) return s_; \
+  } while (0)
+
+// ---- context ----------------------------------------------------------------
+
+struct Context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  int64_t* pinned = nullptr;  // host readback slots
+};
+
+// Stream-ordered scratch from the device's default memory pool (kept cached:
+// the release threshold is raised at context creation).
+int scratch_alloc(Context* ctx, void** p, size_t bytes);
+void scratch_free(Context* ctx, void* p);
+
+template <typename T>
+int scratch_alloc_n(Context* ctx, T** p, size_t count) {
+  return scratch_alloc(ctx, reinterpret_cast<void**>(p), sizeof(T) * (count > 0 ? count : 1));
+}
+
+// Exclusive prefix sum of `in` (int32 or int64 values) into int64 `out`
+// [count+1]; out[count] is the total.
+int exclusive_scan_i32(Context* ctx, const int32_t* in, int64_t* out, int64_t count);
+int exclusive_scan_i64(Context* ctx, const int64_t* in, int64_t* out, int64_t count);
+
+// ---- grid views (kernel parameters) -------------------------------------------
+
+struct SpGridView {
+  const bclx_csr_t* tiles;  // device array, or null: use `single`
+  bclx_csr_t single;
+  int64_t m, n, tm, tn, gm, gn;
+
+  __device__ __forceinline__ bclx_csr_t tile(int64_t i, int64_t j) const {
+    return tiles ? tiles[i * gn + j] : single;
+  }
+  __host__ __device__ __forceinline__ int64_t rows_of(int64_t i) const {
+    int64_t r = m - i * tm;
+    return r < tm ? r : tm;
+  }
+  __host__ __device__ __forceinline__ int64_t cols_of(int64_t j) const {
+    int64_t c = n - j * tn;
+    return c < tn ? c : tn;
+  }
+};
+
+inline SpGridView make_view(const bclx_spgrid_t& g) {
+  SpGridView v{};
+  v.tiles = g.tiles;
+  v.m = g.m; v.n = g.n; v.tm = g.tile_m; v.tn = g.tile_n; v.gm = g.grid_m; v.gn = g.grid_n;
+  return v;
+}
+
+struct DGridView {
+  void* const* tiles;  // device array, or null: use `single`
+  void* single;
+  int64_t m, n, tm, tn, gm, gn;
+  int64_t ld;  // leading dimension in elements
+
+  __device__ __forceinline__ void* tile(int64_t i, int64_t j) const {
+    return tiles ? tiles[i * gn + j] : single;
+  }
+  __host__ __device__ __forceinline__ int64_t rows_of(int64_t i) const {
+    int64_t r = m - i * tm;
+    return r < tm ? r : tm;
+  }
+  __host__ __device__ __forceinline__ int64_t cols_of(int64_t j) const {
+    int64_t c = n - j * tn;
+    return c < tn ? c : tn;
+  }
+};
+
+// ---- device helpers -----------------------------------------------------------
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    T t = __shfl_up_sync(kFull, v, d);
+    if (lane >= d) v += t;
+  }
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kFull, v, d);
+  return v;
+}
+
+// Multiply-add in the value type: one fused multiply-add for float (what the
+// reference's `c += a*b` compiles to), wrapping arithmetic for int32.
+__device__ __forceinline__ float madd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ int32_t madd(int32_t a, int32_t b, int32_t c) {
+  return (int32_t)((uint32_t)a * (uint32_t)b + (uint32_t)c);
+}
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ int32_t vadd(int32_t a, int32_t b) {
+  return (int32_t)((uint32_t)a + (uint32_t)b);
+}
+
+// First position in sorted col[lo, hi) whose value is >= key.
+__device__ __forceinline__ int32_t lower_bound_i32(const int32_t* __restrict__ col, int32_t lo, int32_t hi,
+                                                   int32_t key) {
+  while (lo < hi) {
+    int32_t mid = lo + ((hi - lo) >> 1);
+    if (__ldg(col + mid) < key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace bclx

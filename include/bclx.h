@@ -1,0 +1,198 @@
+/*
+ * bclx — B200 (sm_100a) sparse tile multiply for BCL containers: the C ABI.
+ *
+ * This is the drop-in boundary under the BCL container API.  The reference
+ * (berkeley-container-library/bcl) runs these operations as header-only C++
+ * inside its SUMMA-style tile loop; every entry point below replaces one of
+ * those local kernels (or the whole loop) with device-resident tiles and
+ * hand-written CUDA kernels.  Paths are relative to the BCL tree.
+ *
+ *   bclx_spgemm_symbolic / _numeric   BCL::gemm(SPMatrix, SPMatrix, SPMatrix&)
+ *                                     bcl/containers/algorithms/spgemm.hpp:182-242
+ *                                     (a 1x1x1 grid is the local tile product
+ *                                     CSRMatrix::dot -> gemm(CSR, CSR, CSR&),
+ *                                     spgemm.hpp:41-76, CSRMatrix.hpp:229-235)
+ *   bclx_tile_accumulate_*            SparseHashAccumulator::accumulate/get_matrix
+ *                                     bcl/containers/sequential/SparseHashAccumulator.hpp:86-183
+ *   bclx_spmm_tile                    spmm_wrapper(m, n, k, nnz, c, b, vals, rowptr,
+ *                                     colind, ldb, ldc), spgemm.hpp:140-149 (80-96)
+ *   bclx_spmm_grid                    BCL::gemm(SPMatrix, DMatrix, DMatrix&)
+ *                                     spgemm.hpp:153-179
+ *
+ * Semantics kept from the reference:
+ *   - output structure is the symbolic pattern (entries that sum to zero are
+ *     kept), columns sorted within each row (CSRMatrix.hpp:107-165);
+ *   - per output entry, a tile product sums from 0 in stored A-row order with
+ *     fused multiply-adds; C tile (i, j) adds its partial products for
+ *     k = (k_ + i + j) mod G, k_ = 0..G-1, in that order (spgemm.hpp:204-224,
+ *     SimpleHash.hpp:88-119).  FP32 results are therefore bit-identical to
+ *     the reference CPU build (which contracts `c += a*b` to an FMA), and
+ *     int32 results are exact;
+ *   - SpMM accumulates into C in place (beta = 1), C tiles in rotated k order.
+ *
+ * Conventions: all matrix pointers are DEVICE pointers; index arrays are
+ * int32 (the reference's default index type); row_ptr holds m+1 entries.
+ * No exceptions cross this boundary: every call returns a bclx_status_t
+ * (the C++ layer in include/bclx/ turns errors into std::runtime_error, as
+ * the reference does for bad shapes and out-of-memory).  Calls on one context
+ * are ordered on the context's stream and are not thread-safe against each
+ * other; distinct contexts are independent.
+ */
+#ifndef BCLX_H
+#define BCLX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BCLX_API __attribute__((visibility("default")))
+#else
+#define BCLX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  BCLX_OK = 0,
+  BCLX_ERR_INVALID = 1,         /* bad argument or shape mismatch */
+  BCLX_ERR_DTYPE = 2,           /* unsupported value type for this call */
+  BCLX_ERR_CUDA = 3,            /* a CUDA runtime call failed (see bclx_last_error) */
+  BCLX_ERR_NO_MEMORY = 4,       /* device allocation failed */
+  BCLX_ERR_INDEX_OVERFLOW = 5,  /* a tile's nnz does not fit the int32 index type */
+  BCLX_ERR_DEVICE_TIMEOUT = 6,  /* a bounded device-side wait gave up */
+  BCLX_ERR_NO_DEVICE = 7        /* no usable sm_100 device */
+} bclx_status_t;
+
+typedef enum {
+  BCLX_F32 = 0,   /* float */
+  BCLX_I32 = 1,   /* int32_t */
+  BCLX_BF16 = 2   /* bfloat16 storage (SpMM B and C only) */
+} bclx_dtype_t;
+
+/* One CSR tile (CSRMatrix<T, int>): m x n, nnz entries, device pointers. */
+typedef struct {
+  int64_t m, n, nnz;
+  int32_t* row_ptr; /* [m+1] */
+  int32_t* col_ind; /* [nnz], tile-local columns, sorted per row */
+  void* vals;       /* [nnz] of dtype */
+  int32_t dtype;
+  int32_t pad_;
+} bclx_csr_t;
+
+/* A tile grid of CSR tiles (SPMatrix<T, int>): tile (i, j) holds rows
+ * [i*tile_m, min((i+1)*tile_m, m)) and columns [j*tile_n, min(.., n)),
+ * as in SPMatrix::tile_shape(index) (SPMatrix.hpp:401-405).
+ * `tiles` is a DEVICE array of grid_m*grid_n descriptors, row-major. */
+typedef struct {
+  int64_t m, n;
+  int64_t tile_m, tile_n;
+  int64_t grid_m, grid_n;
+  const bclx_csr_t* tiles;
+  int32_t dtype;
+  int32_t pad_;
+} bclx_spgrid_t;
+
+/* Output tile grid of a sparse product, packed in one allocation per array:
+ * tile t = i*grid_n + j owns entries [tile_offset[t], tile_offset[t+1]) of
+ * col_ind/vals, and its local row_ptr is tile_row_ptr + t*(tile_m+1)
+ * (edge tiles repeat their nnz past their last row). */
+typedef struct {
+  int64_t m, n;
+  int64_t tile_m, tile_n;
+  int64_t grid_m, grid_n;
+  int32_t* tile_row_ptr; /* [grid_m*grid_n*(tile_m+1)], written by symbolic */
+  int64_t* tile_offset;  /* [grid_m*grid_n+1], written by symbolic */
+  int32_t* col_ind;      /* [nnz], written by numeric */
+  void* vals;            /* [nnz], written by numeric */
+  int32_t dtype;
+  int32_t pad_;
+} bclx_spgrid_out_t;
+
+/* A tile grid of dense tiles (DMatrix<T>): every tile is a row-major
+ * tile_m x tile_n block with leading dimension tile_n, padded to full size
+ * even at the edges (DMatrix.hpp:55-95, 151-173).  `tiles` is a DEVICE array
+ * of grid_m*grid_n base pointers, row-major. */
+typedef struct {
+  int64_t m, n;
+  int64_t tile_m, tile_n;
+  int64_t grid_m, grid_n;
+  void* const* tiles;
+  int32_t dtype;
+  int32_t pad_;
+} bclx_dgrid_t;
+
+typedef struct bclx_context_s* bclx_context_t;
+typedef struct bclx_spgemm_plan_s* bclx_spgemm_plan_t;
+
+/* ---- context: device, stream, stream-ordered scratch pool ------------- */
+/* Replaces the backend/segment set-up of BCL::init (backends/mpi/backend.hpp:78-118):
+ * one context per device; scratch comes from a stream-ordered pool. */
+BCLX_API int bclx_context_create(int device, bclx_context_t* ctx);
+BCLX_API int bclx_context_destroy(bclx_context_t ctx);
+/* Use `stream` (a cudaStream_t; NULL = legacy default) for every later call. */
+BCLX_API int bclx_context_set_stream(bclx_context_t ctx, void* stream);
+BCLX_API int bclx_context_synchronize(bclx_context_t ctx);
+/* Text of the last CUDA error seen on this thread (empty if none). */
+BCLX_API const char* bclx_last_error(void);
+/* Library version, e.g. 100 for 0.1.0. */
+BCLX_API int bclx_version(void);
+
+/* ---- sparse x sparse ---------------------------------------------------
+ * C = A * B over tile grids: A is m x k with grid (gm x gk), B is k x n with
+ * grid (gk x gn), C is m x n with grid (gm x gn); A's tile_n must equal B's
+ * tile_m, C's tile_m/tile_n must equal A's tile_m / B's tile_n
+ * (BCL::gemm(SPMatrix, SPMatrix, SPMatrix&), spgemm.hpp:182-242).
+ *
+ * Two phases.  symbolic sizes every output row (the union of all partial
+ * products of the row's tile), writes c->tile_row_ptr and c->tile_offset,
+ * returns the total nnz in *nnz (one device->host read) and a plan that holds
+ * the work decomposition.  The caller then provides c->col_ind and c->vals of
+ * that size, and numeric fills them.  numeric may run the SUMMA stages
+ * k_ in [stage_begin, stage_end) only: stage_begin == 0 starts C from zero,
+ * later ranges add onto the values already in c->vals, so running the stages
+ * one call at a time gives bit-identical results to one call over all of them
+ * (stage_end <= 0 means all stages). */
+BCLX_API int bclx_spgemm_symbolic(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_spgrid_t* b,
+                         bclx_spgrid_out_t* c, bclx_spgemm_plan_t* plan, int64_t* nnz);
+BCLX_API int bclx_spgemm_numeric(bclx_context_t ctx, bclx_spgemm_plan_t plan, const bclx_spgrid_t* a,
+                        const bclx_spgrid_t* b, bclx_spgrid_out_t* c, int32_t stage_begin,
+                        int32_t stage_end);
+BCLX_API int bclx_spgemm_plan_destroy(bclx_spgemm_plan_t plan);
+/* Plan statistics: [0] intermediate products, [1] row items, [2] work items,
+ * [3] work items in the large-accumulator class, [4] stages, [5] output nnz. */
+BCLX_API int bclx_spgemm_plan_stats(bclx_spgemm_plan_t plan, int64_t* out6);
+
+/* ---- tile accumulation ---------------------------------------------------
+ * C = parts[0] + parts[1] + ... (all m x n), per entry summed in list order
+ * from 0, union structure (SparseHashAccumulator::get_matrix,
+ * SparseHashAccumulator.hpp:101-182).  `parts` is a DEVICE array of nparts
+ * descriptors.  symbolic writes c_row_ptr[m+1] and returns *nnz; numeric
+ * fills c->col_ind / c->vals (c->row_ptr = the same c_row_ptr). */
+BCLX_API int bclx_tile_accumulate_symbolic(bclx_context_t ctx, const bclx_csr_t* parts, int32_t nparts,
+                                  int64_t m, int64_t n, int32_t dtype, int32_t* c_row_ptr,
+                                  bclx_spgemm_plan_t* plan, int64_t* nnz);
+BCLX_API int bclx_tile_accumulate_numeric(bclx_context_t ctx, bclx_spgemm_plan_t plan, const bclx_csr_t* parts,
+                                 int32_t nparts, bclx_csr_t* c);
+
+/* ---- sparse x dense ------------------------------------------------------
+ * C += A * B for one tile (spmm_wrapper, spgemm.hpp:140-149): A is m x k CSR
+ * (FP32 values), B is k x n row-major with leading dimension ldb, C is m x n
+ * row-major with leading dimension ldc.  bc_dtype: BCLX_F32 (bit-identical to
+ * the reference), or BCLX_BF16 (B and C stored as bfloat16, products chained
+ * in FP32 and each C row rounded once). */
+BCLX_API int bclx_spmm_tile(bclx_context_t ctx, int64_t m, int64_t n, int64_t k, int64_t nnz, void* c,
+                   const void* b, const float* a_values, const int32_t* a_rowptr,
+                   const int32_t* a_colind, int64_t ldb, int64_t ldc, int32_t bc_dtype);
+/* C += A * B over tile grids, every C tile over all k in rotated order, in
+ * one launch (BCL::gemm(SPMatrix, DMatrix, DMatrix&), spgemm.hpp:153-179).
+ * b->dtype == c->dtype selects FP32 or BF16 storage. */
+BCLX_API int bclx_spmm_grid(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_dgrid_t* b,
+                   const bclx_dgrid_t* c);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BCLX_H */

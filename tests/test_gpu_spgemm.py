@@ -1,0 +1,154 @@
+"""GPU parity of the sparse x sparse path, through the C ABI.
+
+Bar: structure (row_ptr, sorted col_ind, explicit zeros kept) bit-exact;
+values bit-exact for int32 and also bit-exact for FP32, because the kernels
+reproduce the reference's per-entry order of fused multiply-adds; the
+north-star tolerance (1e-5 relative per entry against the reference) is
+therefore met with zero error, and the FP32 result's error against an FP64
+accumulation is stated in test_fp32_error_vs_fp64."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from bcl_b200 import gen
+from oracle import oracle as O
+
+from gpu_util import GOLD, assert_csr_identical, assert_rel_close, load_csr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def product(a, b, tiles, mode="fused"):
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm, spgemm_plain
+    tm, tk, tn = tiles
+    A = SPMatrix.from_csr(a, BlockCustom((tm, tk)))
+    B = SPMatrix.from_csr(b, BlockCustom((tk, tn)))
+    if mode == "plain":
+        C = spgemm_plain(A, B)
+    else:
+        C = spgemm(A, B, stages=mode)
+    return C
+
+
+@pytest.mark.parametrize("mode", ["fused", "per_stage", "plain"])
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "spgemm_*.npz"))), ids=os.path.basename)
+def test_golden_spgemm(path, mode):
+    d = np.load(path)
+    a, b, c = load_csr(d, "a"), load_csr(d, "b"), load_csr(d, "c")
+    C = product(a, b, [int(t) for t in d["tiles"]], mode)
+    got = C.get()
+    assert_csr_identical(got, c.row_ptr, c.col_ind, c.vals)
+    assert C.nnz() == c.nnz
+
+
+def test_golden_dot_one_tile():
+    """The local tile kernel alone (CSRMatrix::dot) is a 1x1x1 grid."""
+    d = np.load(os.path.join(GOLD, "dot_rmat9_f32.npz"))
+    a, c = load_csr(d, "a"), load_csr(d, "c")
+    got = product(a, a, (a.m, a.n, a.n)).get()
+    assert_csr_identical(got, c.row_ptr, c.col_ind, c.vals)
+
+
+@pytest.mark.parametrize("name,mode", [("accumulate_rmat9x4_f32", "f32"), ("accumulate_rmat8x3_i32", "i32")])
+def test_golden_tile_accumulate(name, mode):
+    from bcl_b200.containers import BlockCustom, SPMatrix, tile_accumulate
+    d = np.load(os.path.join(GOLD, name + ".npz"))
+    parts, i = [], 0
+    while f"p{i}_shape" in d:
+        p = load_csr(d, f"p{i}")
+        parts.append(SPMatrix.from_csr(p, BlockCustom((p.m, p.n))))
+        i += 1
+    c = load_csr(d, "c")
+    got = tile_accumulate(parts).get()
+    assert_csr_identical(got, c.row_ptr, c.col_ind, c.vals)
+
+
+@pytest.mark.parametrize("value_type", ["f32", "i32"])
+@pytest.mark.parametrize("tiles", [(512, 512, 512), (300, 700, 260), (2048, 2048, 2048)])
+def test_rmat11_vs_oracle(value_type, tiles):
+    a = gen.rmat(11, seed=101, value_type=value_type)
+    rp, ci, cv = O.gemm_tiled(a, a, *tiles, mode=value_type)
+    got = product(a, a, tiles).get()
+    assert_csr_identical(got, rp, ci, cv)
+
+
+def test_sliced_rows_and_large_accumulator():
+    """Tiles 16384 columns wide force every row into >= 2 column slices, and
+    R-MAT's long rows produce work items with more than 512 outputs (the
+    large-accumulator kernel)."""
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm
+    a = gen.rmat(14, seed=7)
+    A = SPMatrix.from_csr(a, BlockCustom((4096, 16384)))
+    B = SPMatrix.from_csr(a, BlockCustom((16384, 16384)))
+    C, plan = spgemm(A, B, keep_plan=True)
+    st = plan.stats()
+    plan.close()
+    assert st["big_items"] > 0 and st["work_items"] > st["row_items"] // 4
+    rows = np.random.default_rng(0).choice(a.m, 2000, replace=False)
+    rows.sort()
+    rp, ci, cv = O.gemm_tiled(a, a, 4096, 16384, 16384, rows=rows)
+    full = C.get()
+    got_rp = full.row_ptr.astype(np.int64)
+    for q, r in enumerate(rows[:400]):
+        seg = slice(got_rp[r], got_rp[r + 1])
+        assert np.array_equal(full.col_ind[seg], ci[rp[q]:rp[q + 1]])
+        assert np.array_equal(full.vals[seg].view(np.uint32), cv[rp[q]:rp[q + 1]].view(np.uint32))
+    counts = np.diff(got_rp)[rows]
+    assert np.array_equal(counts, np.diff(rp))
+
+
+def test_empty_and_degenerate():
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm
+    z = gen.CSR(300, 200, np.zeros(301, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32))
+    b = gen.rmat(8, seed=1)
+    b = gen.CSR(200, 256, *_crop(b, 200, 256))
+    C = spgemm(SPMatrix.from_csr(z, BlockCustom((64, 50))), SPMatrix.from_csr(b, BlockCustom((50, 100))))
+    assert C.nnz() == 0
+    got = C.get()
+    assert got.m == 300 and got.n == 256 and got.row_ptr[-1] == 0
+    # a single nonzero
+    one = gen.CSR(1, 1, np.array([0, 1], np.int32), np.array([0], np.int32), np.array([3.0], np.float32))
+    C = spgemm(SPMatrix.from_csr(one, BlockCustom((1, 1))), SPMatrix.from_csr(one, BlockCustom((1, 1))))
+    assert C.get().vals.tolist() == [9.0]
+
+
+def _crop(a, m, n):
+    keep_rows = np.arange(m)
+    rp, ci, v = [0], [], []
+    for r in keep_rows:
+        s = slice(a.row_ptr[r], a.row_ptr[r + 1])
+        sel = a.col_ind[s] < n
+        ci.extend(a.col_ind[s][sel])
+        v.extend(a.vals[s][sel])
+        rp.append(len(ci))
+    return np.array(rp, np.int32), np.array(ci, np.int32), np.array(v, np.float32)
+
+
+def test_stencil_square_closed_form():
+    s = gen.stencil27(12)
+    C = product(s, s, (1024, 1024, 1024))
+    assert C.nnz() == (5 * 12 - 6) ** 3
+    rp, ci, cv = O.gemm_tiled(s, s, 1024, 1024, 1024)
+    assert_csr_identical(C.get(), rp, ci, cv)
+
+
+def test_fp32_error_vs_fp64():
+    """State the FP32 result's error against FP64 accumulation (R-MAT s12)."""
+    a = gen.rmat(12, seed=5)
+    got = product(a, a, (1024, 1024, 1024)).get()
+    _, _, c64 = O.gemm_tiled(a, a, 1024, 1024, 1024, mode="f64")
+    err = np.abs(got.vals.astype(np.float64) - c64)
+    scale = np.abs(c64)
+    rel = err / np.maximum(scale, 1e-12)
+    print(f"\nFP32 vs FP64: max abs {err.max():.3e}, median rel {np.median(rel):.3e}, "
+          f"norm ratio {np.linalg.norm(err) / np.linalg.norm(c64):.3e}")
+    assert np.linalg.norm(err) / np.linalg.norm(c64) < 1e-6

@@ -1,0 +1,102 @@
+"""GPU parity of the sparse x dense path, through the C ABI.
+
+FP32: bit-exact against the reference's own outputs (golden fixtures) and
+the oracle (same order of fused multiply-adds, C accumulated in place).
+BF16 storage: bit-exact against the oracle's BF16 restatement, and within
+1e-2 relative (Frobenius) of FP64 accumulation."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from bcl_b200 import gen
+from oracle import oracle as O
+
+from gpu_util import GOLD, bits, load_csr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def run(a, bd, tiles, mode="grid", dtype="f32", c0=None):
+    import torch
+    from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm, spmm_plain
+    tm, tk, tn = tiles
+    tdt = torch.float32 if dtype == "f32" else torch.bfloat16
+    A = SPMatrix.from_csr(a, BlockCustom((tm, tk)))
+    if dtype == "f32":
+        B = DMatrix.from_array(torch.from_numpy(bd), BlockCustom((tk, tn)), dtype=tdt)
+    else:
+        B = DMatrix.from_array(torch.from_numpy(bd.view(np.int16)).view(torch.bfloat16), BlockCustom((tk, tn)),
+                               dtype=tdt)
+    C = DMatrix.zeros((a.m, bd.shape[1]), BlockCustom((tm, tn)), dtype=tdt)
+    if c0 is not None:
+        C.set_matrix(torch.from_numpy(c0) if dtype == "f32" else torch.from_numpy(c0.view(np.int16)).view(torch.bfloat16))
+    (spmm if mode == "grid" else spmm_plain)(A, B, C)
+    out = C.get_matrix().cpu()
+    return out.numpy() if dtype == "f32" else out.view(torch.int16).numpy().view(np.uint16)
+
+
+@pytest.mark.parametrize("mode", ["grid", "plain"])
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "spmm_*.npz"))), ids=os.path.basename)
+def test_golden_spmm(path, mode):
+    d = np.load(path)
+    a = load_csr(d, "a")
+    got = run(a, d["b"], [int(t) for t in d["tiles"]], mode)
+    assert np.array_equal(bits(got), bits(d["c"]))
+
+
+@pytest.mark.parametrize("n,tiles", [(128, (4096, 4096, 128)), (37, (1000, 700, 37)), (600, (2048, 4096, 600)),
+                                     (256, (8192, 8192, 256))])
+def test_spmm_vs_oracle(n, tiles):
+    a = gen.rmat(13, seed=3)
+    b = gen.dense(a.n, n, seed=4)
+    c0 = gen.dense(a.m, n, seed=5)
+    got = run(a, b, tiles, c0=c0)
+    want = O.spmm_tiled(a, b, c0, *tiles)
+    assert np.array_equal(bits(got), bits(want))
+
+
+@pytest.mark.parametrize("n,tiles", [(256, (8192, 8192, 256)), (128, (4096, 4096, 128)), (40, (3000, 5000, 40))])
+def test_spmm_bf16(n, tiles):
+    a = gen.rmat(13, seed=8)
+    b = gen.dense(a.n, n, seed=9, dist="normal")
+    b16 = O.to_bf16(b)
+    got = run(a, b16, tiles, dtype="bf16", c0=np.zeros((a.m, n), np.uint16))
+    want = O.spmm_tiled_bf16(a, b16, np.zeros((a.m, n), np.uint16), *tiles)
+    assert np.array_equal(got, want)
+    c64 = O.spmm_f64(a, b)
+    err = np.linalg.norm(O.bf16_to_f32(got) - c64) / np.linalg.norm(c64)
+    print(f"\nBF16 storage vs FP64: relative Frobenius error {err:.3e}")
+    assert err < 1e-2
+
+
+def test_spmm_tile_single_call_ld():
+    """bclx_spmm_tile with leading dimensions larger than n (sub-blocks)."""
+    import ctypes
+    import torch
+    from bcl_b200 import _lib
+    from bcl_b200.containers import context
+    a = gen.erdos_renyi(500, 7, seed=1)
+    b = gen.dense(500, 96, seed=2)
+    c0 = gen.dense(500, 64, seed=3)
+    B = torch.from_numpy(b).cuda()            # ldb = 96, use the first 64 columns
+    C = torch.zeros((500, 80), device="cuda")  # ldc = 80
+    C[:, :64] = torch.from_numpy(c0)
+    rp = torch.from_numpy(a.row_ptr).cuda()
+    ci = torch.from_numpy(a.col_ind).cuda()
+    v = torch.from_numpy(a.vals).cuda()
+    h = context().use_current_stream()
+    _lib.call("bclx_spmm_tile", h, 500, 64, 500, a.nnz, ctypes.c_void_p(C.data_ptr()),
+              ctypes.c_void_p(B.data_ptr()), ctypes.c_void_p(v.data_ptr()), ctypes.c_void_p(rp.data_ptr()),
+              ctypes.c_void_p(ci.data_ptr()), 96, 80, _lib.F32)
+    want = O.spmm_tiled(a, b[:, :64].copy(), c0, 500, 500, 64)
+    assert np.array_equal(bits(C[:, :64].cpu().numpy()), bits(want))
+    assert torch.count_nonzero(C[:, 64:]) == 0
