@@ -61,6 +61,7 @@ SIGNATURES = {
     "bclx_context_synchronize": [vp],
     "bclx_last_error": [],
     "bclx_version": [],
+    "bclx_launch_count": [],
     "bclx_spgemm_symbolic": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
                              ctypes.POINTER(vp), ctypes.POINTER(i64)],
     "bclx_spgemm_numeric": [vp, vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
@@ -72,7 +73,7 @@ SIGNATURES = {
     "bclx_spmm_tile": [vp, i64, i64, i64, i64, vp, vp, vp, vp, vp, i64, i64, i32],
     "bclx_spmm_grid": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid)],
 }
-_RESTYPES = {"bclx_last_error": ctypes.c_char_p}
+_RESTYPES = {"bclx_last_error": ctypes.c_char_p, "bclx_launch_count": ctypes.c_longlong}
 
 
 class BclxError(RuntimeError):

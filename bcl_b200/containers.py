@@ -418,7 +418,7 @@ class SpgemmPlan:
     def stats(self) -> dict:
         arr = (ctypes.c_int64 * 6)()
         call("bclx_spgemm_plan_stats", self.h, arr)
-        keys = ["products", "row_items", "work_items", "big_items", "stages", "nnz"]
+        keys = ["products", "light_rows", "heavy_rows", "heavy_items", "stages", "nnz"]
         return dict(zip(keys, [int(x) for x in arr]))
 
     def close(self):

@@ -20,6 +20,9 @@ constexpr int kWarp = 32;
 
 void set_last_error(const std::string& msg);
 
+// Kernel launches issued by this library (all contexts), for launch accounting.
+void note_launch(int n = 1);
+
 #define BCLX_CK(call)                                                              \
   do {                                                                            \
     cudaError_t e_ = (call);                                                      \

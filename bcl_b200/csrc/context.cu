@@ -2,6 +2,7 @@
 // exclusive scan used to turn per-row counts into CSR offsets.
 #include "common.cuh"
 
+#include <atomic>
 #include <cstring>
 #include <string>
 
@@ -10,6 +11,9 @@ namespace bclx {
 static thread_local std::string g_last_error;
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<long long> g_launches{0};
+void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int scratch_alloc(Context* ctx, void** p, size_t bytes) {
   cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
@@ -115,6 +119,7 @@ static int exclusive_scan_impl(Context* ctx, const TIn* in, int64_t* out, int64_
   k_scan_reduce<TIn><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(in, n, sums);
   k_scan_sums<<<1, kScanThreads, 0, ctx->stream>>>(sums, nb);
   k_scan_final<TIn><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(in, n, sums, out);
+  note_launch(3);
   cudaError_t e = cudaGetLastError();
   scratch_free(ctx, sums);
   if (e != cudaSuccess) {
@@ -140,6 +145,8 @@ extern "C" {
 const char* bclx_last_error(void) { return g_last_error.c_str(); }
 
 int bclx_version(void) { return 100; }
+
+long long bclx_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int bclx_context_create(int device, bclx_context_t* out) {
   if (!out) return BCLX_ERR_INVALID;

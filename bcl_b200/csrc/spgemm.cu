@@ -3,29 +3,39 @@
 // spgemm.hpp:182-242, with its local kernel spgemm.hpp:41-76 and the tile
 // accumulation of SparseHashAccumulator.hpp:101-182), and tile accumulation.
 //
-// Work decomposition.  A "row item" is one row r of one C tile (i, j); it
-// owns every product A_ik[r, :] * B_kj over all k.  Long row items are split
-// into column slices ("work items") so that no work item sees more than a
-// few thousand products or more than kSliceCols output columns.
+// Work decomposition.  A "row" is one row r of one C tile (i, j); it owns the
+// products A_ik[r, :] * B_kj over every stage k.  Its intermediate-product
+// count (ub) classifies it:
+//   light (ub <= kLightUb):  one warp does the symbolic count and, later, the
+//                            whole numeric row (at most kLightUb outputs);
+//   heavy:                   one block does the symbolic pass (no ordering is
+//                            needed there) and leaves the row's column bitmap
+//                            in global memory; the row is then cut at
+//                            kFineCols-column block boundaries into items of
+//                            at most kVcap outputs, one warp each.
+// B rows are cut at the same block boundaries by a per-row table, so a heavy
+// item finds its part of every B row with two loads.
 //
-// Per work item, one warp:
-//   symbolic: sets one bit per product column in a shared-memory bitmap of
-//             the slice; the popcount is the output count.
-//   numeric:  rebuilds the bitmap (or reads the already-written columns),
-//             turns it into per-word prefix counts so that the output
-//             position of column j is rank(j) = prefix[j/32] + popc(lower
-//             bits); writes the sorted columns directly; then walks the
-//             products again in the reference's order and accumulates
-//             values into a shared-memory row indexed by rank.
+// Numeric, per item (one warp): the item's column bitmap (rebuilt from the
+// products for light rows, loaded for heavy items) is turned into per-word
+// prefix counts, so that column j's output position is
+// rank(j) = prefix[j/32] + popc(lower bits of its word); sorted columns are
+// written directly.  Then the products are walked in the reference's order
+// and values are accumulated in shared memory at rank(j).
 //
-// Order.  Products are enumerated 32 at a time in exactly the reference's
-// sequence: stages k = (k_ + i + j) mod G; inside a stage the A-row entries
-// in stored order; inside an entry the B-row entries in stored order.  In a
-// batch, lanes holding the same column are grouped with __match_any_sync and
-// the lowest lane applies the group's multiply-adds in lane order; batches
-// are separated by __syncwarp.  Every output entry therefore sees the same
-// chain of fused multiply-adds (from 0) per stage and the same chain of adds
-// across stages as the reference, so FP32 results are bit-identical.
+// Order.  The product stream of a row is: stages k = (k_ + i + j) mod G for
+// k_ = 0..G-1; inside a stage the A-row entries in stored order; inside an
+// entry the B-row entries in stored order.  It is walked 32 products at a
+// time, packed across A entries and stages.  Lanes holding the same column
+// are grouped with __match_any_sync and the lowest lane applies the group's
+// updates in lane order; batches are separated by __syncwarp.  Every column
+// keeps a running stage partial (`part`, started at 0 and advanced with a
+// fused multiply-add per product) and the sum of its finished stage partials
+// (`acc`, started at 0); when a product of a later stage arrives the partial
+// is added to acc first.  That is exactly the reference's arithmetic: each
+// tile product is an FMA chain from 0 in A-row order, and the partial tiles
+// are added from 0 in stage order.  FP32 results are bit-identical; int32
+// uses wrapping arithmetic and is exact.
 #include "common.cuh"
 
 #include <algorithm>
@@ -34,51 +44,38 @@
 
 namespace bclx {
 
-constexpr int kSliceCols = 8192;                 // bitmap capacity per work item (columns)
-constexpr int kBitmapWords = kSliceCols / 32;    // 256
-constexpr int64_t kSliceTarget = 4096;           // products per work item before a row is split
-constexpr int kMaxSlices = 64;
-constexpr int kVcapSmall = 512;                  // outputs per work item, small-accumulator kernel
-constexpr int kVcapBig = kSliceCols;             // outputs per work item, large kernel (= slice width)
+constexpr int kLightUb = 512;        // products of a light row (so <= 512 outputs)
+constexpr int kVcap = 512;           // outputs per numeric item
+constexpr int kFineCols = 256;       // column block of heavy rows and of the B-row table
+constexpr int kMaxWords = 512;       // bitmap words per warp (tiles up to 16384 columns)
+constexpr int kMaxCols = kMaxWords * 32;
 constexpr int kWarpsSym = 8;
-constexpr int kWarpsSmall = 8;
-constexpr int kWarpsBig = 2;
+constexpr int kHeavyThreads = 256;
+constexpr int kWarpsNum = 8;
+constexpr int kNoStage = 0xff;
 
 struct Geom {
-  int64_t gm, gk, gn;  // C grid is gm x gn; the k grid has gk tiles
-  int64_t tm, tn;      // C tile shape
-  int64_t m, n;        // C shape
-  int64_t n_row_items; // gm * gn * tm
+  int64_t gm, gk, gn;   // C grid is gm x gn; the k grid has gk tiles
+  int64_t tm, tn, tk;   // C tile shape; A tile width (= B tile height)
+  int64_t m, n;         // C shape
+  int64_t n_row_items;  // gm * gn * tm
+  int64_t nfb;          // fine blocks per (full) tile width: ceil(tn / kFineCols)
 };
 
-struct ItemInfo {
-  int64_t ri, ti, tj, r;
-  int s, ns, lo, hi;
+struct RowInfo {
+  int64_t ti, tj, r;
+  int w;  // width of the C tile (columns)
 };
 
-__device__ __forceinline__ void decode_row_item(const Geom& g, int64_t ri, int64_t& ti, int64_t& tj,
-                                                int64_t& r) {
-  int64_t t = ri / g.tm;
-  r = ri - t * g.tm;
-  ti = t / g.gn;
-  tj = t - ti * g.gn;
-}
-
-__device__ __forceinline__ int64_t encode_item(int64_t ri, int s, int ns) {
-  return ri | ((int64_t)s << 40) | ((int64_t)ns << 50);
-}
-
-__device__ __forceinline__ ItemInfo decode_item(const Geom& g, int64_t code) {
-  ItemInfo it;
-  it.ri = code & ((1LL << 40) - 1);
-  it.s = (int)((code >> 40) & 1023);
-  it.ns = (int)((code >> 50) & 1023);
-  decode_row_item(g, it.ri, it.ti, it.tj, it.r);
-  int64_t w = g.n - it.tj * g.tn;
-  if (w > g.tn) w = g.tn;
-  it.lo = (int)(w * it.s / it.ns);
-  it.hi = (int)(w * (it.s + 1) / it.ns);
-  return it;
+__device__ __forceinline__ RowInfo decode_row(const Geom& g, int64_t ri) {
+  RowInfo x;
+  const int64_t t = ri / g.tm;
+  x.r = ri - t * g.tm;
+  x.ti = t / g.gn;
+  x.tj = t - x.ti * g.gn;
+  int64_t w = g.n - x.tj * g.tn;
+  x.w = (int)(w < g.tn ? w : g.tn);
+  return x;
 }
 
 template <typename VT>
@@ -86,75 +83,129 @@ __device__ __forceinline__ VT load_val(const void* p, int64_t i) {
   return __ldg(reinterpret_cast<const VT*>(p) + i);
 }
 
-// Walk the products of C tile row r for one stage (A tile At, B tile Bt),
-// restricted to columns [lo, hi) when SLICED, 32 at a time in the reference's
-// order.  Every lane calls f(valid, j, a, b) once per batch (warp-uniform
-// control flow), valid lanes form a prefix of the warp.
-template <typename VT, bool SLICED, bool VALUES, typename F>
-__device__ __forceinline__ void for_each_product(const bclx_csr_t& At, const bclx_csr_t& Bt, int64_t r,
-                                                 int lo, int hi, F&& f) {
-  const int lane = lane_id();
-  const int32_t a0 = __ldg(At.row_ptr + r), a1 = __ldg(At.row_ptr + r + 1);
-  for (int32_t c0 = a0; c0 < a1; c0 += 32) {
-    const int32_t p = c0 + lane;
-    int32_t bs = 0, len = 0;
-    VT av = VT(0);
-    if (p < a1) {
-      const int32_t kc = __ldg(At.col_ind + p);
-      if (VALUES) av = load_val<VT>(At.vals, p);
-      bs = __ldg(Bt.row_ptr + kc);
-      int32_t be = __ldg(Bt.row_ptr + kc + 1);
-      if (SLICED) {
-        const int32_t s0 = lower_bound_i32(Bt.col_ind, bs, be, lo);
-        be = lower_bound_i32(Bt.col_ind, s0, be, hi);
-        bs = s0;
-      }
-      len = be - bs;
-    }
-    const int32_t incl = warp_inclusive_scan(len);
-    const int32_t total = __shfl_sync(kFull, incl, 31);
-    const int32_t excl = incl - len;
-    for (int32_t base = 0; base < total; base += 32) {
-      const int32_t q = base + lane;
-      int src = 0;
+// Number of lanes whose inclusive prefix is <= q (incl is nondecreasing).
+__device__ __forceinline__ int warp_search(int32_t incl, int32_t q) {
+  int src = 0;
 #pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const int32_t v = __shfl_sync(kFull, incl, src + step - 1);
-        if (v <= q) src += step;
+  for (int step = 16; step >= 1; step >>= 1) {
+    const int32_t v = __shfl_sync(kFull, incl, src + step - 1);
+    if (v <= q) src += step;
+  }
+  return src;
+}
+
+template <typename P>
+__device__ __forceinline__ P* shfl_ptr(P* p, int src) {
+  unsigned long long u = reinterpret_cast<unsigned long long>(p);
+  u = __shfl_sync(kFull, u, src);
+  return reinterpret_cast<P*>(u);
+}
+
+// Walk the product stream of C-tile row `x` over stages [s0, s1), restricted
+// to fine blocks [fb_lo, fb_hi) of the row when RANGED (through the B-row
+// table `tab`), in the reference's order, 32 products per batch.  The batches
+// are dealt round-robin to `nparts` walkers and this one takes share `part`
+// (the numeric pass uses one share; the order-free symbolic pass of a heavy
+// row spreads the batches over the warps of a block).
+// Every lane calls f(valid, j, a, b, stage) once per batch.
+template <typename VT, bool VALUES, bool RANGED, typename F>
+__device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridView& B, const Geom& g,
+                                              const RowInfo& x, int s0, int s1, int fb_lo, int fb_hi,
+                                              const int32_t* __restrict__ tab, int part, int nparts, F&& f) {
+  const int lane = lane_id();
+  for (int g0 = s0; g0 < s1; g0 += 32) {
+    // one lane per stage: its A-row segment
+    const int kk = g0 + lane;
+    const bool sv = kk < s1;
+    const int64_t k = sv ? (kk + x.ti + x.tj) % g.gk : 0;
+    int32_t as = 0, alen = 0;
+    const int32_t* acol = nullptr;
+    const VT* aval = nullptr;
+    if (sv) {
+      const bclx_csr_t At = A.tile(x.ti, k);
+      as = __ldg(At.row_ptr + x.r);
+      alen = __ldg(At.row_ptr + x.r + 1) - as;
+      acol = At.col_ind;
+      aval = reinterpret_cast<const VT*>(At.vals);
+    }
+    const int32_t aincl = warp_inclusive_scan(alen);
+    const int32_t atot = __shfl_sync(kFull, aincl, 31);
+    const int32_t aexcl = aincl - alen;
+    for (int32_t e0 = 0; e0 < atot; e0 += 32) {
+      // one lane per A entry of the flattened stage stream
+      const int32_t e = e0 + lane;
+      const int sl = warp_search(aincl, e);
+      const int64_t sk = __shfl_sync(kFull, k, sl);
+      const int32_t sas = __shfl_sync(kFull, as, sl);
+      const int32_t sax = __shfl_sync(kFull, aexcl, sl);
+      const int32_t* sacol = shfl_ptr(acol, sl);
+      const VT* saval = VALUES ? shfl_ptr(aval, sl) : nullptr;
+      const int stage = g0 + sl;
+      int32_t len = 0;
+      VT av = VT(0);
+      const int32_t* bcol = nullptr;
+      const VT* bval = nullptr;
+      if (e < atot) {
+        const int32_t p = sas + (e - sax);
+        const int32_t kc = __ldg(sacol + p);
+        if (VALUES) av = __ldg(saval + p);
+        const bclx_csr_t Bt = B.tile(sk, x.tj);
+        int32_t bs, be;
+        if (RANGED) {
+          const int32_t* trow = tab + ((sk * g.gn + x.tj) * g.tk + kc) * (g.nfb + 1);
+          bs = __ldg(trow + fb_lo);
+          be = __ldg(trow + fb_hi);
+        } else {
+          bs = __ldg(Bt.row_ptr + kc);
+          be = __ldg(Bt.row_ptr + kc + 1);
+        }
+        len = be - bs;
+        bcol = Bt.col_ind + bs;
+        if (VALUES) bval = reinterpret_cast<const VT*>(Bt.vals) + bs;
       }
-      const int32_t sbs = __shfl_sync(kFull, bs, src);
-      const int32_t sex = __shfl_sync(kFull, excl, src);
-      const VT a = __shfl_sync(kFull, av, src);
-      const bool valid = q < total;
-      int32_t j = -1;
-      VT bv = VT(0);
-      if (valid) {
-        const int32_t bpos = sbs + (q - sex);
-        j = __ldg(Bt.col_ind + bpos);
-        if (VALUES) bv = load_val<VT>(Bt.vals, bpos);
+      const int32_t incl = warp_inclusive_scan(len);
+      const int32_t total = __shfl_sync(kFull, incl, 31);
+      const int32_t excl = incl - len;
+      for (int32_t base = part * 32; base < total; base += nparts * 32) {
+        const int32_t q = base + lane;
+        const int src = warp_search(incl, q);
+        const int32_t sex = __shfl_sync(kFull, excl, src);
+        const int32_t* sbcol = shfl_ptr(bcol, src);
+        const VT* sbval = VALUES ? shfl_ptr(bval, src) : nullptr;
+        const VT a = VALUES ? __shfl_sync(kFull, av, src) : VT(0);
+        const int pstage = __shfl_sync(kFull, stage, src);
+        const bool valid = q < total;
+        int32_t j = -1;
+        VT bv = VT(0);
+        if (valid) {
+          j = __ldg(sbcol + (q - sex));
+          if (VALUES) bv = __ldg(sbval + (q - sex));
+        }
+        f(valid, j, a, bv, pstage);
       }
-      f(valid, j, a, bv);
     }
   }
 }
 
-// ---- planning -------------------------------------------------------------------
+// ---- planning --------------------------------------------------------------------
 
-__global__ void k_spgemm_ub(SpGridView A, SpGridView B, Geom g, int64_t* __restrict__ ub,
-                            int32_t* __restrict__ nslices, unsigned long long* __restrict__ products) {
+// Per row: intermediate products; light/heavy classification into two lists.
+__global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restrict__ light_list,
+                           int32_t* __restrict__ heavy_list, int32_t* __restrict__ counters,
+                           unsigned long long* __restrict__ products, int heavy_min_cols) {
   const int lane = lane_id();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  int64_t mine = 0;
+  unsigned long long mine = 0;
   for (int64_t ri = warp; ri < g.n_row_items; ri += nwarps) {
-    int64_t ti, tj, r;
-    decode_row_item(g, ri, ti, tj, r);
+    const RowInfo x = decode_row(g, ri);
     int64_t tot = 0;
-    if (r < A.rows_of(ti)) {
+    if (x.r < A.rows_of(x.ti)) {
       for (int64_t k = 0; k < g.gk; k++) {
-        const bclx_csr_t At = A.tile(ti, k);
-        const bclx_csr_t Bt = B.tile(k, tj);
-        const int32_t a0 = __ldg(At.row_ptr + r), a1 = __ldg(At.row_ptr + r + 1);
+        const bclx_csr_t At = A.tile(x.ti, k);
+        const int32_t a0 = __ldg(At.row_ptr + x.r), a1 = __ldg(At.row_ptr + x.r + 1);
+        if (a0 == a1) continue;
+        const bclx_csr_t Bt = B.tile(k, x.tj);
         for (int32_t p = a0 + lane; p < a1; p += 32) {
           const int32_t kc = __ldg(At.col_ind + p);
           tot += __ldg(Bt.row_ptr + kc + 1) - __ldg(Bt.row_ptr + kc);
@@ -162,79 +213,118 @@ __global__ void k_spgemm_ub(SpGridView A, SpGridView B, Geom g, int64_t* __restr
       }
       tot = warp_sum(tot);
     }
-    if (lane == 0) {
-      ub[ri] = tot;
-      mine += tot;
-      int ns = 0;
-      if (tot > 0) {
-        int64_t w = g.n - tj * g.tn;
-        if (w > g.tn) w = g.tn;
-        int64_t by_cols = (w + kSliceCols - 1) / kSliceCols;
-        int64_t by_work = (tot + kSliceTarget - 1) / kSliceTarget;
-        if (by_work > kMaxSlices) by_work = kMaxSlices;
-        int64_t s = by_cols > by_work ? by_cols : by_work;
-        if (s > w) s = w;
-        ns = (int)s;
-      }
-      nslices[ri] = ns;
+    if (lane == 0 && tot > 0) {
+      mine += (unsigned long long)tot;
+      if (tot <= kLightUb && x.w < heavy_min_cols)
+        light_list[atomicAdd(&counters[0], 1)] = (int32_t)ri;
+      else
+        heavy_list[atomicAdd(&counters[1], 1)] = (int32_t)ri;
     }
   }
-  if (lane == 0 && mine) atomicAdd(products, (unsigned long long)mine);
+  if (lane == 0 && mine) atomicAdd(products, mine);
 }
 
-__global__ void k_build_items(Geom g, const int32_t* __restrict__ nslices, const int64_t* __restrict__ first,
-                              int64_t* __restrict__ items) {
-  for (int64_t ri = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ri < g.n_row_items;
-       ri += (int64_t)gridDim.x * blockDim.x) {
-    const int ns = nslices[ri];
-    const int64_t f = first[ri];
-    for (int s = 0; s < ns; s++) items[f + s] = encode_item(ri, s, ns);
+// B-row table: for every row of every B tile (k, j), the position of the
+// first entry in each fine column block: tab[((k*gn + j)*tk + r)*(nfb+1) + b]
+// = first entry with column >= b*kFineCols (b = nfb: the row end).
+__global__ void k_btable(SpGridView B, Geom g, int32_t* __restrict__ tab) {
+  const int lane = lane_id();
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t nrows = g.gk * g.gn * g.tk;
+  for (int64_t x = warp; x < nrows; x += nwarps) {
+    const int64_t kt = x / g.tk, r = x - kt * g.tk;
+    const int64_t k = kt / g.gn, j = kt - k * g.gn;
+    if (r >= B.rows_of(k)) continue;
+    int32_t* trow = tab + x * (g.nfb + 1);
+    const bclx_csr_t Bt = B.tile(k, j);
+    const int32_t b0 = __ldg(Bt.row_ptr + r), b1 = __ldg(Bt.row_ptr + r + 1);
+    // entry q (or the row end) starts every block in (block(col[q-1]), block(col[q])]
+    for (int32_t q0 = b0; q0 <= b1; q0 += 32) {
+      const int32_t q = q0 + lane;
+      if (q <= b1) {
+        const int cur = q < b1 ? __ldg(Bt.col_ind + q) / kFineCols : (int)g.nfb;
+        const int prev = q > b0 ? __ldg(Bt.col_ind + q - 1) / kFineCols : -1;
+        for (int b = prev + 1; b <= cur && b <= g.nfb; b++) trow[b] = q;
+      }
+    }
   }
 }
 
-// ---- symbolic ------------------------------------------------------------------------
+// ---- symbolic ----------------------------------------------------------------------
 
 template <typename VT>
 __global__ void __launch_bounds__(kWarpsSym * 32)
-    k_spgemm_symbolic(SpGridView A, SpGridView B, Geom g, const int64_t* __restrict__ items, int64_t n_items,
-                      int32_t* __restrict__ item_count, int32_t* __restrict__ row_count,
-                      int64_t* __restrict__ big_list, int32_t* __restrict__ big_n) {
-  __shared__ uint32_t bm_all[kWarpsSym][kBitmapWords];
+    k_symbolic_light(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
+                     const int32_t* __restrict__ counters, int32_t* __restrict__ row_count) {
+  __shared__ uint32_t bm_all[kWarpsSym][kMaxWords];
   uint32_t* bm = bm_all[threadIdx.x >> 5];
   const int lane = lane_id();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t idx = warp; idx < n_items; idx += nwarps) {
-    const ItemInfo it = decode_item(g, items[idx]);
-    const int words = (it.hi - it.lo + 31) >> 5;
+  const int n_light = counters[0];
+  for (int64_t idx = warp; idx < n_light; idx += nwarps) {
+    const int64_t ri = light_list[idx];
+    const RowInfo x = decode_row(g, ri);
+    const int words = (x.w + 31) >> 5;
     for (int w = lane; w < words; w += 32) bm[w] = 0u;
     __syncwarp();
-    const int lo = it.lo;
-    auto setbit = [&](bool valid, int32_t j, VT, VT) {
-      if (valid) atomicOr(&bm[(j - lo) >> 5], 1u << ((j - lo) & 31));
-    };
-    for (int64_t k = 0; k < g.gk; k++) {
-      const bclx_csr_t At = A.tile(it.ti, k);
-      const bclx_csr_t Bt = B.tile(k, it.tj);
-      if (it.ns > 1)
-        for_each_product<VT, true, false>(At, Bt, it.r, it.lo, it.hi, setbit);
-      else
-        for_each_product<VT, false, false>(At, Bt, it.r, it.lo, it.hi, setbit);
-    }
+    walk_products<VT, false, false>(A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, 0, 1,
+                                    [&](bool valid, int32_t j, VT, VT, int) {
+                                      if (valid) atomicOr(&bm[j >> 5], 1u << (j & 31));
+                                    });
     __syncwarp();
     int cnt = 0;
     for (int w = lane; w < words; w += 32) cnt += __popc(bm[w]);
     cnt = warp_sum(cnt);
-    if (lane == 0) {
-      item_count[idx] = cnt;
-      if (cnt) atomicAdd(&row_count[it.ri], cnt);
-      if (cnt > kVcapSmall) big_list[atomicAdd(big_n, 1)] = idx;
-    }
+    if (lane == 0) row_count[ri] = cnt;
     __syncwarp();
   }
 }
 
-// tile_row_ptr / tile_offset from the row offsets (row items are tile-major).
+// One block per heavy row: all warps set bits of the row's bitmap in shared
+// memory (bit order does not matter), then the bitmap is stored for the
+// numeric pass.  hbm_words = words per stored bitmap.
+template <typename VT>
+__global__ void __launch_bounds__(kHeavyThreads)
+    k_symbolic_heavy(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ heavy_list,
+                     const int32_t* __restrict__ counters, int32_t* __restrict__ row_count,
+                     uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words) {
+  extern __shared__ uint32_t hbm_smem[];  // hbm_words
+  __shared__ int red[kHeavyThreads / 32];
+  const int n_heavy = counters[1];
+  const int wid = threadIdx.x >> 5, nw = kHeavyThreads / 32;
+  for (int64_t h = blockIdx.x; h < n_heavy; h += gridDim.x) {
+    const int64_t ri = heavy_list[h];
+    const RowInfo x = decode_row(g, ri);
+    const int words = (x.w + 31) >> 5;
+    for (int w = threadIdx.x; w < words; w += kHeavyThreads) hbm_smem[w] = 0u;
+    __syncthreads();
+    walk_products<VT, false, false>(A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, wid, nw,
+                                    [&](bool valid, int32_t j, VT, VT, int) {
+                                      if (valid) atomicOr(&hbm_smem[j >> 5], 1u << (j & 31));
+                                    });
+    __syncthreads();
+    int cnt = 0;
+    uint32_t* out = heavy_bitmaps + h * hbm_words;
+    for (int w = threadIdx.x; w < words; w += kHeavyThreads) {
+      const uint32_t v = hbm_smem[w];
+      out[w] = v;
+      cnt += __popc(v);
+    }
+    cnt = warp_sum(cnt);
+    if ((threadIdx.x & 31) == 0) red[wid] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int q = 0; q < nw; q++) t += red[q];
+      row_count[ri] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// tile_row_ptr / tile_offset from the row offsets (rows are tile-major).
 __global__ void k_tile_ptrs(Geom g, const int64_t* __restrict__ row_offset, int32_t* __restrict__ tile_row_ptr,
                             int64_t* __restrict__ tile_offset, int32_t* __restrict__ overflow) {
   const int64_t ntiles = g.gm * g.gn;
@@ -250,82 +340,147 @@ __global__ void k_tile_ptrs(Geom g, const int64_t* __restrict__ row_offset, int3
   }
 }
 
-// ---- numeric -------------------------------------------------------------------------
-
-template <typename VT, int VCAP>
-struct WarpSmem {
-  uint32_t bm[kBitmapWords];
-  uint32_t pre[kBitmapWords];
-  VT part[VCAP];
-  VT acc[VCAP];
-  VT sa[32];
-  VT sb[32];
+// Heavy rows are cut at fine-block boundaries into items of <= kVcap outputs
+// (greedy left to right; leading empty blocks are skipped).  One thread per
+// heavy row; FILL = false counts the items, FILL = true writes them.
+struct HeavyItem {
+  int32_t h;       // heavy slot
+  int16_t fb_lo;   // first fine block
+  int16_t fb_hi;   // one past the last
+  int32_t rel;     // output offset inside the row
+  int32_t count;   // outputs
 };
 
-template <typename VT, int VCAP, int WARPS, bool BIG>
-__global__ void __launch_bounds__(WARPS * 32)
-    k_spgemm_numeric(SpGridView A, SpGridView B, Geom g, const int64_t* __restrict__ items, int64_t n_items,
-                     const int64_t* __restrict__ big_list, const int32_t* __restrict__ big_n,
-                     const int32_t* __restrict__ item_count, const int64_t* __restrict__ row_offset,
-                     int32_t* __restrict__ out_col, VT* __restrict__ out_val, int stage_begin, int stage_end) {
+template <bool FILL>
+__global__ void k_cut_heavy(Geom g, const int32_t* __restrict__ heavy_list, const int32_t* __restrict__ counters,
+                            const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
+                            int32_t* __restrict__ n_items, const int64_t* __restrict__ first,
+                            HeavyItem* __restrict__ items) {
+  const int n_heavy = counters[1];
+  for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n_heavy; h += (int64_t)gridDim.x * blockDim.x) {
+    const RowInfo x = decode_row(g, heavy_list[h]);
+    const int nfb = (x.w + kFineCols - 1) / kFineCols;
+    const uint32_t* bm = heavy_bitmaps + h * hbm_words;
+    const int words = (x.w + 31) >> 5;
+    int nit = 0, cur = 0, start = 0, rel = 0;
+    int64_t out = FILL ? first[h] : 0;
+    for (int b = 0; b < nfb; b++) {
+      int c = 0;
+      for (int w = b * (kFineCols / 32); w < (b + 1) * (kFineCols / 32) && w < words; w++) c += __popc(__ldg(bm + w));
+      if (cur > 0 && cur + c > kVcap) {
+        if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)b, rel, cur};
+        nit++;
+        rel += cur;
+        cur = 0;
+        start = b;
+      }
+      if (cur == 0 && c == 0) start = b + 1;
+      cur += c;
+    }
+    if (cur > 0) {
+      if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)nfb, rel, cur};
+      nit++;
+    }
+    if (!FILL) n_items[h] = nit;
+  }
+}
+
+// ---- numeric ------------------------------------------------------------------------------
+
+template <typename VT, int WORDS>
+struct WarpSmem {
+  uint32_t bm[WORDS];
+  uint16_t pre[WORDS];
+  VT acc[kVcap];
+  VT part[kVcap];
+  unsigned char tag[kVcap];
+  VT sa[32];
+  VT sb[32];
+  int32_t ss[32];
+};
+
+template <typename VT, int WORDS>
+__global__ void __launch_bounds__(kWarpsNum * 32)
+    k_numeric(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
+              const int32_t* __restrict__ heavy_list, const int32_t* __restrict__ counters,
+              const HeavyItem* __restrict__ heavy_items, const int64_t* __restrict__ heavy_first,
+              const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, const int32_t* __restrict__ tab,
+              const int32_t* __restrict__ row_count, const int64_t* __restrict__ row_offset,
+              int32_t* __restrict__ out_col, VT* __restrict__ out_val, int s0, int s1) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  WarpSmem<VT, VCAP>& S = reinterpret_cast<WarpSmem<VT, VCAP>*>(smem_raw)[threadIdx.x >> 5];
+  WarpSmem<VT, WORDS>& S = reinterpret_cast<WarpSmem<VT, WORDS>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = lane_id();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t limit = BIG ? (int64_t)*big_n : n_items;
-  for (int64_t w_i = warp; w_i < limit; w_i += nwarps) {
-    const int64_t idx = BIG ? big_list[w_i] : w_i;
-    const int cnt = item_count[idx];
-    if (!BIG && (cnt == 0 || cnt > VCAP)) continue;
-    const ItemInfo it = decode_item(g, items[idx]);
-    const int lo = it.lo;
-    const int words = (it.hi - it.lo + 31) >> 5;
-
-    // output offset: the row's offset plus the counts of the earlier slices
-    int64_t off = 0;
-    for (int q = lane; q < it.s; q += 32) off += item_count[idx - it.s + q];
-    off = warp_sum(off) + row_offset[it.ri];
-
-    // 1. bitmap of the item's output columns
-    for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
-    __syncwarp();
-    if (stage_begin == 0) {
-      auto setbit = [&](bool valid, int32_t j, VT, VT) {
-        if (valid) atomicOr(&S.bm[(j - lo) >> 5], 1u << ((j - lo) & 31));
-      };
-      for (int64_t k = 0; k < g.gk; k++) {
-        const bclx_csr_t At = A.tile(it.ti, k);
-        const bclx_csr_t Bt = B.tile(k, it.tj);
-        if (it.ns > 1)
-          for_each_product<VT, true, false>(At, Bt, it.r, it.lo, it.hi, setbit);
-        else
-          for_each_product<VT, false, false>(At, Bt, it.r, it.lo, it.hi, setbit);
-      }
+  const int n_light = counters[0];
+  const int64_t n_heavy_items = heavy_first[counters[1]];
+  const int64_t n_total = n_heavy_items + n_light;
+  for (int64_t idx = warp; idx < n_total; idx += nwarps) {
+    // heavy items first (they are the larger ones)
+    const bool heavy = idx < n_heavy_items;
+    int64_t ri;
+    int cnt, fb_lo = 0, fb_hi = 0, lo = 0, hi;
+    int64_t off;
+    const uint32_t* hb = nullptr;
+    if (heavy) {
+      const HeavyItem it = heavy_items[idx];
+      ri = heavy_list[it.h];
+      cnt = it.count;
+      fb_lo = it.fb_lo;
+      fb_hi = it.fb_hi;
+      off = row_offset[ri] + it.rel;
+      hb = heavy_bitmaps + (int64_t)it.h * hbm_words;
     } else {
-      for (int q = lane; q < cnt; q += 32) {
-        const int x = out_col[off + q] - lo;
-        atomicOr(&S.bm[x >> 5], 1u << (x & 31));
+      ri = light_list[idx - n_heavy_items];
+      cnt = row_count[ri];
+      off = row_offset[ri];
+    }
+    const RowInfo x = decode_row(g, ri);
+    if (heavy) {
+      lo = fb_lo * kFineCols;
+      hi = min(fb_hi * kFineCols, x.w);
+    } else {
+      hi = x.w;
+    }
+    const int w0 = lo >> 5;
+    const int words = ((hi - lo) + 31) >> 5;
+
+    // 1. column bitmap of the item (word w covers columns lo + 32w ..)
+    if (heavy) {
+      for (int w = lane; w < words; w += 32) S.bm[w] = __ldg(hb + w0 + w);
+    } else {
+      for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
+      __syncwarp();
+      if (s0 == 0) {
+        walk_products<VT, false, false>(A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, 0, 1,
+                                        [&](bool valid, int32_t j, VT, VT, int) {
+                                          if (valid) atomicOr(&S.bm[j >> 5], 1u << (j & 31));
+                                        });
+      } else {
+        for (int q = lane; q < cnt; q += 32) {
+          const int j = out_col[off + q];
+          atomicOr(&S.bm[j >> 5], 1u << (j & 31));
+        }
       }
     }
     __syncwarp();
 
-    // 2. per-word exclusive prefix of the popcounts
+    // 2. per-word exclusive prefix counts
     {
       const int per = (words + 31) >> 5;
-      const int w0 = lane * per;
+      const int wa = lane * per;
       int loc = 0;
-      for (int w = w0; w < w0 + per && w < words; w++) loc += __popc(S.bm[w]);
+      for (int w = wa; w < wa + per && w < words; w++) loc += __popc(S.bm[w]);
       int ex = warp_inclusive_scan(loc) - loc;
-      for (int w = w0; w < w0 + per && w < words; w++) {
-        S.pre[w] = ex;
+      for (int w = wa; w < wa + per && w < words; w++) {
+        S.pre[w] = (uint16_t)ex;
         ex += __popc(S.bm[w]);
       }
     }
     __syncwarp();
 
-    // 3. sorted columns (first pass only) and accumulator start values
-    if (stage_begin == 0) {
+    // 3. sorted columns (first stage range only) and the accumulators
+    if (s0 == 0) {
       for (int w = lane; w < words; w += 32) {
         uint32_t bits = S.bm[w];
         int pos = S.pre[w];
@@ -336,67 +491,58 @@ __global__ void __launch_bounds__(WARPS * 32)
         }
       }
     }
-    VT* acc = S.acc;
-    VT* part = S.part;
     for (int q = lane; q < cnt; q += 32) {
-      acc[q] = stage_begin == 0 ? VT(0) : out_val[off + q];
-      part[q] = VT(0);
+      S.acc[q] = s0 == 0 ? VT(0) : out_val[off + q];
+      S.part[q] = VT(0);
+      S.tag[q] = (unsigned char)kNoStage;
     }
-    bool acc_zero = stage_begin == 0;
     __syncwarp();
 
-    // 4. values, stage by stage in rotated order
-    for (int kk = stage_begin; kk < stage_end; kk++) {
-      const int64_t k = (kk + it.ti + it.tj) % g.gk;
-      const bclx_csr_t At = A.tile(it.ti, k);
-      const bclx_csr_t Bt = B.tile(k, it.tj);
-      bool any = false;
-      auto update = [&](bool valid, int32_t j, VT a, VT b) {
-        any = true;
-        int rank = 0;
-        if (valid) {
-          const int x = j - lo;
-          rank = S.pre[x >> 5] + __popc(S.bm[x >> 5] & ((1u << (x & 31)) - 1u));
-        }
-        const unsigned peers = __match_any_sync(kFull, valid ? j : -1);
-        S.sa[lane] = a;
-        S.sb[lane] = b;
-        __syncwarp();
-        if (valid && lane == __ffs(peers) - 1) {
-          VT v = part[rank];
-          unsigned gmask = peers;
-          do {
-            const int mbr = __ffs(gmask) - 1;
-            gmask &= gmask - 1;
-            v = madd(S.sa[mbr], S.sb[mbr], v);
-          } while (gmask);
-          part[rank] = v;
-        }
-        __syncwarp();
-      };
-      if (it.ns > 1)
-        for_each_product<VT, true, true>(At, Bt, it.r, it.lo, it.hi, update);
-      else
-        for_each_product<VT, false, true>(At, Bt, it.r, it.lo, it.hi, update);
-      if (!any) continue;
-      if (acc_zero) {
-        // 0 + partial == partial: swap roles instead of adding (the old
-        // accumulator is all zeros and becomes the next partial).
-        VT* t = acc;
-        acc = part;
-        part = t;
-        acc_zero = false;
-      } else {
-        for (int q = lane; q < cnt; q += 32) {
-          acc[q] = vadd(acc[q], part[q]);
-          part[q] = VT(0);
-        }
+    // 4. values in the reference's order, with a lazy per-column stage fold
+    auto update = [&](bool valid, int32_t j, VT a, VT b, int stage) {
+      int rank = 0;
+      if (valid) {
+        const int xx = j - lo;
+        rank = S.pre[xx >> 5] + __popc(S.bm[xx >> 5] & ((1u << (xx & 31)) - 1u));
+      }
+      const unsigned peers = __match_any_sync(kFull, valid ? j : -1);
+      S.sa[lane] = a;
+      S.sb[lane] = b;
+      S.ss[lane] = stage;
+      __syncwarp();
+      if (valid && lane == __ffs(peers) - 1) {
+        VT v = S.part[rank];
+        int t = S.tag[rank];
+        VT ac = S.acc[rank];
+        unsigned gmask = peers;
+        do {
+          const int mb = __ffs(gmask) - 1;
+          gmask &= gmask - 1;
+          const int st = S.ss[mb];
+          if (st != t) {
+            if (t != kNoStage) ac = vadd(ac, v);
+            v = VT(0);
+            t = st;
+          }
+          v = madd(S.sa[mb], S.sb[mb], v);
+        } while (gmask);
+        S.part[rank] = v;
+        S.tag[rank] = (unsigned char)t;
+        S.acc[rank] = ac;
       }
       __syncwarp();
-    }
+    };
+    if (heavy)
+      walk_products<VT, true, true>(A, B, g, x, s0, s1, fb_lo, fb_hi, tab, 0, 1, update);
+    else
+      walk_products<VT, true, false>(A, B, g, x, s0, s1, 0, 0, nullptr, 0, 1, update);
 
-    // 5. values out
-    for (int q = lane; q < cnt; q += 32) out_val[off + q] = acc[q];
+    // 5. last fold and values out
+    for (int q = lane; q < cnt; q += 32) {
+      VT v = S.acc[q];
+      if (S.tag[q] != kNoStage) v = vadd(v, S.part[q]);
+      out_val[off + q] = v;
+    }
     __syncwarp();
   }
 }
@@ -426,17 +572,19 @@ struct bclx_spgemm_plan_s {
   Context* ctx = nullptr;
   Geom g{};
   int dtype = BCLX_F32;
-  int64_t products = 0, n_items = 0, nnz = 0, n_big = 0;
-  int64_t* ub = nullptr;
-  int32_t* nslices = nullptr;
-  int64_t* first = nullptr;
-  int64_t* items = nullptr;
-  int32_t* item_count = nullptr;
+  int64_t products = 0, nnz = 0, n_light = 0, n_heavy = 0, n_heavy_items = 0;
+  int64_t hbm_words = 0;
+  int32_t* light_list = nullptr;
+  int32_t* heavy_list = nullptr;
+  int32_t* counters = nullptr;  // [0] light rows, [1] heavy rows, [2] overflow flag
+  unsigned long long* products_dev = nullptr;
   int32_t* row_count = nullptr;
   int64_t* row_offset = nullptr;
-  int64_t* big_list = nullptr;
-  int32_t* flags = nullptr;  // [0] big count, [1] overflow
-  unsigned long long* products_dev = nullptr;
+  uint32_t* heavy_bitmaps = nullptr;
+  int32_t* heavy_nitems = nullptr;
+  int64_t* heavy_first = nullptr;
+  HeavyItem* heavy_items = nullptr;
+  int32_t* tab = nullptr;
   // tile accumulation: identity A tiles and their descriptors, 1x1 C offsets
   int32_t* id_rp = nullptr;
   int32_t* id_ci = nullptr;
@@ -445,12 +593,16 @@ struct bclx_spgemm_plan_s {
   int64_t* acc_tile_offset = nullptr;
 
   void release() {
-    void* ps[] = {ub, nslices, first, items, item_count, row_count, row_offset, big_list, flags, products_dev,
-                  id_rp, id_ci, id_v, id_desc, acc_tile_offset};
+    void* ps[] = {light_list, heavy_list, counters, products_dev, row_count, row_offset, heavy_bitmaps,
+                  heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset};
     for (void* p : ps) scratch_free(ctx, p);
-    ub = nullptr; nslices = nullptr; first = nullptr; items = nullptr; item_count = nullptr;
-    row_count = nullptr; row_offset = nullptr; big_list = nullptr; flags = nullptr; products_dev = nullptr;
-    id_rp = nullptr; id_ci = nullptr; id_v = nullptr; id_desc = nullptr; acc_tile_offset = nullptr;
+    light_list = heavy_list = counters = row_count = heavy_nitems = tab = id_rp = id_ci = nullptr;
+    products_dev = nullptr;
+    row_offset = heavy_first = acc_tile_offset = nullptr;
+    heavy_bitmaps = nullptr;
+    heavy_items = nullptr;
+    id_v = nullptr;
+    id_desc = nullptr;
   }
 };
 
@@ -469,9 +621,15 @@ static int check_grids(const bclx_spgrid_t* a, const bclx_spgrid_t* b, const bcl
   if (a->n != b->m || a->m != c->m || b->n != c->n) return BCLX_ERR_INVALID;
   if (a->tile_n != b->tile_m || a->grid_n != b->grid_m) return BCLX_ERR_INVALID;
   if (a->tile_m != c->tile_m || b->tile_n != c->tile_n) return BCLX_ERR_INVALID;
-  if (a->grid_n < 1 || a->grid_n > INT32_MAX) return BCLX_ERR_INVALID;
-  if (c->tile_n > (int64_t)1023 * kSliceCols) return BCLX_ERR_INVALID;
-  if (a->tile_m > INT32_MAX || b->tile_n > INT32_MAX) return BCLX_ERR_INDEX_OVERFLOW;
+  if (a->grid_n < 1 || a->grid_n >= kNoStage) {
+    set_last_error("the k dimension must have between 1 and 254 tiles");
+    return BCLX_ERR_INVALID;
+  }
+  if (c->tile_n > kMaxCols) {
+    set_last_error("tiles wider than 16384 columns are not supported; use a finer tile grid");
+    return BCLX_ERR_INVALID;
+  }
+  if (c->grid_m * c->grid_n * c->tile_m > INT32_MAX) return BCLX_ERR_INDEX_OVERFLOW;
   if (a->dtype != b->dtype || a->dtype != c->dtype || !value_size(a->dtype)) return BCLX_ERR_DTYPE;
   return BCLX_OK;
 }
@@ -486,10 +644,34 @@ static unsigned grid_for(Context* ctx, int64_t work_warps, int warps_per_block, 
 
 template <typename VT>
 static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P) {
-  unsigned blocks = grid_for(ctx, P->n_items, kWarpsSym, 16);
-  k_spgemm_symbolic<VT><<<blocks, kWarpsSym * 32, 0, ctx->stream>>>(A, B, P->g, P->items, P->n_items,
-                                                                   P->item_count, P->row_count, P->big_list,
-                                                                   P->flags);
+  const Geom& g = P->g;
+  if (P->n_light > 0) {
+    k_symbolic_light<VT><<<grid_for(ctx, P->n_light, kWarpsSym, 8), kWarpsSym * 32, 0, ctx->stream>>>(
+        A, B, g, P->light_list, P->counters, P->row_count);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+  if (P->n_heavy > 0) {
+    const size_t smem = sizeof(uint32_t) * (size_t)P->hbm_words;
+    k_symbolic_heavy<VT><<<grid_for(ctx, P->n_heavy, 1, 8), kHeavyThreads, smem, ctx->stream>>>(
+        A, B, g, P->heavy_list, P->counters, P->row_count, P->heavy_bitmaps, P->hbm_words);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+  return BCLX_OK;
+}
+
+template <typename VT, int WORDS>
+static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P,
+                            int32_t* out_col, void* out_val, int s0, int s1) {
+  constexpr size_t smem = sizeof(WarpSmem<VT, WORDS>) * kWarpsNum;
+  auto kern = k_numeric<VT, WORDS>;
+  BCLX_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t n_total = P->n_light + P->n_heavy_items;
+  kern<<<grid_for(ctx, n_total, kWarpsNum, 4), kWarpsNum * 32, smem, ctx->stream>>>(
+      A, B, P->g, P->light_list, P->heavy_list, P->counters, P->heavy_items, P->heavy_first, P->heavy_bitmaps,
+      P->hbm_words, P->tab, P->row_count, P->row_offset, out_col, reinterpret_cast<VT*>(out_val), s0, s1);
+  note_launch();
   BCLX_CK_LAUNCH();
   return BCLX_OK;
 }
@@ -497,86 +679,89 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
 template <typename VT>
 static int launch_numeric(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P,
                           int32_t* out_col, void* out_val, int s0, int s1) {
-  constexpr size_t small_smem = sizeof(WarpSmem<VT, kVcapSmall>) * kWarpsSmall;
-  constexpr size_t big_smem = sizeof(WarpSmem<VT, kVcapBig>) * kWarpsBig;
-  auto ks = k_spgemm_numeric<VT, kVcapSmall, kWarpsSmall, false>;
-  auto kb = k_spgemm_numeric<VT, kVcapBig, kWarpsBig, true>;
-  BCLX_CK(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small_smem));
-  BCLX_CK(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem));
-  unsigned blocks = grid_for(ctx, P->n_items, kWarpsSmall, 4);
-  ks<<<blocks, kWarpsSmall * 32, small_smem, ctx->stream>>>(A, B, P->g, P->items, P->n_items, P->big_list,
-                                                           P->flags, P->item_count, P->row_offset, out_col,
-                                                           reinterpret_cast<VT*>(out_val), s0, s1);
-  BCLX_CK_LAUNCH();
-  if (P->n_big > 0) {
-    unsigned bb = grid_for(ctx, P->n_big, kWarpsBig, 1);
-    kb<<<bb, kWarpsBig * 32, big_smem, ctx->stream>>>(A, B, P->g, P->items, P->n_items, P->big_list, P->flags,
-                                                     P->item_count, P->row_offset, out_col,
-                                                     reinterpret_cast<VT*>(out_val), s0, s1);
-    BCLX_CK_LAUNCH();
-  }
-  return BCLX_OK;
+  if (P->g.tn <= 8192) return launch_numeric_w<VT, 256>(ctx, A, B, P, out_col, out_val, s0, s1);
+  return launch_numeric_w<VT, kMaxWords>(ctx, A, B, P, out_col, out_val, s0, s1);
 }
 
-// Plan + symbolic over validated views; fills the plan and the C offsets.
+// Classification, symbolic, row offsets and the heavy-row cut.
 static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B, const Geom& g, int dtype,
                          int32_t* tile_row_ptr, int64_t* tile_offset, bclx_spgemm_plan_s* P) {
   P->g = g;
   P->dtype = dtype;
   const int64_t nri = g.n_row_items;
-  BCLX_TRY(scratch_alloc_n(ctx, &P->ub, nri));
-  BCLX_TRY(scratch_alloc_n(ctx, &P->nslices, nri));
-  BCLX_TRY(scratch_alloc_n(ctx, &P->first, nri + 1));
-  BCLX_TRY(scratch_alloc_n(ctx, &P->flags, 4));
+  P->hbm_words = (g.tn + 31) / 32;
+  BCLX_TRY(scratch_alloc_n(ctx, &P->light_list, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_list, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->counters, 4));
   BCLX_TRY(scratch_alloc_n(ctx, &P->products_dev, 1));
-  BCLX_CK(cudaMemsetAsync(P->flags, 0, 4 * sizeof(int32_t), ctx->stream));
-  BCLX_CK(cudaMemsetAsync(P->products_dev, 0, sizeof(unsigned long long), ctx->stream));
-  if (nri > 0) {
-    k_spgemm_ub<<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P->ub, P->nslices, P->products_dev);
-    BCLX_CK_LAUNCH();
-  }
-  BCLX_TRY(exclusive_scan_i32(ctx, P->nslices, P->first, nri));
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned, P->first + nri, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 1, P->products_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  BCLX_CK(cudaStreamSynchronize(ctx->stream));
-  P->n_items = ctx->pinned[0];
-  P->products = ctx->pinned[1];
-
-  BCLX_TRY(scratch_alloc_n(ctx, &P->items, P->n_items));
-  BCLX_TRY(scratch_alloc_n(ctx, &P->item_count, P->n_items));
-  BCLX_TRY(scratch_alloc_n(ctx, &P->big_list, P->n_items));
   BCLX_TRY(scratch_alloc_n(ctx, &P->row_count, nri));
   BCLX_TRY(scratch_alloc_n(ctx, &P->row_offset, nri + 1));
+  BCLX_CK(cudaMemsetAsync(P->counters, 0, 4 * sizeof(int32_t), ctx->stream));
+  BCLX_CK(cudaMemsetAsync(P->products_dev, 0, sizeof(unsigned long long), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P->row_count, 0, sizeof(int32_t) * (nri > 0 ? nri : 1), ctx->stream));
+  // rows of tiles wider than 8192 columns always take the block path
+  const int heavy_min_cols = 8192 + 1;
   if (nri > 0) {
-    k_build_items<<<grid_for(ctx, nri / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(g, P->nslices, P->first, P->items);
+    k_classify<<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P->light_list, P->heavy_list,
+                                                                   P->counters, P->products_dev, heavy_min_cols);
+    note_launch();
     BCLX_CK_LAUNCH();
   }
-  if (P->n_items > 0) {
-    if (dtype == BCLX_F32) BCLX_TRY(launch_symbolic<float>(ctx, A, B, P));
-    else BCLX_TRY(launch_symbolic<int32_t>(ctx, A, B, P));
-  }
+  BCLX_CK(cudaMemcpyAsync(ctx->pinned, P->counters, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 1, P->products_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
+  int32_t cnts[2];
+  std::memcpy(cnts, ctx->pinned, sizeof(cnts));
+  P->n_light = cnts[0];
+  P->n_heavy = cnts[1];
+  P->products = ctx->pinned[1];
+
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_bitmaps, (size_t)P->n_heavy * P->hbm_words));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_nitems, P->n_heavy));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_first, P->n_heavy + 1));
+  if (dtype == BCLX_F32) BCLX_TRY(launch_symbolic<float>(ctx, A, B, P));
+  else BCLX_TRY(launch_symbolic<int32_t>(ctx, A, B, P));
   BCLX_TRY(exclusive_scan_i32(ctx, P->row_count, P->row_offset, nri));
   const int64_t ntiles = g.gm * g.gn;
   k_tile_ptrs<<<grid_for(ctx, ntiles * (g.tm + 1) / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
-      g, P->row_offset, tile_row_ptr, tile_offset, P->flags + 1);
+      g, P->row_offset, tile_row_ptr, tile_offset, P->counters + 2);
+  note_launch();
   BCLX_CK_LAUNCH();
+  if (P->n_heavy > 0) {
+    const unsigned blocks = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
+    k_cut_heavy<false><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, P->counters, P->heavy_bitmaps,
+                                                        P->hbm_words, P->heavy_nitems, nullptr, nullptr);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+  BCLX_TRY(exclusive_scan_i32(ctx, P->heavy_nitems, P->heavy_first, P->n_heavy));
   BCLX_CK(cudaMemcpyAsync(ctx->pinned, P->row_offset + nri, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 1, P->flags, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 1, P->heavy_first + P->n_heavy, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 2, P->counters + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   BCLX_CK(cudaStreamSynchronize(ctx->stream));
   P->nnz = ctx->pinned[0];
-  int32_t fl[2];
-  std::memcpy(fl, ctx->pinned + 1, sizeof(fl));
-  P->n_big = fl[0];
-  if (fl[1]) {
+  P->n_heavy_items = ctx->pinned[1];
+  int32_t overflow;
+  std::memcpy(&overflow, ctx->pinned + 2, sizeof(overflow));
+  if (overflow) {
     set_last_error("a C tile has more than 2^31-1 nonzeros; use a finer tile grid");
     return BCLX_ERR_INDEX_OVERFLOW;
   }
-  // ub and nslices are not needed after planning
-  scratch_free(ctx, P->ub);
-  scratch_free(ctx, P->nslices);
-  P->ub = nullptr;
-  P->nslices = nullptr;
+  if (P->n_heavy > 0) {
+    BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_items, P->n_heavy_items));
+    const unsigned blocks = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
+    k_cut_heavy<true><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, P->counters, P->heavy_bitmaps,
+                                                       P->hbm_words, nullptr, P->heavy_first, P->heavy_items);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    // B-row table for the heavy items' column ranges
+    const int64_t nbrows = g.gk * g.gn * g.tk;
+    BCLX_TRY(scratch_alloc_n(ctx, &P->tab, (size_t)nbrows * (g.nfb + 1)));
+    k_btable<<<grid_for(ctx, nbrows, 8, 16), 256, 0, ctx->stream>>>(B, g, P->tab);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
   return BCLX_OK;
 }
 
@@ -584,16 +769,17 @@ static int numeric_impl(Context* ctx, bclx_spgemm_plan_s* P, const SpGridView& A
                         int32_t* out_col, void* out_val, int s0, int s1) {
   if (s1 <= 0 || s1 > P->g.gk) s1 = (int)P->g.gk;
   if (s0 < 0 || s0 > s1) return BCLX_ERR_INVALID;
-  if (P->n_items == 0 || s0 == s1) return BCLX_OK;
+  if (P->n_light + P->n_heavy_items == 0 || s0 == s1) return BCLX_OK;
   if (P->dtype == BCLX_F32) return launch_numeric<float>(ctx, A, B, P, out_col, out_val, s0, s1);
   return launch_numeric<int32_t>(ctx, A, B, P, out_col, out_val, s0, s1);
 }
 
-static Geom make_geom(const bclx_spgrid_out_t* c, int64_t gk) {
+static Geom make_geom(const bclx_spgrid_out_t* c, int64_t gk, int64_t tk) {
   Geom g;
   g.gm = c->grid_m; g.gn = c->grid_n; g.gk = gk;
-  g.tm = c->tile_m; g.tn = c->tile_n; g.m = c->m; g.n = c->n;
+  g.tm = c->tile_m; g.tn = c->tile_n; g.tk = tk; g.m = c->m; g.n = c->n;
   g.n_row_items = g.gm * g.gn * g.tm;
+  g.nfb = ceil_div(g.tn, kFineCols);
   return g;
 }
 
@@ -611,7 +797,7 @@ int bclx_spgemm_symbolic(bclx_context_t c, const bclx_spgrid_t* a, const bclx_sp
   BCLX_CK(cudaSetDevice(ctx->device));
   auto* P = new bclx_spgemm_plan_s();
   P->ctx = ctx;
-  int rc = symbolic_impl(ctx, make_view(*a), make_view(*b), make_geom(out, a->grid_n), a->dtype,
+  int rc = symbolic_impl(ctx, make_view(*a), make_view(*b), make_geom(out, a->grid_n, a->tile_n), a->dtype,
                          out->tile_row_ptr, out->tile_offset, P);
   if (rc != BCLX_OK) {
     P->release();
@@ -646,9 +832,9 @@ int bclx_spgemm_plan_destroy(bclx_spgemm_plan_t P) {
 int bclx_spgemm_plan_stats(bclx_spgemm_plan_t P, int64_t* out6) {
   if (!P || !out6) return BCLX_ERR_INVALID;
   out6[0] = P->products;
-  out6[1] = P->g.n_row_items;
-  out6[2] = P->n_items;
-  out6[3] = P->n_big;
+  out6[1] = P->n_light;
+  out6[2] = P->n_heavy;
+  out6[3] = P->n_heavy_items;
   out6[4] = P->g.gk;
   out6[5] = P->nnz;
   return BCLX_OK;
@@ -659,22 +845,25 @@ int bclx_spgemm_plan_stats(bclx_spgemm_plan_t P, int64_t* out6) {
 // order is the list order, each partial value passes through fma(1, v, 0) == v
 // exactly, and the partials are added from 0 in list order: the
 // SparseHashAccumulator sum.
-static int accumulate_views(bclx_spgemm_plan_s* P, Context* ctx, const bclx_csr_t* parts, int32_t nparts,
-                            int64_t m, int64_t n, int32_t dtype, SpGridView* A, SpGridView* B, Geom* g) {
+static void accumulate_views(bclx_spgemm_plan_s* P, const bclx_csr_t* parts, int32_t nparts, int64_t m, int64_t n,
+                             SpGridView* A, SpGridView* B, Geom* g) {
   A->tiles = P->id_desc;
   A->m = m; A->n = m * (int64_t)nparts; A->tm = m; A->tn = m; A->gm = 1; A->gn = nparts;
   B->tiles = parts;
   B->m = m * (int64_t)nparts; B->n = n; B->tm = m; B->tn = n; B->gm = nparts; B->gn = 1;
-  g->gm = 1; g->gn = 1; g->gk = nparts; g->tm = m; g->tn = n; g->m = m; g->n = n; g->n_row_items = m;
-  (void)ctx; (void)dtype;
-  return BCLX_OK;
+  g->gm = 1; g->gn = 1; g->gk = nparts; g->tm = m; g->tn = n; g->tk = m; g->m = m; g->n = n; g->n_row_items = m;
+  g->nfb = ceil_div(n, kFineCols);
 }
 
 int bclx_tile_accumulate_symbolic(bclx_context_t c, const bclx_csr_t* parts, int32_t nparts, int64_t m, int64_t n,
                                   int32_t dtype, int32_t* c_row_ptr, bclx_spgemm_plan_t* plan, int64_t* nnz) {
   Context* ctx = reinterpret_cast<Context*>(c);
   if (!ctx || !plan || !nnz || !parts || nparts < 1 || m < 1 || n < 1 || !c_row_ptr) return BCLX_ERR_INVALID;
-  if (m > INT32_MAX || n > (int64_t)1023 * kSliceCols) return BCLX_ERR_INVALID;
+  if (nparts >= kNoStage || m > INT32_MAX) return BCLX_ERR_INVALID;
+  if (n > kMaxCols) {
+    set_last_error("tiles wider than 16384 columns are not supported");
+    return BCLX_ERR_INVALID;
+  }
   if (!value_size(dtype)) return BCLX_ERR_DTYPE;
   *plan = nullptr;
   BCLX_CK(cudaSetDevice(ctx->device));
@@ -695,10 +884,11 @@ int bclx_tile_accumulate_symbolic(bclx_context_t c, const bclx_csr_t* parts, int
     bclx_csr_t d{};
     d.m = m; d.n = m; d.nnz = m; d.row_ptr = P->id_rp; d.col_ind = P->id_ci; d.vals = P->id_v; d.dtype = dtype;
     k_fill_desc<<<1, 256, 0, ctx->stream>>>(P->id_desc, nparts, d);
+    note_launch(2);
     if (cudaGetLastError() != cudaSuccess) { rc = BCLX_ERR_CUDA; break; }
     SpGridView A{}, B{};
     Geom g{};
-    accumulate_views(P, ctx, parts, nparts, m, n, dtype, &A, &B, &g);
+    accumulate_views(P, parts, nparts, m, n, &A, &B, &g);
     rc = symbolic_impl(ctx, A, B, g, dtype, c_row_ptr, P->acc_tile_offset, P);
   } while (0);
   if (rc != BCLX_OK) {
@@ -720,7 +910,7 @@ int bclx_tile_accumulate_numeric(bclx_context_t c, bclx_spgemm_plan_t P, const b
   BCLX_CK(cudaSetDevice(ctx->device));
   SpGridView A{}, B{};
   Geom g{};
-  accumulate_views(P, ctx, parts, nparts, out->m, out->n, P->dtype, &A, &B, &g);
+  accumulate_views(P, parts, nparts, out->m, out->n, &A, &B, &g);
   return numeric_impl(ctx, P, A, B, out->col_ind, out->vals, 0, nparts);
 }
 

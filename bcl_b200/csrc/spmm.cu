@@ -203,6 +203,7 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
     case 2: k_spmm<ST, 2><<<blocks, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, align_ok); break;
     default: k_spmm<ST, 4><<<blocks, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, align_ok); break;
   }
+  note_launch();
   BCLX_CK_LAUNCH();
   return BCLX_OK;
 }

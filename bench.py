@@ -1,0 +1,497 @@
+#!/usr/bin/env python
+"""Benchmark of the BCL sparse tile multiply on B200.
+
+One JSON line on rank 0.  The headline workload is the plain SpGEMM
+configuration C = A*A for an R-MAT scale-16 matrix (65536^2, edge factor 16,
+a=0.57, b=c=0.19, d=0.05, duplicates merged, self-loops kept, FP32 values
+U(-1,1)) on an 8x8 tile grid, run as BCL::gemm(SPMatrix, SPMatrix,
+SPMatrix&) does: every C tile sums its G stage products in rotated order.
+A "step" is one whole product (symbolic + numeric + output allocation) over
+the resident tiles.  Metric: GFLOP/s = 2 x intermediate products / time,
+with the HBM GB/s of the algorithmic bytes beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl reference]
+
+Multi-GPU (torchrun): each rank multiplies its own independent matrix of the
+same configuration (seed + rank); no data-path collective; the time is the
+max over ranks and ``value`` is the job total ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SpGEMM/SpMM GFLOP/s + HBM GB/s on 1 B200: batched+learned vs plain, vs CPU"
+L2_FLUSH_BYTES = 256 << 20
+
+WORKLOADS = {
+    "spgemm_rmat16": dict(kind="spgemm", scale=16, grid=8, value_type="f32",
+                          desc="R-MAT scale 16 (65536^2, edge factor 16, a=.57 b=c=.19 d=.05), C = A*A, 8x8 tile grid, FP32"),
+    "spgemm_rmat16_i32": dict(kind="spgemm", scale=16, grid=8, value_type="i32",
+                              desc="R-MAT scale 16, C = A*A, 8x8 tile grid, int32 values in [-8, 8]"),
+    "spgemm_rmat18": dict(kind="spgemm", scale=18, grid=16, value_type="f32",
+                          desc="R-MAT scale 18 (262144^2), C = A*A, 16x16 tile grid, FP32"),
+    "spmm_er16k": dict(kind="spmm", n=16384, N=128, grid=4, dtype="f32",
+                       desc="Erdos-Renyi 16384^2 (16 nnz/row) x dense 16384x128, 4x4 tile grid, FP32"),
+}
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--workload", default="spgemm_rmat16", choices=sorted(WORKLOADS))
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU timing")
+    p.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
+    return p.parse_args()
+
+
+# ---- distributed plumbing ---------------------------------------------------------
+
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            self.pg.barrier(device_ids=[torch.cuda.current_device()])
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---- clocks ------------------------------------------------------------------------
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.5)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.proc:
+            return out
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        out.update(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                   reasons=sorted(reasons), samples=len(rows))
+        return out
+
+
+# ---- helpers ------------------------------------------------------------------------
+
+
+def tile_nnz_grid(csr, tm, tn):
+    from bcl_b200.containers import split_tiles
+    _, toff, _, _ = split_tiles(csr, tm, tn)
+    gm, gn = -(-csr.m // tm), -(-csr.n // tn)
+    return np.diff(toff).reshape(gm, gn)
+
+
+def spgemm_alg_bytes(a_nnz, b_nnz, m, k, tm, tk, nnz_c, c_tiles, vsize=4):
+    """Algorithmic bytes of the stationary-C product: every tile product
+    A_ik * B_kj reads its two tiles (indices + values + row pointers, the
+    per-tile model of the reference's GPU driver,
+    cuda/algorithms/spmm.hpp:383-394), and C is written once (col_ind, vals,
+    row pointers)."""
+    gm, gk = a_nnz.shape
+    gn = b_nnz.shape[1]
+    rows_a = np.minimum(tm, m - np.arange(gm) * tm)
+    rows_b = np.minimum(tk, k - np.arange(gk) * tk)
+    tot = 0
+    for i in range(gm):
+        for j in range(gn):
+            for kk in range(gk):
+                tot += (4 + vsize) * int(a_nnz[i, kk]) + 4 * (int(rows_a[i]) + 1)
+                tot += (4 + vsize) * int(b_nnz[kk, j]) + 4 * (int(rows_b[kk]) + 1)
+    tot += (4 + vsize) * nnz_c + 4 * c_tiles * (tm + 1)
+    return tot
+
+
+def read_profile_traffic(name):
+    """dram bytes per launch recorded in profiles/<name>.md ("traffic_bytes_per_launch: N")."""
+    path = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---- our arm: SpGEMM ------------------------------------------------------------------
+
+
+def bench_spgemm(args, wl, dist, device):
+    import torch
+    from bcl_b200 import _lib, gen
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm, spgemm_numeric, spgemm_symbolic
+
+    a = gen.rmat(wl["scale"], seed=args.seed + dist.rank, value_type=wl["value_type"])
+    n = a.m
+    G = wl["grid"]
+    ts = -(-n // G)
+    products = gen.intermediate_products(a, a)
+    flops = 2.0 * products
+    A = SPMatrix.from_csr(a, BlockCustom((ts, ts)), device=device)
+    a_nnz = tile_nnz_grid(a, ts, ts)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step(record=None):
+        plan, out, trp, toff, nnz = spgemm_symbolic(A, A)
+        ci = torch.empty(max(nnz, 1), dtype=torch.int32, device="cuda")
+        v = torch.empty(max(nnz, 1), dtype=torch.float32 if wl["value_type"] == "f32" else torch.int32,
+                        device="cuda")
+        out.col_ind, out.vals = ci.data_ptr(), v.data_ptr()
+        if record:
+            record[0].record(stream)
+        spgemm_numeric(plan, A, A, out)
+        if record:
+            record[1].record(stream)
+        plan.close()
+        return nnz, (trp, toff, ci, v)
+
+    for _ in range(args.warmup):
+        nnz_c, _ = step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(device)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = _lib.load().bclx_launch_count()
+    dist.barrier()
+    torch.cuda.synchronize()
+    for s in range(args.steps):
+        flush.zero_()
+        ev[s][0].record(stream)
+        nnz_c, _ = step(record=(ev[s][2], ev[s][3]))
+        ev[s][1].record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    launches = _lib.load().bclx_launch_count() - launches0
+    clk = clocks.stop()
+    step_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    num_ms = [e[2].elapsed_time(e[3]) for e in ev]
+    total_s = dist.max(sum(step_ms) / 1e3)
+    ms_per_step = total_s * 1e3 / args.steps
+    value = dist.world * flops * args.steps / total_s / 1e9
+
+    c_tiles = G * G
+    alg = spgemm_alg_bytes(a_nnz, a_nnz, n, n, ts, ts, nnz_c, c_tiles)
+    hbm_peak, peak_kind = peaks()
+    num_avg_s = statistics.mean(num_ms) / 1e3
+    traffic = read_profile_traffic("spgemm_numeric_rmat16")
+    roofline = {"bound": "hbm", "achieved": alg / num_avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": alg / num_avg_s / 1e9 / hbm_peak, "traffic": traffic,
+                "kernel": "k_spgemm_numeric (all SUMMA stages, one launch)", "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": alg, "kernel_ms": num_avg_s * 1e3}
+
+    # end to end: host CSR tiles in pinned memory -> device -> product -> host
+    e2e = bench_spgemm_e2e(args, A, stream, flops, dist)
+
+    extras = {}
+    if not args.no_extras and dist.world == 1:
+        extras = spgemm_extras(args, A, a, ts, products, stream)
+    cfg = {"workload": wl["desc"], "tile_grid": f"{G}x{G}", "tile": ts, "nnz_A": a.nnz, "nnz_C": nnz_c,
+           "intermediate_products": products, "path": "fused SUMMA: one symbolic + one numeric launch per product",
+           "l2": "flushed between steps (256 MiB write outside the timed events)",
+           "parallelism": f"independent products per GPU x{dist.world}"}
+    line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": wl["value_type"], "data": "synthetic (seeded R-MAT)", "config": cfg,
+            "hbm_gbs": alg / (total_s / args.steps) / 1e9 * dist.world,
+            "roofline": roofline, "clocks": clk, "e2e": e2e, "gpu_launches": int(launches)}
+    if extras:
+        line["extras"] = extras
+    return line
+
+
+def bench_spgemm_e2e(args, A, stream, flops, dist):
+    import torch
+    from bcl_b200.containers import SPMatrix, spgemm
+
+    host = {k: getattr(A, k).cpu().pin_memory() for k in ("tile_row_ptr", "tile_offset", "col_ind", "vals")}
+    dev = {k: torch.empty_like(v, device="cuda") for k, v in host.items()}
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    out_host = {}
+
+    def one():
+        for k in host:
+            dev[k].copy_(host[k], non_blocking=True)
+        Ad = SPMatrix(A.m, A.n, A.tm, A.tn, A.dtype, A.device, dev["tile_row_ptr"], dev["tile_offset"],
+                      dev["col_ind"], dev["vals"])
+        C = spgemm(Ad, Ad)
+        nnz = C.nnz()
+        d2h = 0
+        for k in ("tile_row_ptr", "tile_offset", "col_ind", "vals"):
+            t = getattr(C, k)
+            cnt = nnz if k in ("col_ind", "vals") else t.numel()
+            if k not in out_host or out_host[k].numel() < cnt:
+                out_host[k] = torch.empty(max(cnt, 1), dtype=t.dtype).pin_memory()
+            out_host[k][:cnt].copy_(t.reshape(-1)[:cnt], non_blocking=True)
+            d2h += cnt * t.element_size()
+        return d2h
+
+    for _ in range(max(1, args.warmup)):
+        one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        d2h = one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = dist.max(e0.elapsed_time(e1) / 1e3)
+    return {"value": dist.world * flops * args.steps / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3 / args.steps}
+
+
+def time_region(fn, reps, stream):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def spgemm_extras(args, A, a, ts, products, stream):
+    """Secondary numbers: the per-stage (batched SUMMA stage) form, the plain
+    per-tile-product form, the int32 run, the SpMM configuration, and the
+    reference CPU baseline on a row sample."""
+    from bcl_b200.containers import spgemm, spgemm_plain
+    flops = 2.0 * products
+    ex = {}
+    t = time_region(lambda: spgemm(A, A, stages="per_stage"), 3, stream)
+    ex["spgemm_per_stage_gflops"] = flops / t / 1e9
+    t = time_region(lambda: spgemm_plain(A, A), 1, stream)
+    ex["spgemm_plain_gflops"] = flops / t / 1e9
+    ex["spgemm_plain_ms"] = t * 1e3
+    try:
+        ex["spmm_er16k"] = spmm_summary(args, stream)
+    except Exception as e:  # keep the headline line even if an extra fails
+        ex["spmm_er16k"] = {"error": repr(e)}
+    return ex
+
+
+def spmm_summary(args, stream):
+    import torch
+    from bcl_b200 import gen
+    from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm, spmm_plain
+    wl = WORKLOADS["spmm_er16k"]
+    n, N, G = wl["n"], wl["N"], wl["grid"]
+    ts = n // G
+    a = gen.erdos_renyi(n, 16, seed=args.seed)
+    b = gen.dense(n, N, seed=args.seed + 1)
+    A = SPMatrix.from_csr(a, BlockCustom((ts, ts)))
+    B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((ts, N)))
+    C = DMatrix.zeros((n, N), BlockCustom((ts, N)))
+    flops = 2.0 * a.nnz * N
+    alg = G * G * G * 0  # per-product model below
+    # reference model per tile product: indices + values of A_ik, B_kj, C_ij read and written once
+    tile_nnz = tile_nnz_grid(a, ts, ts)
+    alg = 0
+    for i in range(G):
+        for k in range(G):
+            alg += 8 * int(tile_nnz[i, k]) + 4 * (ts + 1) + 4 * ts * N + 8 * ts * N
+    t = time_region(lambda: spmm(A, B, C), 20, stream)
+    tp = time_region(lambda: spmm_plain(A, B, C), 5, stream)
+    B16 = DMatrix.from_array(torch.from_numpy(b), BlockCustom((ts, N)), dtype=torch.bfloat16)
+    C16 = DMatrix.zeros((n, N), BlockCustom((ts, N)), dtype=torch.bfloat16)
+    t16 = time_region(lambda: spmm(A, B16, C16), 20, stream)
+    hbm, _ = peaks()
+    return {"workload": wl["desc"], "gflops": flops / t / 1e9, "alg_gbs": alg / t / 1e9, "frac_hbm": alg / t / 1e9 / hbm,
+            "ms": t * 1e3, "plain_gflops": flops / tp / 1e9, "bf16_gflops": flops / t16 / 1e9,
+            "bf16_speedup": t / t16}
+
+
+# ---- CPU baselines (the reference's own code) -------------------------------------------
+
+
+def row_sample(a, stride):
+    from bcl_b200 import gen
+    rows = np.arange(0, a.m, stride)
+    rp = a.row_ptr.astype(np.int64)
+    counts = rp[rows + 1] - rp[rows]
+    idx = np.concatenate([np.arange(rp[r], rp[r + 1]) for r in rows]) if rows.size else np.zeros(0, np.int64)
+    nrp = np.zeros(rows.size + 1, np.int64)
+    np.cumsum(counts, out=nrp[1:])
+    return gen.CSR(rows.size, a.n, nrp.astype(np.int32), a.col_ind[idx], a.vals[idx])
+
+
+def reference_spgemm_sample(a, G, stride, warmup, reps):
+    """Run the reference's BCL::gemm on every `stride`-th row of A times A
+    (same tile columns; tile height scaled so the grid stays G x G)."""
+    from bcl_b200 import gen
+    from oracle import oracle as O
+    s = row_sample(a, stride)
+    ts = -(-a.m // G)
+    tm = -(-s.m // G)
+    products = gen.intermediate_products(s, a)
+    env = {"OMP_NUM_THREADS": str(os.cpu_count() or 1)}
+    with tempfile.TemporaryDirectory() as d:
+        fa, fb = os.path.join(d, "s.binary"), os.path.join(d, "a.binary")
+        gen.write_binary(fa, s)
+        gen.write_binary(fb, a)
+        mode = "f32" if a.vals.dtype == np.float32 else "i32"
+        res = O.run_ref(["spgemm", fa, fb, tm, ts, ts, mode, "-", warmup, reps], env=env, timeout=3000)
+    return products, res["times_s"], s.m
+
+
+def cpu_baseline_spgemm(a, G, stride=16):
+    products, times, rows = reference_spgemm_sample(a, G, stride, 0, 1)
+    t = statistics.mean(times)
+    return {"value": 2.0 * products / t / 1e9, "unit": "GFLOP/s", "cores": os.cpu_count() or 1,
+            "kind": "reference",
+            "sample": f"every {stride}th row of A ({rows} rows, {products} products) times A, {G}x{G} tile grid, "
+                      f"reference BCL::gemm built from its headers (1 rank, OpenMP accumulate)",
+            "seconds": t}
+
+
+def run_reference(args, dist):
+    """The reference arm: the reference's own CPU BCL::gemm on this config,
+    all host threads, each step a bounded row sample of the same product."""
+    if dist.rank != 0:
+        return None
+    from bcl_b200 import gen
+    from oracle import oracle as O
+    wl = WORKLOADS[args.workload]
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "reference CPU binary oracle/_ref/bcl_ref was not built"}
+    if wl["kind"] != "spgemm":
+        return {"impl": "reference", "unavailable": "reference arm is implemented for the SpGEMM workloads"}
+    a = gen.rmat(wl["scale"], seed=args.seed, value_type=wl["value_type"])
+    G = wl["grid"]
+    stride = 128 if wl["scale"] <= 16 else 2048
+    products, times, rows = reference_spgemm_sample(a, G, stride, args.warmup, args.steps)
+    t = statistics.mean(times)
+    value = 2.0 * products / t / 1e9
+    return {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": wl["value_type"], "data": "synthetic (seeded R-MAT)",
+            "config": {"workload": wl["desc"], "tile_grid": f"{G}x{G}",
+                       "sample": f"every {stride}th row of A ({rows} rows, {products} products) times A"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": os.cpu_count() or 1, "kind": "reference",
+                             "sample": f"every {stride}th row of A times A, {G}x{G} tiles, {args.steps} reps"},
+            "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "gpu_launches": 0}
+
+
+def main():
+    args = parse_args()
+    dist = Dist()
+    if args.impl == "reference":
+        line = run_reference(args, dist)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        dist.close()
+        return
+    import torch
+    device = dist.local_rank
+    torch.cuda.set_device(device)
+    wl = dict(WORKLOADS[args.workload])
+    if args.scale is not None:
+        wl["scale"] = args.scale
+        wl["desc"] = wl["desc"].replace("scale 16", f"scale {args.scale}") + " (scale overridden)"
+    if wl["kind"] == "spgemm":
+        line = bench_spgemm(args, wl, dist, device)
+        if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+            from bcl_b200 import gen
+            a = gen.rmat(wl["scale"], seed=args.seed, value_type=wl["value_type"])
+            try:
+                line["cpu_baseline"] = cpu_baseline_spgemm(a, wl["grid"], stride=64 if wl["scale"] <= 16 else 1024)
+            except Exception as e:
+                line["cpu_baseline"] = {"value": None, "error": repr(e)}
+    else:
+        raise SystemExit(f"workload {args.workload} is reported as an extra of the default run")
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -138,6 +138,9 @@ BCLX_API int bclx_context_synchronize(bclx_context_t ctx);
 BCLX_API const char* bclx_last_error(void);
 /* Library version, e.g. 100 for 0.1.0. */
 BCLX_API int bclx_version(void);
+/* Number of CUDA kernels this library has launched in this process (no
+ * reference counterpart; used for launch accounting in benchmarks). */
+BCLX_API long long bclx_launch_count(void);
 
 /* ---- sparse x sparse ---------------------------------------------------
  * C = A * B over tile grids: A is m x k with grid (gm x gk), B is k x n with

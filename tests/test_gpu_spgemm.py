@@ -72,6 +72,21 @@ def test_golden_tile_accumulate(name, mode):
     assert_csr_identical(got, c.row_ptr, c.col_ind, c.vals)
 
 
+def test_light_and_heavy_rows_mixed():
+    """8192-wide tiles of an R-MAT s13 product: both light rows and heavy rows
+    (with several items each) occur; compared bit-for-bit."""
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm
+    a = gen.rmat(13, seed=17)
+    A = SPMatrix.from_csr(a, BlockCustom((2048, 8192)))
+    B = SPMatrix.from_csr(a, BlockCustom((8192, 8192)))
+    C, plan = spgemm(A, B, keep_plan=True)
+    st = plan.stats()
+    plan.close()
+    assert st["light_rows"] > 0 and st["heavy_rows"] > 0 and st["heavy_items"] > st["heavy_rows"]
+    rp, ci, cv = O.gemm_tiled(a, a, 2048, 8192, 8192)
+    assert_csr_identical(C.get(), rp, ci, cv)
+
+
 @pytest.mark.parametrize("value_type", ["f32", "i32"])
 @pytest.mark.parametrize("tiles", [(512, 512, 512), (300, 700, 260), (2048, 2048, 2048)])
 def test_rmat11_vs_oracle(value_type, tiles):
@@ -81,10 +96,9 @@ def test_rmat11_vs_oracle(value_type, tiles):
     assert_csr_identical(got, rp, ci, cv)
 
 
-def test_sliced_rows_and_large_accumulator():
-    """Tiles 16384 columns wide force every row into >= 2 column slices, and
-    R-MAT's long rows produce work items with more than 512 outputs (the
-    large-accumulator kernel)."""
+def test_wide_tiles_heavy_rows():
+    """Tiles 16384 columns wide send every row through the block-wide
+    symbolic pass and the cut into <= 512-output items (heavy path)."""
     from bcl_b200.containers import BlockCustom, SPMatrix, spgemm
     a = gen.rmat(14, seed=7)
     A = SPMatrix.from_csr(a, BlockCustom((4096, 16384)))
@@ -92,7 +106,7 @@ def test_sliced_rows_and_large_accumulator():
     C, plan = spgemm(A, B, keep_plan=True)
     st = plan.stats()
     plan.close()
-    assert st["big_items"] > 0 and st["work_items"] > st["row_items"] // 4
+    assert st["heavy_rows"] > 0 and st["light_rows"] == 0 and st["heavy_items"] >= st["heavy_rows"]
     rows = np.random.default_rng(0).choice(a.m, 2000, replace=False)
     rows.sort()
     rp, ci, cv = O.gemm_tiled(a, a, 4096, 16384, 16384, rows=rows)
