@@ -53,6 +53,7 @@ constexpr int kWarpsSym = 8;
 constexpr int kHeavyThreads = 256;
 constexpr int kWarpsNum = 8;
 constexpr int kNoStage = 0xff;
+constexpr int kLongSeg = 24;          // B segments at least this long are walked in direct mode
 
 struct Geom {
   int64_t gm, gk, gn;   // C grid is gm x gn; the k grid has gk tiles
@@ -103,15 +104,25 @@ __device__ __forceinline__ P* shfl_ptr(P* p, int src) {
 
 // Walk the product stream of C-tile row `x` over stages [s0, s1), restricted
 // to fine blocks [fb_lo, fb_hi) of the row when RANGED (through the B-row
-// table `tab`), in the reference's order, 32 products per batch.  The batches
-// are dealt round-robin to `nparts` walkers and this one takes share `part`
-// (the numeric pass uses one share; the order-free symbolic pass of a heavy
-// row spreads the batches over the warps of a block).
-// Every lane calls f(valid, j, a, b, stage) once per batch.
-template <typename VT, bool VALUES, bool RANGED, typename F>
+// table `tab`), in the reference's order.
+//
+// The A entries of the row (all stages, flattened) are taken 32 at a time,
+// one per lane.  An entry whose B segment has at least kLongSeg products is
+// walked in "direct" mode: lanes stride over the segment and each lane calls
+// fd(j, a, b, stage) for its own products (the columns of one B row are
+// distinct, so lanes never touch the same column; a __syncwarp follows the
+// segment).  Runs of shorter entries are packed 32 products per batch and
+// every lane calls f(valid, j, a, b, stage) once per batch (warp-uniform);
+// valid lanes form a prefix of the warp and lane order is product order.
+//
+// The work is dealt round-robin to `nparts` walkers and this one takes share
+// `part` (the numeric pass uses one share; the order-free symbolic pass of a
+// heavy row spreads it over the warps of a block).
+template <typename VT, bool VALUES, bool RANGED, typename F, typename FD>
 __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridView& B, const Geom& g,
                                               const RowInfo& x, int s0, int s1, int fb_lo, int fb_hi,
-                                              const int32_t* __restrict__ tab, int part, int nparts, F&& f) {
+                                              const int32_t* __restrict__ tab, int part, int nparts, F&& f,
+                                              FD&& fd) {
   const int lane = lane_id();
   for (int g0 = s0; g0 < s1; g0 += 32) {
     // one lane per stage: its A-row segment
@@ -163,25 +174,60 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
         bcol = Bt.col_ind + bs;
         if (VALUES) bval = reinterpret_cast<const VT*>(Bt.vals) + bs;
       }
-      const int32_t incl = warp_inclusive_scan(len);
-      const int32_t total = __shfl_sync(kFull, incl, 31);
-      const int32_t excl = incl - len;
-      for (int32_t base = part * 32; base < total; base += nparts * 32) {
-        const int32_t q = base + lane;
-        const int src = warp_search(incl, q);
-        const int32_t sex = __shfl_sync(kFull, excl, src);
-        const int32_t* sbcol = shfl_ptr(bcol, src);
-        const VT* sbval = VALUES ? shfl_ptr(bval, src) : nullptr;
-        const VT a = VALUES ? __shfl_sync(kFull, av, src) : VT(0);
-        const int pstage = __shfl_sync(kFull, stage, src);
-        const bool valid = q < total;
-        int32_t j = -1;
-        VT bv = VT(0);
-        if (valid) {
-          j = __ldg(sbcol + (q - sex));
-          if (VALUES) bv = __ldg(sbval + (q - sex));
+      const int nent = min(32, atot - e0);
+      // (with several walkers a segment must be long enough to feed them all)
+      const unsigned longm = __ballot_sync(kFull, len >= kLongSeg * nparts);
+      int e_start = 0;
+      while (e_start < nent) {
+        const unsigned lm = longm & (kFull << e_start);
+        const int e_long = lm ? __ffs(lm) - 1 : nent;
+        if (e_long > e_start) {
+          // packed batches over the short entries [e_start, e_long)
+          const int32_t lenm = (lane >= e_start && lane < e_long) ? len : 0;
+          const int32_t incl = warp_inclusive_scan(lenm);
+          const int32_t total = __shfl_sync(kFull, incl, 31);
+          const int32_t excl = incl - lenm;
+          for (int32_t base = part * 32; base < total; base += nparts * 32) {
+            const int32_t q = base + lane;
+            const int src = warp_search(incl, q);
+            const int32_t sex = __shfl_sync(kFull, excl, src);
+            const int32_t* sbcol = shfl_ptr(bcol, src);
+            const VT* sbval = VALUES ? shfl_ptr(bval, src) : nullptr;
+            const VT a = VALUES ? __shfl_sync(kFull, av, src) : VT(0);
+            const int pstage = __shfl_sync(kFull, stage, src);
+            const bool valid = q < total;
+            int32_t j = -1;
+            VT bv = VT(0);
+            if (valid) {
+              j = __ldg(sbcol + (q - sex));
+              if (VALUES) bv = __ldg(sbval + (q - sex));
+            }
+            f(valid, j, a, bv, pstage);
+          }
         }
-        f(valid, j, a, bv, pstage);
+        if (e_long < nent) {
+          // direct mode over one long segment
+          const int32_t dl = __shfl_sync(kFull, len, e_long);
+          const int32_t* dcol = shfl_ptr(bcol, e_long);
+          const VT* dval = VALUES ? shfl_ptr(bval, e_long) : nullptr;
+          const VT da = VALUES ? __shfl_sync(kFull, av, e_long) : VT(0);
+          const int dst = __shfl_sync(kFull, stage, e_long);
+          const int32_t step = 32 * nparts;
+          int32_t q = lane + 32 * part;
+          for (; q + step < dl; q += 2 * step) {
+            const int32_t j0 = __ldg(dcol + q), j1 = __ldg(dcol + q + step);
+            VT b0 = VT(0), b1 = VT(0);
+            if (VALUES) {
+              b0 = __ldg(dval + q);
+              b1 = __ldg(dval + q + step);
+            }
+            fd(j0, da, b0, dst);
+            fd(j1, da, b1, dst);
+          }
+          if (q < dl) fd(__ldg(dcol + q), da, VALUES ? __ldg(dval + q) : VT(0), dst);
+          __syncwarp();
+        }
+        e_start = e_long + 1;
       }
     }
   }
@@ -190,6 +236,8 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
 // ---- planning --------------------------------------------------------------------
 
 // Per row: intermediate products; light/heavy classification into two lists.
+// One warp per row: one lane per stage reads the A-row segment, then the
+// flattened entries are read 32 at a time.
 __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restrict__ light_list,
                            int32_t* __restrict__ heavy_list, int32_t* __restrict__ counters,
                            unsigned long long* __restrict__ products, int heavy_min_cols) {
@@ -201,14 +249,31 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
     const RowInfo x = decode_row(g, ri);
     int64_t tot = 0;
     if (x.r < A.rows_of(x.ti)) {
-      for (int64_t k = 0; k < g.gk; k++) {
-        const bclx_csr_t At = A.tile(x.ti, k);
-        const int32_t a0 = __ldg(At.row_ptr + x.r), a1 = __ldg(At.row_ptr + x.r + 1);
-        if (a0 == a1) continue;
-        const bclx_csr_t Bt = B.tile(k, x.tj);
-        for (int32_t p = a0 + lane; p < a1; p += 32) {
-          const int32_t kc = __ldg(At.col_ind + p);
-          tot += __ldg(Bt.row_ptr + kc + 1) - __ldg(Bt.row_ptr + kc);
+      for (int g0 = 0; g0 < g.gk; g0 += 32) {
+        const int kk = g0 + lane;
+        int32_t as = 0, alen = 0;
+        const int32_t* acol = nullptr;
+        const int32_t* brp = nullptr;
+        if (kk < g.gk) {
+          const bclx_csr_t At = A.tile(x.ti, kk);
+          as = __ldg(At.row_ptr + x.r);
+          alen = __ldg(At.row_ptr + x.r + 1) - as;
+          acol = At.col_ind;
+          brp = B.tile(kk, x.tj).row_ptr;
+        }
+        const int32_t aincl = warp_inclusive_scan(alen);
+        const int32_t atot = __shfl_sync(kFull, aincl, 31);
+        for (int32_t e0 = 0; e0 < atot; e0 += 32) {
+          const int32_t e = e0 + lane;
+          const int sl = warp_search(aincl, e);
+          const int32_t sas = __shfl_sync(kFull, as, sl);
+          const int32_t sax = __shfl_sync(kFull, aincl - alen, sl);
+          const int32_t* sacol = shfl_ptr(acol, sl);
+          const int32_t* sbrp = shfl_ptr(brp, sl);
+          if (e < atot) {
+            const int32_t kc = __ldg(sacol + sas + (e - sax));
+            tot += __ldg(sbrp + kc + 1) - __ldg(sbrp + kc);
+          }
         }
       }
       tot = warp_sum(tot);
@@ -227,27 +292,22 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
 // B-row table: for every row of every B tile (k, j), the position of the
 // first entry in each fine column block: tab[((k*gn + j)*tk + r)*(nfb+1) + b]
 // = first entry with column >= b*kFineCols (b = nfb: the row end).
+// One thread per B row (rows of a tile are short on average).
 __global__ void k_btable(SpGridView B, Geom g, int32_t* __restrict__ tab) {
-  const int lane = lane_id();
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t nrows = g.gk * g.gn * g.tk;
-  for (int64_t x = warp; x < nrows; x += nwarps) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < nrows; x += (int64_t)gridDim.x * blockDim.x) {
     const int64_t kt = x / g.tk, r = x - kt * g.tk;
     const int64_t k = kt / g.gn, j = kt - k * g.gn;
     if (r >= B.rows_of(k)) continue;
     int32_t* trow = tab + x * (g.nfb + 1);
     const bclx_csr_t Bt = B.tile(k, j);
     const int32_t b0 = __ldg(Bt.row_ptr + r), b1 = __ldg(Bt.row_ptr + r + 1);
-    // entry q (or the row end) starts every block in (block(col[q-1]), block(col[q])]
-    for (int32_t q0 = b0; q0 <= b1; q0 += 32) {
-      const int32_t q = q0 + lane;
-      if (q <= b1) {
-        const int cur = q < b1 ? __ldg(Bt.col_ind + q) / kFineCols : (int)g.nfb;
-        const int prev = q > b0 ? __ldg(Bt.col_ind + q - 1) / kFineCols : -1;
-        for (int b = prev + 1; b <= cur && b <= g.nfb; b++) trow[b] = q;
-      }
+    int b = 0;
+    for (int32_t q = b0; q < b1; q++) {
+      const int blk = __ldg(Bt.col_ind + q) / kFineCols;
+      while (b <= blk) trow[b++] = q;
     }
+    while (b <= g.nfb) trow[b++] = b1;
   }
 }
 
@@ -269,10 +329,12 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
     const int words = (x.w + 31) >> 5;
     for (int w = lane; w < words; w += 32) bm[w] = 0u;
     __syncwarp();
-    walk_products<VT, false, false>(A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, 0, 1,
-                                    [&](bool valid, int32_t j, VT, VT, int) {
-                                      if (valid) atomicOr(&bm[j >> 5], 1u << (j & 31));
-                                    });
+    walk_products<VT, false, false>(
+        A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, 0, 1,
+        [&](bool valid, int32_t j, VT, VT, int) {
+          if (valid) atomicOr(&bm[j >> 5], 1u << (j & 31));
+        },
+        [&](int32_t j, VT, VT, int) { atomicOr(&bm[j >> 5], 1u << (j & 31)); });
     __syncwarp();
     int cnt = 0;
     for (int w = lane; w < words; w += 32) cnt += __popc(bm[w]);
@@ -300,10 +362,12 @@ __global__ void __launch_bounds__(kHeavyThreads)
     const int words = (x.w + 31) >> 5;
     for (int w = threadIdx.x; w < words; w += kHeavyThreads) hbm_smem[w] = 0u;
     __syncthreads();
-    walk_products<VT, false, false>(A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, wid, nw,
-                                    [&](bool valid, int32_t j, VT, VT, int) {
-                                      if (valid) atomicOr(&hbm_smem[j >> 5], 1u << (j & 31));
-                                    });
+    walk_products<VT, false, false>(
+        A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, wid, nw,
+        [&](bool valid, int32_t j, VT, VT, int) {
+          if (valid) atomicOr(&hbm_smem[j >> 5], 1u << (j & 31));
+        },
+        [&](int32_t j, VT, VT, int) { atomicOr(&hbm_smem[j >> 5], 1u << (j & 31)); });
     __syncthreads();
     int cnt = 0;
     uint32_t* out = heavy_bitmaps + h * hbm_words;
@@ -452,10 +516,12 @@ __global__ void __launch_bounds__(kWarpsNum * 32)
       for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
       __syncwarp();
       if (s0 == 0) {
-        walk_products<VT, false, false>(A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, 0, 1,
-                                        [&](bool valid, int32_t j, VT, VT, int) {
-                                          if (valid) atomicOr(&S.bm[j >> 5], 1u << (j & 31));
-                                        });
+        walk_products<VT, false, false>(
+            A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, 0, 1,
+            [&](bool valid, int32_t j, VT, VT, int) {
+              if (valid) atomicOr(&S.bm[j >> 5], 1u << (j & 31));
+            },
+            [&](int32_t j, VT, VT, int) { atomicOr(&S.bm[j >> 5], 1u << (j & 31)); });
       } else {
         for (int q = lane; q < cnt; q += 32) {
           const int j = out_col[off + q];
@@ -532,10 +598,23 @@ __global__ void __launch_bounds__(kWarpsNum * 32)
       }
       __syncwarp();
     };
+    // direct mode: the lanes hold distinct columns, each updates its own
+    auto update_direct = [&](int32_t j, VT a, VT b, int stage) {
+      const int xx = j - lo;
+      const int rank = S.pre[xx >> 5] + __popc(S.bm[xx >> 5] & ((1u << (xx & 31)) - 1u));
+      VT v = S.part[rank];
+      const int t = S.tag[rank];
+      if (t != stage) {
+        if (t != kNoStage) S.acc[rank] = vadd(S.acc[rank], v);
+        v = VT(0);
+        S.tag[rank] = (unsigned char)stage;
+      }
+      S.part[rank] = madd(a, b, v);
+    };
     if (heavy)
-      walk_products<VT, true, true>(A, B, g, x, s0, s1, fb_lo, fb_hi, tab, 0, 1, update);
+      walk_products<VT, true, true>(A, B, g, x, s0, s1, fb_lo, fb_hi, tab, 0, 1, update, update_direct);
     else
-      walk_products<VT, true, false>(A, B, g, x, s0, s1, 0, 0, nullptr, 0, 1, update);
+      walk_products<VT, true, false>(A, B, g, x, s0, s1, 0, 0, nullptr, 0, 1, update, update_direct);
 
     // 5. last fold and values out
     for (int q = lane; q < cnt; q += 32) {
@@ -758,7 +837,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     // B-row table for the heavy items' column ranges
     const int64_t nbrows = g.gk * g.gn * g.tk;
     BCLX_TRY(scratch_alloc_n(ctx, &P->tab, (size_t)nbrows * (g.nfb + 1)));
-    k_btable<<<grid_for(ctx, nbrows, 8, 16), 256, 0, ctx->stream>>>(B, g, P->tab);
+    k_btable<<<grid_for(ctx, nbrows / 32 + 1, 8, 16), 256, 0, ctx->stream>>>(B, g, P->tab);
     note_launch();
     BCLX_CK_LAUNCH();
   }

@@ -215,18 +215,30 @@ def bench_spgemm(args, wl, dist, device):
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
+    host_t = {"symbolic": 0.0, "alloc": 0.0, "numeric": 0.0, "close": 0.0}
+
     def step(record=None):
+        t0 = time.perf_counter()
         plan, out, trp, toff, nnz = spgemm_symbolic(A, A)
+        t1 = time.perf_counter()
         ci = torch.empty(max(nnz, 1), dtype=torch.int32, device="cuda")
         v = torch.empty(max(nnz, 1), dtype=torch.float32 if wl["value_type"] == "f32" else torch.int32,
                         device="cuda")
         out.col_ind, out.vals = ci.data_ptr(), v.data_ptr()
+        t2 = time.perf_counter()
         if record:
             record[0].record(stream)
         spgemm_numeric(plan, A, A, out)
         if record:
             record[1].record(stream)
+        t3 = time.perf_counter()
         plan.close()
+        t4 = time.perf_counter()
+        if record:
+            host_t["symbolic"] += t1 - t0
+            host_t["alloc"] += t2 - t1
+            host_t["numeric"] += t3 - t2
+            host_t["close"] += t4 - t3
         return nnz, (trp, toff, ci, v)
 
     for _ in range(args.warmup):
@@ -278,7 +290,9 @@ def bench_spgemm(args, wl, dist, device):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": wl["value_type"], "data": "synthetic (seeded R-MAT)", "config": cfg,
             "hbm_gbs": alg / (total_s / args.steps) / 1e9 * dist.world,
-            "roofline": roofline, "clocks": clk, "e2e": e2e, "gpu_launches": int(launches)}
+            "roofline": roofline, "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
+            "host_ms_per_step": {k: v * 1e3 / args.steps for k, v in host_t.items()},
+            "step_ms": step_ms}
     if extras:
         line["extras"] = extras
     return line
