@@ -50,10 +50,13 @@ constexpr int kFineCols = 256;       // column block of heavy rows and of the B-
 constexpr int kMaxWords = 512;       // bitmap words per warp (tiles up to 16384 columns)
 constexpr int kMaxCols = kMaxWords * 32;
 constexpr int kWarpsSym = 8;
-constexpr int kHeavyThreads = 256;
 constexpr int kWarpsNum = 8;
 constexpr int kNoStage = 0xff;
-constexpr int kLongSeg = 24;          // B segments at least this long are walked in direct mode
+#ifndef BCLX_LONG_SEG
+#define BCLX_LONG_SEG 48
+#endif
+constexpr int kLongSeg = BCLX_LONG_SEG;  // B segments at least this long are walked in direct mode
+constexpr int64_t kVeryHeavyUb = 32768;  // rows above this many products get a whole block in the symbolic pass
 
 struct Geom {
   int64_t gm, gk, gn;   // C grid is gm x gn; the k grid has gk tiles
@@ -106,38 +109,42 @@ __device__ __forceinline__ P* shfl_ptr(P* p, int src) {
 // to fine blocks [fb_lo, fb_hi) of the row when RANGED (through the B-row
 // table `tab`), in the reference's order.
 //
-// The A entries of the row (all stages, flattened) are taken 32 at a time,
-// one per lane.  An entry whose B segment has at least kLongSeg products is
-// walked in "direct" mode: lanes stride over the segment and each lane calls
-// fd(j, a, b, stage) for its own products (the columns of one B row are
-// distinct, so lanes never touch the same column; a __syncwarp follows the
-// segment).  Runs of shorter entries are packed 32 products per batch and
-// every lane calls f(valid, j, a, b, stage) once per batch (warp-uniform);
-// valid lanes form a prefix of the warp and lane order is product order.
-//
-// The work is dealt round-robin to `nparts` walkers and this one takes share
-// `part` (the numeric pass uses one share; the order-free symbolic pass of a
-// heavy row spreads it over the warps of a block).
-template <typename VT, bool VALUES, bool RANGED, typename F, typename FD>
+// One lane per stage first reads that stage's A-row segment and B-tile
+// pointers.  The A entries of the row (all stages, flattened) are then taken
+// 32 at a time, one per lane, each finding its B segment.  An entry whose B
+// segment has at least kLongSeg products is walked in "direct" mode: lanes
+// stride over the segment and each lane calls fd(j, a, b, stage) for its own
+// products (the columns of one B row are distinct, so lanes never touch the
+// same column; a __syncwarp follows the segment).  Runs of shorter entries
+// are packed 32 products per batch and every lane calls f(valid, j, a, b,
+// stage) once per batch (warp-uniform); valid lanes form a prefix of the warp
+// and lane order is product order.  The loads of batch n+1 are issued before
+// f runs on batch n.
+template <typename VT, bool RANGED, typename F, typename FD>
 __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridView& B, const Geom& g,
                                               const RowInfo& x, int s0, int s1, int fb_lo, int fb_hi,
-                                              const int32_t* __restrict__ tab, int part, int nparts, F&& f,
-                                              FD&& fd) {
+                                              const int32_t* __restrict__ tab, F&& f, FD&& fd) {
   const int lane = lane_id();
   for (int g0 = s0; g0 < s1; g0 += 32) {
-    // one lane per stage: its A-row segment
+    // one lane per stage: its A-row segment and its B tile
     const int kk = g0 + lane;
-    const bool sv = kk < s1;
-    const int64_t k = sv ? (kk + x.ti + x.tj) % g.gk : 0;
     int32_t as = 0, alen = 0;
     const int32_t* acol = nullptr;
     const VT* aval = nullptr;
-    if (sv) {
+    const int32_t* brow = nullptr;  // B row_ptr, or the stage's table block when RANGED
+    const int32_t* bci = nullptr;
+    const VT* bva = nullptr;
+    if (kk < s1) {
+      const int64_t k = (kk + x.ti + x.tj) % g.gk;
       const bclx_csr_t At = A.tile(x.ti, k);
       as = __ldg(At.row_ptr + x.r);
       alen = __ldg(At.row_ptr + x.r + 1) - as;
-      acol = At.col_ind;
-      aval = reinterpret_cast<const VT*>(At.vals);
+      acol = At.col_ind + as;
+      aval = reinterpret_cast<const VT*>(At.vals) + as;
+      const bclx_csr_t Bt = B.tile(k, x.tj);
+      brow = RANGED ? tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1) : Bt.row_ptr;
+      bci = Bt.col_ind;
+      bva = reinterpret_cast<const VT*>(Bt.vals);
     }
     const int32_t aincl = warp_inclusive_scan(alen);
     const int32_t atot = __shfl_sync(kFull, aincl, 31);
@@ -146,88 +153,156 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
       // one lane per A entry of the flattened stage stream
       const int32_t e = e0 + lane;
       const int sl = warp_search(aincl, e);
-      const int64_t sk = __shfl_sync(kFull, k, sl);
-      const int32_t sas = __shfl_sync(kFull, as, sl);
-      const int32_t sax = __shfl_sync(kFull, aexcl, sl);
+      const int32_t off = e - __shfl_sync(kFull, aexcl, sl);
       const int32_t* sacol = shfl_ptr(acol, sl);
-      const VT* saval = VALUES ? shfl_ptr(aval, sl) : nullptr;
+      const VT* saval = shfl_ptr(aval, sl);
+      const int32_t* sbrow = shfl_ptr(brow, sl);
+      const int32_t* sbci = shfl_ptr(bci, sl);
+      const VT* sbva = shfl_ptr(bva, sl);
       const int stage = g0 + sl;
       int32_t len = 0;
       VT av = VT(0);
       const int32_t* bcol = nullptr;
       const VT* bval = nullptr;
       if (e < atot) {
-        const int32_t p = sas + (e - sax);
-        const int32_t kc = __ldg(sacol + p);
-        if (VALUES) av = __ldg(saval + p);
-        const bclx_csr_t Bt = B.tile(sk, x.tj);
+        const int32_t kc = __ldg(sacol + off);
+        av = __ldg(saval + off);
         int32_t bs, be;
         if (RANGED) {
-          const int32_t* trow = tab + ((sk * g.gn + x.tj) * g.tk + kc) * (g.nfb + 1);
+          const int32_t* trow = sbrow + (int64_t)kc * (g.nfb + 1);
           bs = __ldg(trow + fb_lo);
           be = __ldg(trow + fb_hi);
         } else {
-          bs = __ldg(Bt.row_ptr + kc);
-          be = __ldg(Bt.row_ptr + kc + 1);
+          bs = __ldg(sbrow + kc);
+          be = __ldg(sbrow + kc + 1);
         }
         len = be - bs;
-        bcol = Bt.col_ind + bs;
-        if (VALUES) bval = reinterpret_cast<const VT*>(Bt.vals) + bs;
+        bcol = sbci + bs;
+        bval = sbva + bs;
       }
       const int nent = min(32, atot - e0);
-      // (with several walkers a segment must be long enough to feed them all)
-      const unsigned longm = __ballot_sync(kFull, len >= kLongSeg * nparts);
+      const unsigned longm = __ballot_sync(kFull, len >= kLongSeg);
       int e_start = 0;
       while (e_start < nent) {
         const unsigned lm = longm & (kFull << e_start);
         const int e_long = lm ? __ffs(lm) - 1 : nent;
         if (e_long > e_start) {
-          // packed batches over the short entries [e_start, e_long)
+          // packed batches over the short entries [e_start, e_long), software pipelined
           const int32_t lenm = (lane >= e_start && lane < e_long) ? len : 0;
           const int32_t incl = warp_inclusive_scan(lenm);
           const int32_t total = __shfl_sync(kFull, incl, 31);
           const int32_t excl = incl - lenm;
-          for (int32_t base = part * 32; base < total; base += nparts * 32) {
+          int32_t nj = -1;
+          VT na = VT(0), nb = VT(0);
+          int nst = 0;
+          auto fetch = [&](int32_t base) {
             const int32_t q = base + lane;
             const int src = warp_search(incl, q);
-            const int32_t sex = __shfl_sync(kFull, excl, src);
+            const int32_t pos = q - __shfl_sync(kFull, excl, src);
             const int32_t* sbcol = shfl_ptr(bcol, src);
-            const VT* sbval = VALUES ? shfl_ptr(bval, src) : nullptr;
-            const VT a = VALUES ? __shfl_sync(kFull, av, src) : VT(0);
-            const int pstage = __shfl_sync(kFull, stage, src);
-            const bool valid = q < total;
-            int32_t j = -1;
-            VT bv = VT(0);
-            if (valid) {
-              j = __ldg(sbcol + (q - sex));
-              if (VALUES) bv = __ldg(sbval + (q - sex));
+            const VT* sbval = shfl_ptr(bval, src);
+            na = __shfl_sync(kFull, av, src);
+            nst = __shfl_sync(kFull, stage, src);
+            nj = -1;
+            nb = VT(0);
+            if (q < total) {
+              nj = __ldg(sbcol + pos);
+              nb = __ldg(sbval + pos);
             }
-            f(valid, j, a, bv, pstage);
+          };
+          if (total > 0) fetch(0);
+          for (int32_t base = 0; base < total; base += 32) {
+            const int32_t j = nj;
+            const VT a = na, b = nb;
+            const int st = nst;
+            if (base + 32 < total) fetch(base + 32);
+            f(j >= 0, j, a, b, st);
           }
         }
         if (e_long < nent) {
           // direct mode over one long segment
           const int32_t dl = __shfl_sync(kFull, len, e_long);
           const int32_t* dcol = shfl_ptr(bcol, e_long);
-          const VT* dval = VALUES ? shfl_ptr(bval, e_long) : nullptr;
-          const VT da = VALUES ? __shfl_sync(kFull, av, e_long) : VT(0);
+          const VT* dval = shfl_ptr(bval, e_long);
+          const VT da = __shfl_sync(kFull, av, e_long);
           const int dst = __shfl_sync(kFull, stage, e_long);
-          const int32_t step = 32 * nparts;
-          int32_t q = lane + 32 * part;
-          for (; q + step < dl; q += 2 * step) {
-            const int32_t j0 = __ldg(dcol + q), j1 = __ldg(dcol + q + step);
-            VT b0 = VT(0), b1 = VT(0);
-            if (VALUES) {
-              b0 = __ldg(dval + q);
-              b1 = __ldg(dval + q + step);
-            }
+          int32_t q = lane;
+          for (; q + 32 < dl; q += 64) {
+            const int32_t j0 = __ldg(dcol + q), j1 = __ldg(dcol + q + 32);
+            const VT b0 = __ldg(dval + q), b1 = __ldg(dval + q + 32);
             fd(j0, da, b0, dst);
             fd(j1, da, b1, dst);
           }
-          if (q < dl) fd(__ldg(dcol + q), da, VALUES ? __ldg(dval + q) : VT(0), dst);
+          if (q < dl) fd(__ldg(dcol + q), da, __ldg(dval + q), dst);
           __syncwarp();
         }
         e_start = e_long + 1;
+      }
+    }
+  }
+}
+
+// Order-free walk for the symbolic pass: calls fs(j) for every product
+// column of C-tile row `x` (all stages).  Short B segments are looped over by
+// their own lane, long ones by the whole warp.  With nparts walkers (the warps
+// of a block) each takes every nparts-th chunk of short segments and an
+// interleaved share of every long segment.
+template <typename FS>
+__device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridView& B, const Geom& g,
+                                             const RowInfo& x, int part, int nparts, FS&& fs) {
+  const int lane = lane_id();
+  for (int g0 = 0; g0 < g.gk; g0 += 32) {
+    const int kk = g0 + lane;
+    int32_t as = 0, alen = 0;
+    const int32_t* acol = nullptr;
+    const int32_t* brp = nullptr;
+    const int32_t* bci = nullptr;
+    if (kk < g.gk) {
+      const bclx_csr_t At = A.tile(x.ti, kk);
+      as = __ldg(At.row_ptr + x.r);
+      alen = __ldg(At.row_ptr + x.r + 1) - as;
+      acol = At.col_ind;
+      const bclx_csr_t Bt = B.tile(kk, x.tj);
+      brp = Bt.row_ptr;
+      bci = Bt.col_ind;
+    }
+    const int32_t aincl = warp_inclusive_scan(alen);
+    const int32_t atot = __shfl_sync(kFull, aincl, 31);
+    const int32_t aexcl = aincl - alen;
+    for (int32_t e0 = 0, chunk = 0; e0 < atot; e0 += 32, chunk++) {
+      const int32_t e = e0 + lane;
+      const int sl = warp_search(aincl, e);
+      const int32_t sas = __shfl_sync(kFull, as, sl);
+      const int32_t sax = __shfl_sync(kFull, aexcl, sl);
+      const int32_t* sacol = shfl_ptr(acol, sl);
+      const int32_t* sbrp = shfl_ptr(brp, sl);
+      const int32_t* sbci = shfl_ptr(bci, sl);
+      int32_t bs = 0, be = 0;
+      if (e < atot) {
+        const int32_t kc = __ldg(sacol + sas + (e - sax));
+        bs = __ldg(sbrp + kc);
+        be = __ldg(sbrp + kc + 1);
+      }
+      const bool lng = be - bs >= 32;
+      if (!lng && chunk % nparts == part)
+        for (int32_t q = bs; q < be; q++) fs(__ldg(sbci + q));
+      unsigned longm = __ballot_sync(kFull, lng);
+      while (longm) {
+        const int src = __ffs(longm) - 1;
+        longm &= longm - 1;
+        const int32_t lb = __shfl_sync(kFull, bs, src), le = __shfl_sync(kFull, be, src);
+        const int32_t* lci = shfl_ptr(sbci, src);
+        const int32_t step = 32 * nparts;
+        int32_t q = lb + lane + 32 * part;
+        for (; q + 3 * step < le; q += 4 * step) {
+          const int32_t j0 = __ldg(lci + q), j1 = __ldg(lci + q + step);
+          const int32_t j2 = __ldg(lci + q + 2 * step), j3 = __ldg(lci + q + 3 * step);
+          fs(j0);
+          fs(j1);
+          fs(j2);
+          fs(j3);
+        }
+        for (; q < le; q += step) fs(__ldg(lci + q));
       }
     }
   }
@@ -239,8 +314,9 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
 // One warp per row: one lane per stage reads the A-row segment, then the
 // flattened entries are read 32 at a time.
 __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restrict__ light_list,
-                           int32_t* __restrict__ heavy_list, int32_t* __restrict__ counters,
-                           unsigned long long* __restrict__ products, int heavy_min_cols) {
+                           int32_t* __restrict__ heavy_list, int32_t* __restrict__ vheavy_list,
+                           int32_t* __restrict__ counters, unsigned long long* __restrict__ products,
+                           int heavy_min_cols) {
   const int lane = lane_id();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -282,8 +358,10 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
       mine += (unsigned long long)tot;
       if (tot <= kLightUb && x.w < heavy_min_cols)
         light_list[atomicAdd(&counters[0], 1)] = (int32_t)ri;
-      else
+      else if (tot <= kVeryHeavyUb)
         heavy_list[atomicAdd(&counters[1], 1)] = (int32_t)ri;
+      else
+        vheavy_list[atomicAdd(&counters[3], 1)] = (int32_t)ri;
     }
   }
   if (lane == 0 && mine) atomicAdd(products, mine);
@@ -313,66 +391,62 @@ __global__ void k_btable(SpGridView B, Geom g, int32_t* __restrict__ tab) {
 
 // ---- symbolic ----------------------------------------------------------------------
 
-template <typename VT>
+// Symbolic pass.  Heavy rows are numbered 0..n_heavy-1 (the very heavy ones
+// first); a row's column bitmap is built in shared memory, its popcount is
+// the row's output count, and heavy rows also store the bitmap for the
+// numeric pass (hbm_words words per row).
+//
+// One warp per row for the light and ordinary heavy rows (heavy first) ...
 __global__ void __launch_bounds__(kWarpsSym * 32)
-    k_symbolic_light(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
-                     const int32_t* __restrict__ counters, int32_t* __restrict__ row_count) {
+    k_symbolic(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
+               const int32_t* __restrict__ heavy_list, int n_light, int n_heavy, int n_vheavy,
+               int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words) {
   __shared__ uint32_t bm_all[kWarpsSym][kMaxWords];
   uint32_t* bm = bm_all[threadIdx.x >> 5];
   const int lane = lane_id();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int n_light = counters[0];
-  for (int64_t idx = warp; idx < n_light; idx += nwarps) {
-    const int64_t ri = light_list[idx];
+  for (int64_t idx = n_vheavy + warp; idx < (int64_t)n_light + n_heavy; idx += nwarps) {
+    const bool heavy = idx < n_heavy;
+    const int64_t ri = heavy ? heavy_list[idx] : light_list[idx - n_heavy];
     const RowInfo x = decode_row(g, ri);
     const int words = (x.w + 31) >> 5;
     for (int w = lane; w < words; w += 32) bm[w] = 0u;
     __syncwarp();
-    walk_products<VT, false, false>(
-        A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, 0, 1,
-        [&](bool valid, int32_t j, VT, VT, int) {
-          if (valid) atomicOr(&bm[j >> 5], 1u << (j & 31));
-        },
-        [&](int32_t j, VT, VT, int) { atomicOr(&bm[j >> 5], 1u << (j & 31)); });
+    walk_columns(A, B, g, x, 0, 1, [&](int32_t j) { atomicOr(&bm[j >> 5], 1u << (j & 31)); });
     __syncwarp();
     int cnt = 0;
-    for (int w = lane; w < words; w += 32) cnt += __popc(bm[w]);
+    uint32_t* out = heavy ? heavy_bitmaps + idx * hbm_words : nullptr;
+    for (int w = lane; w < words; w += 32) {
+      const uint32_t v = bm[w];
+      if (heavy) out[w] = v;
+      cnt += __popc(v);
+    }
     cnt = warp_sum(cnt);
     if (lane == 0) row_count[ri] = cnt;
     __syncwarp();
   }
 }
 
-// One block per heavy row: all warps set bits of the row's bitmap in shared
-// memory (bit order does not matter), then the bitmap is stored for the
-// numeric pass.  hbm_words = words per stored bitmap.
-template <typename VT>
-__global__ void __launch_bounds__(kHeavyThreads)
-    k_symbolic_heavy(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ heavy_list,
-                     const int32_t* __restrict__ counters, int32_t* __restrict__ row_count,
-                     uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words) {
-  extern __shared__ uint32_t hbm_smem[];  // hbm_words
-  __shared__ int red[kHeavyThreads / 32];
-  const int n_heavy = counters[1];
-  const int wid = threadIdx.x >> 5, nw = kHeavyThreads / 32;
-  for (int64_t h = blockIdx.x; h < n_heavy; h += gridDim.x) {
+// ... and one block per very heavy row, its warps sharing the bitmap.
+__global__ void __launch_bounds__(kWarpsSym * 32)
+    k_symbolic_block(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ heavy_list, int n_vheavy,
+                     int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words) {
+  __shared__ uint32_t bm[kMaxWords];
+  __shared__ int red[kWarpsSym];
+  const int wid = threadIdx.x >> 5;
+  for (int64_t h = blockIdx.x; h < n_vheavy; h += gridDim.x) {
     const int64_t ri = heavy_list[h];
     const RowInfo x = decode_row(g, ri);
     const int words = (x.w + 31) >> 5;
-    for (int w = threadIdx.x; w < words; w += kHeavyThreads) hbm_smem[w] = 0u;
+    for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
     __syncthreads();
-    walk_products<VT, false, false>(
-        A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, wid, nw,
-        [&](bool valid, int32_t j, VT, VT, int) {
-          if (valid) atomicOr(&hbm_smem[j >> 5], 1u << (j & 31));
-        },
-        [&](int32_t j, VT, VT, int) { atomicOr(&hbm_smem[j >> 5], 1u << (j & 31)); });
+    walk_columns(A, B, g, x, wid, kWarpsSym, [&](int32_t j) { atomicOr(&bm[j >> 5], 1u << (j & 31)); });
     __syncthreads();
     int cnt = 0;
     uint32_t* out = heavy_bitmaps + h * hbm_words;
-    for (int w = threadIdx.x; w < words; w += kHeavyThreads) {
-      const uint32_t v = hbm_smem[w];
+    for (int w = threadIdx.x; w < words; w += blockDim.x) {
+      const uint32_t v = bm[w];
       out[w] = v;
       cnt += __popc(v);
     }
@@ -381,7 +455,7 @@ __global__ void __launch_bounds__(kHeavyThreads)
     __syncthreads();
     if (threadIdx.x == 0) {
       int t = 0;
-      for (int q = 0; q < nw; q++) t += red[q];
+      for (int q = 0; q < kWarpsSym; q++) t += red[q];
       row_count[ri] = t;
     }
     __syncthreads();
@@ -416,11 +490,10 @@ struct HeavyItem {
 };
 
 template <bool FILL>
-__global__ void k_cut_heavy(Geom g, const int32_t* __restrict__ heavy_list, const int32_t* __restrict__ counters,
+__global__ void k_cut_heavy(Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
                             const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
                             int32_t* __restrict__ n_items, const int64_t* __restrict__ first,
                             HeavyItem* __restrict__ items) {
-  const int n_heavy = counters[1];
   for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n_heavy; h += (int64_t)gridDim.x * blockDim.x) {
     const RowInfo x = decode_row(g, heavy_list[h]);
     const int nfb = (x.w + kFineCols - 1) / kFineCols;
@@ -464,10 +537,13 @@ struct WarpSmem {
 };
 
 template <typename VT, int WORDS>
-__global__ void __launch_bounds__(kWarpsNum * 32)
+#ifndef BCLX_NUMERIC_MIN_BLOCKS
+#define BCLX_NUMERIC_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     k_numeric(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
-              const int32_t* __restrict__ heavy_list, const int32_t* __restrict__ counters,
-              const HeavyItem* __restrict__ heavy_items, const int64_t* __restrict__ heavy_first,
+              const int32_t* __restrict__ heavy_list, int n_light, int64_t n_heavy_items,
+              const HeavyItem* __restrict__ heavy_items,
               const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, const int32_t* __restrict__ tab,
               const int32_t* __restrict__ row_count, const int64_t* __restrict__ row_offset,
               int32_t* __restrict__ out_col, VT* __restrict__ out_val, int s0, int s1) {
@@ -476,8 +552,6 @@ __global__ void __launch_bounds__(kWarpsNum * 32)
   const int lane = lane_id();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int n_light = counters[0];
-  const int64_t n_heavy_items = heavy_first[counters[1]];
   const int64_t n_total = n_heavy_items + n_light;
   for (int64_t idx = warp; idx < n_total; idx += nwarps) {
     // heavy items first (they are the larger ones)
@@ -516,12 +590,7 @@ __global__ void __launch_bounds__(kWarpsNum * 32)
       for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
       __syncwarp();
       if (s0 == 0) {
-        walk_products<VT, false, false>(
-            A, B, g, x, 0, (int)g.gk, 0, 0, nullptr, 0, 1,
-            [&](bool valid, int32_t j, VT, VT, int) {
-              if (valid) atomicOr(&S.bm[j >> 5], 1u << (j & 31));
-            },
-            [&](int32_t j, VT, VT, int) { atomicOr(&S.bm[j >> 5], 1u << (j & 31)); });
+        walk_columns(A, B, g, x, 0, 1, [&](int32_t j) { atomicOr(&S.bm[j >> 5], 1u << (j & 31)); });
       } else {
         for (int q = lane; q < cnt; q += 32) {
           const int j = out_col[off + q];
@@ -572,11 +641,24 @@ __global__ void __launch_bounds__(kWarpsNum * 32)
         rank = S.pre[xx >> 5] + __popc(S.bm[xx >> 5] & ((1u << (xx & 31)) - 1u));
       }
       const unsigned peers = __match_any_sync(kFull, valid ? j : -1);
-      S.sa[lane] = a;
-      S.sb[lane] = b;
-      S.ss[lane] = stage;
-      __syncwarp();
-      if (valid && lane == __ffs(peers) - 1) {
+      const bool single = peers == (1u << lane);
+      if (__any_sync(kFull, valid && !single)) {
+        S.sa[lane] = a;
+        S.sb[lane] = b;
+        S.ss[lane] = stage;
+        __syncwarp();
+      }
+      if (valid && single) {
+        // the only product of its column in this batch
+        VT v = S.part[rank];
+        const int t = S.tag[rank];
+        if (t != stage) {
+          if (t != kNoStage) S.acc[rank] = vadd(S.acc[rank], v);
+          v = VT(0);
+          S.tag[rank] = (unsigned char)stage;
+        }
+        S.part[rank] = madd(a, b, v);
+      } else if (valid && lane == __ffs(peers) - 1) {
         VT v = S.part[rank];
         int t = S.tag[rank];
         VT ac = S.acc[rank];
@@ -612,9 +694,9 @@ __global__ void __launch_bounds__(kWarpsNum * 32)
       S.part[rank] = madd(a, b, v);
     };
     if (heavy)
-      walk_products<VT, true, true>(A, B, g, x, s0, s1, fb_lo, fb_hi, tab, 0, 1, update, update_direct);
+      walk_products<VT, true>(A, B, g, x, s0, s1, fb_lo, fb_hi, tab, update, update_direct);
     else
-      walk_products<VT, true, false>(A, B, g, x, s0, s1, 0, 0, nullptr, 0, 1, update, update_direct);
+      walk_products<VT, false>(A, B, g, x, s0, s1, 0, 0, nullptr, update, update_direct);
 
     // 5. last fold and values out
     for (int q = lane; q < cnt; q += 32) {
@@ -651,11 +733,13 @@ struct bclx_spgemm_plan_s {
   Context* ctx = nullptr;
   Geom g{};
   int dtype = BCLX_F32;
-  int64_t products = 0, nnz = 0, n_light = 0, n_heavy = 0, n_heavy_items = 0;
+  int64_t products = 0, nnz = 0, n_light = 0, n_heavy = 0, n_vheavy = 0, n_heavy_items = 0;
   int64_t hbm_words = 0;
   int32_t* light_list = nullptr;
-  int32_t* heavy_list = nullptr;
-  int32_t* counters = nullptr;  // [0] light rows, [1] heavy rows, [2] overflow flag
+  int32_t* heavy_list = nullptr;   // very heavy rows first, then the other heavy rows
+  int32_t* vheavy_list = nullptr;
+  int32_t* heavy_tmp = nullptr;
+  int32_t* counters = nullptr;  // [0] light rows, [1] heavy rows (total after planning), [2] overflow, [3] very heavy
   unsigned long long* products_dev = nullptr;
   int32_t* row_count = nullptr;
   int64_t* row_offset = nullptr;
@@ -672,10 +756,10 @@ struct bclx_spgemm_plan_s {
   int64_t* acc_tile_offset = nullptr;
 
   void release() {
-    void* ps[] = {light_list, heavy_list, counters, products_dev, row_count, row_offset, heavy_bitmaps,
+    void* ps[] = {light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
                   heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset};
     for (void* p : ps) scratch_free(ctx, p);
-    light_list = heavy_list = counters = row_count = heavy_nitems = tab = id_rp = id_ci = nullptr;
+    light_list = heavy_list = vheavy_list = heavy_tmp = counters = row_count = heavy_nitems = tab = id_rp = id_ci = nullptr;
     products_dev = nullptr;
     row_offset = heavy_first = acc_tile_offset = nullptr;
     heavy_bitmaps = nullptr;
@@ -721,19 +805,18 @@ static unsigned grid_for(Context* ctx, int64_t work_warps, int warps_per_block, 
   return (unsigned)want;
 }
 
-template <typename VT>
 static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P) {
-  const Geom& g = P->g;
-  if (P->n_light > 0) {
-    k_symbolic_light<VT><<<grid_for(ctx, P->n_light, kWarpsSym, 8), kWarpsSym * 32, 0, ctx->stream>>>(
-        A, B, g, P->light_list, P->counters, P->row_count);
+  if (P->n_vheavy > 0) {
+    k_symbolic_block<<<grid_for(ctx, P->n_vheavy, 1, 8), kWarpsSym * 32, 0, ctx->stream>>>(
+        A, B, P->g, P->heavy_list, (int)P->n_vheavy, P->row_count, P->heavy_bitmaps, P->hbm_words);
     note_launch();
     BCLX_CK_LAUNCH();
   }
-  if (P->n_heavy > 0) {
-    const size_t smem = sizeof(uint32_t) * (size_t)P->hbm_words;
-    k_symbolic_heavy<VT><<<grid_for(ctx, P->n_heavy, 1, 8), kHeavyThreads, smem, ctx->stream>>>(
-        A, B, g, P->heavy_list, P->counters, P->row_count, P->heavy_bitmaps, P->hbm_words);
+  const int64_t rows = P->n_light + P->n_heavy - P->n_vheavy;
+  if (rows > 0) {
+    k_symbolic<<<grid_for(ctx, rows, kWarpsSym, 8), kWarpsSym * 32, 0, ctx->stream>>>(
+        A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, (int)P->n_heavy, (int)P->n_vheavy,
+        P->row_count, P->heavy_bitmaps, P->hbm_words);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -748,7 +831,7 @@ static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView&
   BCLX_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t n_total = P->n_light + P->n_heavy_items;
   kern<<<grid_for(ctx, n_total, kWarpsNum, 4), kWarpsNum * 32, smem, ctx->stream>>>(
-      A, B, P->g, P->light_list, P->heavy_list, P->counters, P->heavy_items, P->heavy_first, P->heavy_bitmaps,
+      A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, P->n_heavy_items, P->heavy_items, P->heavy_bitmaps,
       P->hbm_words, P->tab, P->row_count, P->row_offset, out_col, reinterpret_cast<VT*>(out_val), s0, s1);
   note_launch();
   BCLX_CK_LAUNCH();
@@ -771,6 +854,8 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   P->hbm_words = (g.tn + 31) / 32;
   BCLX_TRY(scratch_alloc_n(ctx, &P->light_list, nri));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_list, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->vheavy_list, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_tmp, nri));
   BCLX_TRY(scratch_alloc_n(ctx, &P->counters, 4));
   BCLX_TRY(scratch_alloc_n(ctx, &P->products_dev, 1));
   BCLX_TRY(scratch_alloc_n(ctx, &P->row_count, nri));
@@ -781,25 +866,33 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   // rows of tiles wider than 8192 columns always take the block path
   const int heavy_min_cols = 8192 + 1;
   if (nri > 0) {
-    k_classify<<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P->light_list, P->heavy_list,
-                                                                   P->counters, P->products_dev, heavy_min_cols);
+    k_classify<<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P->light_list, P->heavy_tmp,
+                                                                   P->vheavy_list, P->counters, P->products_dev,
+                                                                   heavy_min_cols);
     note_launch();
     BCLX_CK_LAUNCH();
   }
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned, P->counters, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 1, P->products_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(ctx->pinned, P->counters, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 2, P->products_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
   BCLX_CK(cudaStreamSynchronize(ctx->stream));
-  int32_t cnts[2];
+  int32_t cnts[4];
   std::memcpy(cnts, ctx->pinned, sizeof(cnts));
   P->n_light = cnts[0];
-  P->n_heavy = cnts[1];
-  P->products = ctx->pinned[1];
+  P->n_vheavy = cnts[3];
+  P->n_heavy = cnts[1] + cnts[3];
+  P->products = ctx->pinned[2];
+  // heavy slots: the very heavy rows first, then the others
+  if (P->n_vheavy > 0)
+    BCLX_CK(cudaMemcpyAsync(P->heavy_list, P->vheavy_list, sizeof(int32_t) * P->n_vheavy, cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+  if (cnts[1] > 0)
+    BCLX_CK(cudaMemcpyAsync(P->heavy_list + P->n_vheavy, P->heavy_tmp, sizeof(int32_t) * cnts[1],
+                            cudaMemcpyDeviceToDevice, ctx->stream));
 
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_bitmaps, (size_t)P->n_heavy * P->hbm_words));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_nitems, P->n_heavy));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_first, P->n_heavy + 1));
-  if (dtype == BCLX_F32) BCLX_TRY(launch_symbolic<float>(ctx, A, B, P));
-  else BCLX_TRY(launch_symbolic<int32_t>(ctx, A, B, P));
+  BCLX_TRY(launch_symbolic(ctx, A, B, P));
   BCLX_TRY(exclusive_scan_i32(ctx, P->row_count, P->row_offset, nri));
   const int64_t ntiles = g.gm * g.gn;
   k_tile_ptrs<<<grid_for(ctx, ntiles * (g.tm + 1) / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
@@ -808,7 +901,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   BCLX_CK_LAUNCH();
   if (P->n_heavy > 0) {
     const unsigned blocks = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
-    k_cut_heavy<false><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, P->counters, P->heavy_bitmaps,
+    k_cut_heavy<false><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
                                                         P->hbm_words, P->heavy_nitems, nullptr, nullptr);
     note_launch();
     BCLX_CK_LAUNCH();
@@ -830,7 +923,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   if (P->n_heavy > 0) {
     BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_items, P->n_heavy_items));
     const unsigned blocks = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
-    k_cut_heavy<true><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, P->counters, P->heavy_bitmaps,
+    k_cut_heavy<true><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
                                                        P->hbm_words, nullptr, P->heavy_first, P->heavy_items);
     note_launch();
     BCLX_CK_LAUNCH();
