@@ -70,6 +70,8 @@ SIGNATURES = {
     "bclx_spgemm_plan_stats": [vp, ctypes.POINTER(i64)],
     "bclx_tile_accumulate_symbolic": [vp, vp, i32, i64, i64, i32, vp, ctypes.POINTER(vp), ctypes.POINTER(i64)],
     "bclx_tile_accumulate_numeric": [vp, vp, vp, i32, ctypes.POINTER(CSRDesc)],
+    "bclx_spgemm_tile_noalloc": [ctypes.POINTER(CSRDesc), ctypes.POINTER(CSRDesc), vp, vp, vp, i64,
+                                 ctypes.POINTER(i64), vp],
     "bclx_spmm_tile": [vp, i64, i64, i64, i64, vp, vp, vp, vp, vp, i64, i64, i32],
     "bclx_spmm_grid": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid)],
 }

@@ -63,6 +63,10 @@ int scratch_alloc_n(Context* ctx, T** p, size_t count) {
 // [count+1]; out[count] is the total.
 int exclusive_scan_i32(Context* ctx, const int32_t* in, int64_t* out, int64_t count);
 int exclusive_scan_i64(Context* ctx, const int64_t* in, int64_t* out, int64_t count);
+// The same scan with a caller-provided block-sums buffer of
+// exclusive_scan_sums_len(count) entries (allocates nothing).
+int64_t exclusive_scan_sums_len(int64_t count);
+int exclusive_scan_i32_buf(Context* ctx, const int32_t* in, int64_t* out, int64_t count, int64_t* sums);
 
 // ---- grid views (kernel parameters) -------------------------------------------
 

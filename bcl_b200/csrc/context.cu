@@ -129,6 +129,22 @@ static int exclusive_scan_impl(Context* ctx, const TIn* in, int64_t* out, int64_
   return BCLX_OK;
 }
 
+int64_t exclusive_scan_sums_len(int64_t n) { return ceil_div(n > 0 ? n : 1, kScanChunk) + 1; }
+
+int exclusive_scan_i32_buf(Context* ctx, const int32_t* in, int64_t* out, int64_t n, int64_t* sums) {
+  if (n == 0) {
+    BCLX_CK(cudaMemsetAsync(out, 0, sizeof(int64_t), ctx->stream));
+    return BCLX_OK;
+  }
+  const int64_t nb = ceil_div(n, kScanChunk);
+  k_scan_reduce<int32_t><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(in, n, sums);
+  k_scan_sums<<<1, kScanThreads, 0, ctx->stream>>>(sums, nb);
+  k_scan_final<int32_t><<<(unsigned)nb, kScanThreads, 0, ctx->stream>>>(in, n, sums, out);
+  note_launch(3);
+  BCLX_CK_LAUNCH();
+  return BCLX_OK;
+}
+
 int exclusive_scan_i32(Context* ctx, const int32_t* in, int64_t* out, int64_t n) {
   return exclusive_scan_impl(ctx, in, out, n);
 }

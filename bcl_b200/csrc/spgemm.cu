@@ -40,6 +40,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 namespace bclx {
@@ -1087,3 +1088,215 @@ int bclx_tile_accumulate_numeric(bclx_context_t c, bclx_spgemm_plan_t P, const b
 }
 
 }  // extern "C"
+
+// ---- product of one tile pair without allocating -----------------------------------
+//
+// For callers that cannot allocate device memory at the time of the call: a
+// framework that has reserved the device's memory for its own allocator, or
+// code that must not call cudaMalloc/cudaFree because those calls
+// synchronize the device.  Every work array of the two phases comes from one
+// file-scope device array of kNoAllocScratchBytes, which every GPU that loads
+// this library holds until the process exits.  The first call on a device
+// looks up that array's device address (cudaGetSymbolAddress, with the device
+// current); that first call should come before any stream capture.  Every
+// call uses the same array, and whatever the last call left in it: the parts
+// that must start at zero are cleared by each call, and calls whose work
+// overlaps on the GPU (for instance on two streams) race with each other.
+
+namespace bclx {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static void* g_noalloc_base[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mutex;
+
+struct ScratchArena {
+  unsigned char* base;
+  size_t cap;
+  size_t used = 0;
+  bool ok = true;
+  template <typename T>
+  T* take(size_t count) {
+    const size_t bytes = (sizeof(T) * (count > 0 ? count : 1) + 255) & ~size_t(255);
+    if (!ok || used + bytes > cap) {
+      ok = false;
+      return nullptr;
+    }
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+static int noalloc_base(int device, void** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (device < 0 || device >= kNoAllocMaxDevices) {
+    set_last_error("device ordinal out of range for the no-allocation scratch");
+    return BCLX_ERR_NO_DEVICE;
+  }
+  if (!g_noalloc_base[device]) {
+    void* p = nullptr;
+    BCLX_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_base[device] = p;
+  }
+  *out = g_noalloc_base[device];
+  return BCLX_OK;
+}
+
+static int noalloc_exhausted() {
+  set_last_error("this product needs more than the 32 MiB no-allocation scratch; use "
+                 "bclx_spgemm_symbolic/bclx_spgemm_numeric instead");
+  return BCLX_ERR_INVALID;
+}
+
+static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, const bclx_csr_t* b,
+                           int32_t* c_row_ptr, int32_t* c_col_ind, void* c_vals, int64_t c_capacity,
+                           int64_t* c_nnz) {
+  const int64_t m = a->m, k = a->n, n = b->n;
+  bclx_csr_t* dA = ar.take<bclx_csr_t>(1);
+  bclx_csr_t* dB = ar.take<bclx_csr_t>(1);
+  if (!ar.ok) return noalloc_exhausted();
+  BCLX_CK(cudaMemcpyAsync(dA, a, sizeof(bclx_csr_t), cudaMemcpyHostToDevice, ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(dB, b, sizeof(bclx_csr_t), cudaMemcpyHostToDevice, ctx->stream));
+  SpGridView A{}, B{};
+  A.tiles = dA; A.m = m; A.n = k; A.tm = m; A.tn = k; A.gm = 1; A.gn = 1;
+  B.tiles = dB; B.m = k; B.n = n; B.tm = k; B.tn = n; B.gm = 1; B.gn = 1;
+  Geom g;
+  g.gm = 1; g.gn = 1; g.gk = 1; g.tm = m; g.tn = n; g.tk = k; g.m = m; g.n = n;
+  g.n_row_items = m;
+  g.nfb = ceil_div(n, kFineCols);
+
+  bclx_spgemm_plan_s P;  // its arrays live in the arena; it is never released
+  P.ctx = ctx;
+  P.g = g;
+  P.dtype = a->dtype;
+  P.hbm_words = (n + 31) / 32;
+  const int64_t nri = m;
+  P.light_list = ar.take<int32_t>(nri);
+  P.heavy_list = ar.take<int32_t>(nri);
+  P.vheavy_list = ar.take<int32_t>(nri);
+  P.heavy_tmp = ar.take<int32_t>(nri);
+  P.counters = ar.take<int32_t>(4);
+  P.products_dev = ar.take<unsigned long long>(1);
+  P.row_count = ar.take<int32_t>(nri);
+  P.row_offset = ar.take<int64_t>(nri + 1);
+  int64_t* tile_offset = ar.take<int64_t>(2);
+  int64_t* sums = ar.take<int64_t>(exclusive_scan_sums_len(nri));
+  if (!ar.ok) return noalloc_exhausted();
+  BCLX_CK(cudaMemsetAsync(P.counters, 0, 4 * sizeof(int32_t), ctx->stream));
+  BCLX_CK(cudaMemsetAsync(P.products_dev, 0, sizeof(unsigned long long), ctx->stream));
+  BCLX_CK(cudaMemsetAsync(P.row_count, 0, sizeof(int32_t) * nri, ctx->stream));
+  k_classify<<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P.light_list, P.heavy_tmp, P.vheavy_list,
+                                                                 P.counters, P.products_dev, 8192 + 1);
+  note_launch();
+  BCLX_CK_LAUNCH();
+  int32_t cnts[4];
+  BCLX_CK(cudaMemcpyAsync(cnts, P.counters, sizeof(cnts), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
+  P.n_light = cnts[0];
+  P.n_vheavy = cnts[3];
+  P.n_heavy = cnts[1] + cnts[3];
+  if (P.n_vheavy > 0)
+    BCLX_CK(cudaMemcpyAsync(P.heavy_list, P.vheavy_list, sizeof(int32_t) * P.n_vheavy, cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+  if (cnts[1] > 0)
+    BCLX_CK(cudaMemcpyAsync(P.heavy_list + P.n_vheavy, P.heavy_tmp, sizeof(int32_t) * cnts[1],
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+  P.heavy_bitmaps = ar.take<uint32_t>((size_t)P.n_heavy * P.hbm_words);
+  P.heavy_nitems = ar.take<int32_t>(P.n_heavy);
+  P.heavy_first = ar.take<int64_t>(P.n_heavy + 1);
+  int64_t* sums_h = ar.take<int64_t>(exclusive_scan_sums_len(P.n_heavy));
+  if (!ar.ok) return noalloc_exhausted();
+  BCLX_TRY(launch_symbolic(ctx, A, B, &P));
+  BCLX_TRY(exclusive_scan_i32_buf(ctx, P.row_count, P.row_offset, nri, sums));
+  k_tile_ptrs<<<grid_for(ctx, (g.tm + 1) / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(g, P.row_offset, c_row_ptr,
+                                                                                 tile_offset, P.counters + 2);
+  note_launch();
+  BCLX_CK_LAUNCH();
+  if (P.n_heavy > 0) {
+    k_cut_heavy<false><<<grid_for(ctx, P.n_heavy / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
+        g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, P.heavy_nitems, nullptr, nullptr);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+  BCLX_TRY(exclusive_scan_i32_buf(ctx, P.heavy_nitems, P.heavy_first, P.n_heavy, sums_h));
+  int64_t tail[3];
+  BCLX_CK(cudaMemcpyAsync(&tail[0], P.row_offset + nri, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(&tail[1], P.heavy_first + P.n_heavy, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(&tail[2], P.counters + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
+  int32_t overflow;
+  std::memcpy(&overflow, &tail[2], sizeof(overflow));
+  if (overflow) {
+    set_last_error("the product has more than 2^31-1 nonzeros");
+    return BCLX_ERR_INDEX_OVERFLOW;
+  }
+  P.nnz = tail[0];
+  P.n_heavy_items = tail[1];
+  *c_nnz = P.nnz;
+  if (P.nnz > c_capacity) {
+    set_last_error("output capacity too small: the product has " + std::to_string(P.nnz) +
+                   " nonzeros (c_row_ptr and *c_nnz are written; retry with larger c_col_ind/c_vals)");
+    return BCLX_ERR_INVALID;
+  }
+  if (P.n_heavy > 0) {
+    P.heavy_items = ar.take<HeavyItem>(P.n_heavy_items);
+    P.tab = ar.take<int32_t>((size_t)g.tk * (g.nfb + 1));
+    if (!ar.ok) return noalloc_exhausted();
+    k_cut_heavy<true><<<grid_for(ctx, P.n_heavy / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
+        g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, nullptr, P.heavy_first, P.heavy_items);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    if (g.tk > 0) {
+      k_btable<<<grid_for(ctx, g.tk / 32 + 1, 8, 16), 256, 0, ctx->stream>>>(B, g, P.tab);
+      note_launch();
+      BCLX_CK_LAUNCH();
+    }
+  }
+  if (P.n_light + P.n_heavy_items == 0) return BCLX_OK;
+  if (P.dtype == BCLX_F32) return launch_numeric<float>(ctx, A, B, &P, c_col_ind, c_vals, 0, 1);
+  return launch_numeric<int32_t>(ctx, A, B, &P, c_col_ind, c_vals, 0, 1);
+}
+
+}  // namespace bclx
+
+extern "C" int bclx_spgemm_tile_noalloc(const bclx_csr_t* a, const bclx_csr_t* b, int32_t* c_row_ptr,
+                                        int32_t* c_col_ind, void* c_vals, int64_t c_capacity, int64_t* c_nnz,
+                                        void* stream) {
+  if (!a || !b || !c_row_ptr || !c_nnz || c_capacity < 0) return BCLX_ERR_INVALID;
+  *c_nnz = 0;
+  if (a->n != b->m || a->m < 0 || a->n < 0 || b->n < 0) {
+    set_last_error("shape mismatch: A is m x k and B must be k x n");
+    return BCLX_ERR_INVALID;
+  }
+  if (a->dtype != b->dtype || !value_size(a->dtype)) return BCLX_ERR_DTYPE;
+  if (b->n > kMaxCols || a->m > INT32_MAX || a->n > INT32_MAX) {
+    set_last_error("tile too large for the no-allocation product (at most 16384 columns)");
+    return BCLX_ERR_INVALID;
+  }
+  if (a->m > 0 && (!a->row_ptr || (a->nnz > 0 && (!a->col_ind || !a->vals)))) return BCLX_ERR_INVALID;
+  if (a->n > 0 && (!b->row_ptr || (b->nnz > 0 && (!b->col_ind || !b->vals)))) return BCLX_ERR_INVALID;
+  if (c_capacity > 0 && (!c_col_ind || !c_vals)) return BCLX_ERR_INVALID;
+  int device = 0;
+  BCLX_CK(cudaGetDevice(&device));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (a->m == 0) return BCLX_OK;
+  if (b->n == 0 || a->n == 0) {
+    BCLX_CK(cudaMemsetAsync(c_row_ptr, 0, sizeof(int32_t) * (a->m + 1), st));
+    return BCLX_OK;
+  }
+  void* base = nullptr;
+  BCLX_TRY(noalloc_base(device, &base));
+  int nsm = 148;
+  BCLX_CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  Context ctx;
+  ctx.device = device;
+  ctx.num_sms = nsm;
+  ctx.stream = st;
+  ctx.pinned = nullptr;
+  ScratchArena ar{reinterpret_cast<unsigned char*>(base), kNoAllocScratchBytes};
+  return noalloc_product(&ctx, ar, a, b, c_row_ptr, c_col_ind, c_vals, c_capacity, c_nnz);
+}

@@ -179,6 +179,29 @@ BCLX_API int bclx_tile_accumulate_symbolic(bclx_context_t ctx, const bclx_csr_t*
 BCLX_API int bclx_tile_accumulate_numeric(bclx_context_t ctx, bclx_spgemm_plan_t plan, const bclx_csr_t* parts,
                                  int32_t nparts, bclx_csr_t* c);
 
+/* ---- one tile pair, without allocating -----------------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory when they call (a framework that has
+ * reserved the device's memory for its own allocator, or code that must not
+ * call cudaMalloc/cudaFree because they synchronize the device).
+ * C = A * B for one pair of CSR tiles (A m x k, B k x n, both BCLX_F32 or both
+ * BCLX_I32; host structs holding device pointers), with the same results as
+ * bclx_spgemm_symbolic/_numeric on 1x1 grids.  The caller provides
+ * c_row_ptr[m+1] and c_col_ind/c_vals with room for c_capacity entries; the
+ * call writes c_row_ptr and *c_nnz, and returns BCLX_ERR_INVALID without
+ * touching c_col_ind/c_vals when *c_nnz > c_capacity (retry with more room).
+ * No cudaMalloc/cudaFree: all work arrays come from a 32 MiB device array
+ * that the library holds on every GPU it runs on; a tile product that needs
+ * more (or B wider than 16384 columns) is rejected with BCLX_ERR_INVALID.
+ * The first call on a device looks that array up and should come before any
+ * stream capture.  Calls share the array: calls whose work overlaps on the
+ * GPU (different streams) race.  Runs on `stream` on the current device; the
+ * two phases synchronize that stream in between, and the values are ready
+ * when the stream reaches the end of the call. */
+BCLX_API int bclx_spgemm_tile_noalloc(const bclx_csr_t* a, const bclx_csr_t* b, int32_t* c_row_ptr,
+                                      int32_t* c_col_ind, void* c_vals, int64_t c_capacity, int64_t* c_nnz,
+                                      void* stream);
+
 /* ---- sparse x dense ------------------------------------------------------
  * C += A * B for one tile (spmm_wrapper, spgemm.hpp:140-149): A is m x k CSR
  * (FP32 values), B is k x n row-major with leading dimension ldb, C is m x n
