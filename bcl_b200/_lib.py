@@ -67,6 +67,9 @@ SIGNATURES = {
     "bclx_spgemm_numeric": [vp, vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
                             i32, i32],
     "bclx_spgemm_plan_destroy": [vp],
+    "bclx_spgemm_numeric_staged": [vp, vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
+                                   i32],
+    "bclx_spgemm_plan_tune": [vp, i32, i32, i32],
     "bclx_spgemm_plan_stats": [vp, ctypes.POINTER(i64)],
     "bclx_tile_accumulate_symbolic": [vp, vp, i32, i64, i64, i32, vp, ctypes.POINTER(vp), ctypes.POINTER(i64)],
     "bclx_tile_accumulate_numeric": [vp, vp, vp, i32, ctypes.POINTER(CSRDesc)],

@@ -421,6 +421,10 @@ class SpgemmPlan:
         keys = ["products", "light_rows", "heavy_rows", "heavy_items", "stages", "nnz"]
         return dict(zip(keys, [int(x) for x in arr]))
 
+    def tune(self, grab: int, blocks_per_sm: int, long_seg: int) -> None:
+        """Numeric-pass parameters (see bclx_spgemm_plan_tune)."""
+        call("bclx_spgemm_plan_tune", self.h, int(grab), int(blocks_per_sm), int(long_seg))
+
     def close(self):
         if self.h:
             _lib.load().bclx_spgemm_plan_destroy(self.h)
@@ -453,13 +457,20 @@ def spgemm_symbolic(a: SPMatrix, b: SPMatrix):
     return SpgemmPlan(plan), out, trp, toff, int(nnz.value)
 
 
-def spgemm(a: SPMatrix, b: SPMatrix, stages: str = "fused", keep_plan: bool = False):
+def spgemm(a: SPMatrix, b: SPMatrix, stages: str = "fused", keep_plan: bool = False, tuning=None):
     """C = A * B over the tile grids (BCL::gemm(SPMatrix, SPMatrix, SPMatrix&),
     spgemm.hpp:182-242).  ``stages="fused"`` runs every SUMMA stage in one
-    numeric launch; ``"per_stage"`` runs one launch per stage (all G*G tile
-    products of that stage), adding into C between them; the results are
-    bit-identical."""
+    numeric launch; ``"per_stage"`` / ``"batched"`` run one launch per stage
+    (all G*G tile products of that stage), adding into C between them;
+    ``"batched_graph"`` does the same through a CUDA graph kept by the plan.
+    All forms are bit-identical.  ``tuning`` = (grab, blocks_per_sm,
+    long_seg), or "auto" for the autotuner's cached choice."""
     plan, out, trp, toff, nnz = spgemm_symbolic(a, b)
+    if tuning == "auto":
+        from . import autotune
+        tuning = autotune.lookup(a, b, plan)
+    if tuning:
+        plan.tune(*tuning)
     td = a.tile_row_ptr.device
     ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=td)
     v = torch.empty(max(nnz, 1), dtype=_TORCH_OF[_NP_TO_DT[a.dtype]], device=td)
@@ -480,6 +491,9 @@ def spgemm_numeric(plan: SpgemmPlan, a: SPMatrix, b: SPMatrix, out: SpGridOut, s
     elif stages == "per_stage":
         for s in range(a.gn):
             call("bclx_spgemm_numeric", h, plan.h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), s, s + 1)
+    elif stages in ("batched", "batched_graph"):
+        call("bclx_spgemm_numeric_staged", h, plan.h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out),
+             1 if stages == "batched_graph" else 0)
     else:
         raise ValueError(stages)
 

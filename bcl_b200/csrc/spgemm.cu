@@ -39,6 +39,7 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -53,10 +54,8 @@ constexpr int kMaxCols = kMaxWords * 32;
 constexpr int kWarpsSym = 8;
 constexpr int kWarpsNum = 8;
 constexpr int kNoStage = 0xff;
-#ifndef BCLX_LONG_SEG
-#define BCLX_LONG_SEG 48
-#endif
-constexpr int kLongSeg = BCLX_LONG_SEG;  // B segments at least this long are walked in direct mode
+constexpr int kLongSegDefault = 48;
+constexpr int kQueueSlots = 256;          // work-queue heads in a plan (one per stage launch)       // B segments at least this long are walked in direct mode
 constexpr int64_t kVeryHeavyUb = 32768;  // rows above this many products get a whole block in the symbolic pass
 
 struct Geom {
@@ -124,7 +123,7 @@ __device__ __forceinline__ P* shfl_ptr(P* p, int src) {
 template <typename VT, bool RANGED, typename F, typename FD>
 __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridView& B, const Geom& g,
                                               const RowInfo& x, int s0, int s1, int fb_lo, int fb_hi,
-                                              const int32_t* __restrict__ tab, F&& f, FD&& fd) {
+                                              const int32_t* __restrict__ tab, int long_seg, F&& f, FD&& fd) {
   const int lane = lane_id();
   for (int g0 = s0; g0 < s1; g0 += 32) {
     // one lane per stage: its A-row segment and its B tile
@@ -182,7 +181,7 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
         bval = sbva + bs;
       }
       const int nent = min(32, atot - e0);
-      const unsigned longm = __ballot_sync(kFull, len >= kLongSeg);
+      const unsigned longm = __ballot_sync(kFull, len >= long_seg);
       int e_start = 0;
       while (e_start < nent) {
         const unsigned lm = longm & (kFull << e_start);
@@ -547,14 +546,24 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
               const HeavyItem* __restrict__ heavy_items,
               const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, const int32_t* __restrict__ tab,
               const int32_t* __restrict__ row_count, const int64_t* __restrict__ row_offset,
-              int32_t* __restrict__ out_col, VT* __restrict__ out_val, int s0, int s1) {
+              int32_t* __restrict__ out_col, VT* __restrict__ out_val, int s0, int s1,
+              unsigned long long* __restrict__ queue, int grab, int long_seg) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem<VT, WORDS>& S = reinterpret_cast<WarpSmem<VT, WORDS>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = lane_id();
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t n_total = n_heavy_items + n_light;
-  for (int64_t idx = warp; idx < n_total; idx += nwarps) {
+  // persistent warps: take `grab` consecutive items at a time from the queue
+  int64_t next = 0, stop = 0;
+  for (;;) {
+    if (next >= stop) {
+      unsigned long long b = 0;
+      if (lane == 0) b = atomicAdd(queue, (unsigned long long)grab);
+      b = __shfl_sync(kFull, b, 0);
+      if ((int64_t)b >= n_total) break;
+      next = (int64_t)b;
+      stop = min((int64_t)b + grab, n_total);
+    }
+    const int64_t idx = next++;
     // heavy items first (they are the larger ones)
     const bool heavy = idx < n_heavy_items;
     int64_t ri;
@@ -695,9 +704,9 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
       S.part[rank] = madd(a, b, v);
     };
     if (heavy)
-      walk_products<VT, true>(A, B, g, x, s0, s1, fb_lo, fb_hi, tab, update, update_direct);
+      walk_products<VT, true>(A, B, g, x, s0, s1, fb_lo, fb_hi, tab, long_seg, update, update_direct);
     else
-      walk_products<VT, false>(A, B, g, x, s0, s1, 0, 0, nullptr, update, update_direct);
+      walk_products<VT, false>(A, B, g, x, s0, s1, 0, 0, nullptr, long_seg, update, update_direct);
 
     // 5. last fold and values out
     for (int q = lane; q < cnt; q += 32) {
@@ -749,6 +758,14 @@ struct bclx_spgemm_plan_s {
   int64_t* heavy_first = nullptr;
   HeavyItem* heavy_items = nullptr;
   int32_t* tab = nullptr;
+  unsigned long long* queue = nullptr;  // work-queue heads, one per stage launch
+  // numeric tuning (bclx_spgemm_plan_tune)
+  int grab = 2, blocks_per_sm = 4, long_seg = kLongSegDefault;
+  // CUDA graph of the staged numeric pass (bclx_spgemm_numeric_staged)
+  cudaGraphExec_t graph = nullptr;
+  const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t gstream = nullptr;  // capture/replay stream (the caller's may be the legacy default stream)
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   // tile accumulation: identity A tiles and their descriptors, 1x1 C offsets
   int32_t* id_rp = nullptr;
   int32_t* id_ci = nullptr;
@@ -757,9 +774,22 @@ struct bclx_spgemm_plan_s {
   int64_t* acc_tile_offset = nullptr;
 
   void release() {
-    void* ps[] = {light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
+    if (graph) {
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+    if (gstream) {
+      cudaStreamSynchronize(gstream);
+      cudaStreamDestroy(gstream);
+      gstream = nullptr;
+    }
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    ev_in = ev_out = nullptr;
+    void* ps[] = {queue, light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
                   heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset};
     for (void* p : ps) scratch_free(ctx, p);
+    queue = nullptr;
     light_list = heavy_list = vheavy_list = heavy_tmp = counters = row_count = heavy_nitems = tab = id_rp = id_ci = nullptr;
     products_dev = nullptr;
     row_offset = heavy_first = acc_tile_offset = nullptr;
@@ -829,11 +859,20 @@ static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView&
                             int32_t* out_col, void* out_val, int s0, int s1) {
   constexpr size_t smem = sizeof(WarpSmem<VT, WORDS>) * kWarpsNum;
   auto kern = k_numeric<VT, WORDS>;
-  BCLX_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  static std::atomic<unsigned long long> configured{0};  // one bit per device
+  const unsigned long long bit = 1ull << (ctx->device & 63);
+  if (!(configured.load() & bit)) {
+    BCLX_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured.fetch_or(bit);
+  }
   const int64_t n_total = P->n_light + P->n_heavy_items;
-  kern<<<grid_for(ctx, n_total, kWarpsNum, 4), kWarpsNum * 32, smem, ctx->stream>>>(
+  unsigned long long* q = P->queue + (s0 % kQueueSlots);
+  BCLX_CK(cudaMemsetAsync(q, 0, sizeof(unsigned long long), ctx->stream));
+  const int bps = P->blocks_per_sm < 1 ? 1 : (P->blocks_per_sm > 4 ? 4 : P->blocks_per_sm);
+  kern<<<grid_for(ctx, n_total, kWarpsNum, bps), kWarpsNum * 32, smem, ctx->stream>>>(
       A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, P->n_heavy_items, P->heavy_items, P->heavy_bitmaps,
-      P->hbm_words, P->tab, P->row_count, P->row_offset, out_col, reinterpret_cast<VT*>(out_val), s0, s1);
+      P->hbm_words, P->tab, P->row_count, P->row_offset, out_col, reinterpret_cast<VT*>(out_val), s0, s1, q,
+      P->grab < 1 ? 1 : P->grab, P->long_seg < 1 ? 1 : P->long_seg);
   note_launch();
   BCLX_CK_LAUNCH();
   return BCLX_OK;
@@ -861,6 +900,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   BCLX_TRY(scratch_alloc_n(ctx, &P->products_dev, 1));
   BCLX_TRY(scratch_alloc_n(ctx, &P->row_count, nri));
   BCLX_TRY(scratch_alloc_n(ctx, &P->row_offset, nri + 1));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->queue, kQueueSlots));
   BCLX_CK(cudaMemsetAsync(P->counters, 0, 4 * sizeof(int32_t), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P->products_dev, 0, sizeof(unsigned long long), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P->row_count, 0, sizeof(int32_t) * (nri > 0 ? nri : 1), ctx->stream));
@@ -1010,6 +1050,87 @@ int bclx_spgemm_plan_stats(bclx_spgemm_plan_t P, int64_t* out6) {
   out6[3] = P->n_heavy_items;
   out6[4] = P->g.gk;
   out6[5] = P->nnz;
+  return BCLX_OK;
+}
+
+int bclx_spgemm_plan_tune(bclx_spgemm_plan_t P, int32_t grab, int32_t blocks_per_sm, int32_t long_seg) {
+  if (!P || grab < 1 || grab > 64 || blocks_per_sm < 1 || blocks_per_sm > 4 || long_seg < 1)
+    return BCLX_ERR_INVALID;
+  P->grab = grab;
+  P->blocks_per_sm = blocks_per_sm;
+  P->long_seg = long_seg;
+  if (P->graph) {  // the captured launches carry the old parameters
+    cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+  }
+  return BCLX_OK;
+}
+
+int bclx_spgemm_numeric_staged(bclx_context_t c, bclx_spgemm_plan_t P, const bclx_spgrid_t* a,
+                               const bclx_spgrid_t* b, bclx_spgrid_out_t* out, int32_t use_graph) {
+  Context* ctx = reinterpret_cast<Context*>(c);
+  if (!ctx || !P) return BCLX_ERR_INVALID;
+  BCLX_TRY(check_grids(a, b, out));
+  if (a->grid_n != P->g.gk || out->grid_m != P->g.gm || out->grid_n != P->g.gn || a->dtype != P->dtype)
+    return BCLX_ERR_INVALID;
+  if (P->nnz > 0 && (!out->col_ind || !out->vals)) return BCLX_ERR_INVALID;
+  BCLX_CK(cudaSetDevice(ctx->device));
+  const SpGridView A = make_view(*a), B = make_view(*b);
+  const int G = (int)P->g.gk;
+  auto run_all = [&]() -> int {
+    for (int s = 0; s < G; s++) BCLX_TRY(numeric_impl(ctx, P, A, B, out->col_ind, out->vals, s, s + 1));
+    return BCLX_OK;
+  };
+  if (!use_graph) return run_all();
+  const void* key[4] = {a->tiles, b->tiles, out->col_ind, out->vals};
+  if (P->graph && std::memcmp(key, P->graph_key, sizeof(key)) != 0) {
+    cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+  }
+  if (!P->gstream) {
+    BCLX_CK(cudaStreamCreateWithFlags(&P->gstream, cudaStreamNonBlocking));
+    BCLX_CK(cudaEventCreateWithFlags(&P->ev_in, cudaEventDisableTiming));
+    BCLX_CK(cudaEventCreateWithFlags(&P->ev_out, cudaEventDisableTiming));
+  }
+  if (!P->graph) {
+    // this call computes C directly (which also configures the kernels), then
+    // captures the G launches on the plan's stream for later replays
+    BCLX_TRY(run_all());
+    BCLX_CK(cudaEventRecord(P->ev_in, ctx->stream));
+    BCLX_CK(cudaStreamWaitEvent(P->gstream, P->ev_in, 0));
+    Context cap = *ctx;
+    cap.stream = P->gstream;
+    cudaGraph_t graph = nullptr;
+    BCLX_CK(cudaStreamBeginCapture(P->gstream, cudaStreamCaptureModeThreadLocal));
+    int rc = BCLX_OK;
+    for (int s = 0; s < G && rc == BCLX_OK; s++)
+      rc = numeric_impl(&cap, P, A, B, out->col_ind, out->vals, s, s + 1);
+    const cudaError_t e = cudaStreamEndCapture(P->gstream, &graph);
+    if (rc != BCLX_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) {
+      set_last_error(std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+      return BCLX_ERR_CUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+      set_last_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+      return BCLX_ERR_CUDA;
+    }
+    P->graph = exec;
+    std::memcpy(P->graph_key, key, sizeof(key));
+    return BCLX_OK;
+  }
+  BCLX_CK(cudaEventRecord(P->ev_in, ctx->stream));
+  BCLX_CK(cudaStreamWaitEvent(P->gstream, P->ev_in, 0));
+  BCLX_CK(cudaGraphLaunch(P->graph, P->gstream));
+  BCLX_CK(cudaEventRecord(P->ev_out, P->gstream));
+  BCLX_CK(cudaStreamWaitEvent(ctx->stream, P->ev_out, 0));
+  note_launch(G);
   return BCLX_OK;
 }
 
@@ -1184,6 +1305,7 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
   P.row_offset = ar.take<int64_t>(nri + 1);
   int64_t* tile_offset = ar.take<int64_t>(2);
   int64_t* sums = ar.take<int64_t>(exclusive_scan_sums_len(nri));
+  P.queue = ar.take<unsigned long long>(kQueueSlots);
   if (!ar.ok) return noalloc_exhausted();
   BCLX_CK(cudaMemsetAsync(P.counters, 0, 4 * sizeof(int32_t), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P.products_dev, 0, sizeof(unsigned long long), ctx->stream));

@@ -163,6 +163,22 @@ BCLX_API int bclx_spgemm_numeric(bclx_context_t ctx, bclx_spgemm_plan_t plan, co
                         const bclx_spgrid_t* b, bclx_spgrid_out_t* c, int32_t stage_begin,
                         int32_t stage_end);
 BCLX_API int bclx_spgemm_plan_destroy(bclx_spgemm_plan_t plan);
+/* Batched SUMMA form: the numeric pass as one launch per stage k_ (each launch
+ * covers all grid_m*grid_n tile products of that stage, adding into C), in
+ * order.  use_graph = 1 captures the G launches once into a CUDA graph kept
+ * by the plan and replays it on later calls with the same plan, grids and
+ * output arrays (a replay recomputes the values for the same structure; the
+ * call that captures also computes C).  Bit-identical to bclx_spgemm_numeric.
+ * The batched stage loop has no single reference counterpart; it runs the
+ * stages of spgemm.hpp:209-224 for all C tiles at once. */
+BCLX_API int bclx_spgemm_numeric_staged(bclx_context_t ctx, bclx_spgemm_plan_t plan, const bclx_spgrid_t* a,
+                                        const bclx_spgrid_t* b, bclx_spgrid_out_t* c, int32_t use_graph);
+/* Numeric-pass tuning of a plan: grab = work items a warp takes from the
+ * device work queue at a time (1..64), blocks_per_sm (1..4), long_seg = B
+ * segments of at least this many products are walked lane-parallel.  Chosen
+ * by the autotuner (bcl_b200/autotune.py); no reference counterpart. */
+BCLX_API int bclx_spgemm_plan_tune(bclx_spgemm_plan_t plan, int32_t grab, int32_t blocks_per_sm,
+                                   int32_t long_seg);
 /* Plan statistics: [0] intermediate products, [1] row items, [2] work items,
  * [3] work items in the large-accumulator class, [4] stages, [5] output nnz. */
 BCLX_API int bclx_spgemm_plan_stats(bclx_spgemm_plan_t plan, int64_t* out6);

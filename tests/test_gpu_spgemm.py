@@ -166,3 +166,64 @@ def test_fp32_error_vs_fp64():
     print(f"\nFP32 vs FP64: max abs {err.max():.3e}, median rel {np.median(rel):.3e}, "
           f"norm ratio {np.linalg.norm(err) / np.linalg.norm(c64):.3e}")
     assert np.linalg.norm(err) / np.linalg.norm(c64) < 1e-6
+
+
+@pytest.mark.parametrize("mode", ["batched", "batched_graph"])
+def test_batched_forms_match(mode):
+    """One launch per SUMMA stage (all tile products of the stage), directly
+    or through the plan's CUDA graph: bit-identical to the oracle."""
+    a = gen.rmat(12, seed=61)
+    tiles = (1024, 1024, 1024)
+    rp, ci, cv = O.gemm_tiled(a, a, *tiles)
+    assert_csr_identical(product(a, a, tiles, mode).get(), rp, ci, cv)
+
+
+def test_graph_replay_with_new_values():
+    """Same structure, new values: replaying the captured stage launches
+    recomputes C for the new values (the plan keeps the structure)."""
+    import torch
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm_numeric, spgemm_symbolic
+    a = gen.rmat(12, seed=62)
+    A = SPMatrix.from_csr(a, BlockCustom((1024, 1024)))
+    plan, out, trp, toff, nnz = spgemm_symbolic(A, A)
+    ci = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    v = torch.empty(nnz, dtype=torch.float32, device="cuda")
+    out.col_ind, out.vals = ci.data_ptr(), v.data_ptr()
+    spgemm_numeric(plan, A, A, out, "batched_graph")       # captures
+    rng = np.random.default_rng(5)
+    for rep in range(2):
+        a2 = gen.CSR(a.m, a.n, a.row_ptr, a.col_ind, rng.uniform(-1, 1, a.nnz).astype(np.float32))
+        A2 = SPMatrix.from_csr(a2, BlockCustom((1024, 1024)))
+        A.vals.copy_(A2.vals)                               # new values, same structure and addresses
+        spgemm_numeric(plan, A, A, out, "batched_graph")    # replays
+        torch.cuda.synchronize()
+        from bcl_b200.containers import SPMatrix as S
+        C = S(A.m, A.n, A.tm, A.tn, A.dtype, A.device, trp, toff, ci, v)
+        rp, cc, cv = O.gemm_tiled(a2, a2, 1024, 1024, 1024)
+        assert_csr_identical(C.get(), rp, cc, cv)
+    plan.close()
+
+
+@pytest.mark.parametrize("tuning", [(1, 3, 32), (8, 4, 1 << 30), (4, 2, 16)])
+def test_tuning_does_not_change_results(tuning):
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm
+    a = gen.rmat(12, seed=63)
+    A = SPMatrix.from_csr(a, BlockCustom((1024, 1024)))
+    rp, ci, cv = O.gemm_tiled(a, a, 1024, 1024, 1024)
+    assert_csr_identical(spgemm(A, A, tuning=tuning).get(), rp, ci, cv)
+
+
+def test_autotune_roundtrip(tmp_path, monkeypatch):
+    monkeypatch.setenv("BCLX_CACHE", str(tmp_path))
+    from bcl_b200 import autotune
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm
+    a = gen.rmat(11, seed=64)
+    A = SPMatrix.from_csr(a, BlockCustom((1024, 1024)))
+    params, ms, table = autotune.tune(A, A, reps=1, candidates={"grab": (1, 4), "blocks_per_sm": (4,),
+                                                                "long_seg": (48,)})
+    assert len(table) == 2 and ms > 0
+    C, plan = spgemm(A, A, tuning="auto", keep_plan=True)
+    assert autotune.lookup(A, A, plan) == tuple(params)
+    plan.close()
+    rp, ci, cv = O.gemm_tiled(a, a, 1024, 1024, 1024)
+    assert_csr_identical(C.get(), rp, ci, cv)
