@@ -75,6 +75,17 @@ SIGNATURES = {
     "bclx_tile_accumulate_numeric": [vp, vp, vp, i32, ctypes.POINTER(CSRDesc)],
     "bclx_spgemm_tile_noalloc": [ctypes.POINTER(CSRDesc), ctypes.POINTER(CSRDesc), vp, vp, vp, i64,
                                  ctypes.POINTER(i64), vp],
+    "bclx_spgemm_learned_run": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut), vp,
+                                ctypes.POINTER(vp), ctypes.POINTER(i64)],
+    "bclx_spgemm_learned_finish": [vp, vp, ctypes.POINTER(SpGridOut)],
+    "bclx_spgemm_learned_stats": [vp, ctypes.POINTER(i64)],
+    "bclx_spgemm_row_features": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut), vp,
+                                 vp],
+    "bclx_spgemm_plan_row_counts": [vp, vp],
+    "bclx_mlp_num_params": [],
+    "bclx_mlp_predict": [vp, vp, i64, vp, vp],
+    "bclx_mlp_gradient": [vp, vp, vp, i64, vp, vp],
+    "bclx_mlp_train": [vp, vp, vp, i64, vp, i32, ctypes.c_float, vp],
     "bclx_spmm_tile": [vp, i64, i64, i64, i64, vp, vp, vp, vp, vp, i64, i64, i32],
     "bclx_spmm_grid": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid)],
 }

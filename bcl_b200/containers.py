@@ -426,8 +426,10 @@ class SpgemmPlan:
         call("bclx_spgemm_plan_tune", self.h, int(grab), int(blocks_per_sm), int(long_seg))
 
     def close(self):
-        if self.h:
-            _lib.load().bclx_spgemm_plan_destroy(self.h)
+        if getattr(self, "h", None):
+            lib = _lib._lib
+            if lib is not None:  # (at interpreter exit the library may be gone already)
+                lib.bclx_spgemm_plan_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -481,6 +483,45 @@ def spgemm(a: SPMatrix, b: SPMatrix, stages: str = "fused", keep_plan: bool = Fa
         return c, plan
     plan.close()
     return c
+
+
+def spgemm_learned(a: SPMatrix, b: SPMatrix, predictor="default", keep_plan: bool = False):
+    """C = A * B through the learned product: a row-nnz predictor sizes the
+    work instead of a symbolic pass; rows it mispredicts are redone exactly,
+    so the result is bit-identical to spgemm().  ``predictor``: a
+    learned.RowNnzPredictor, "default" (the cached trained model), or None
+    (size the work from the product counts instead of a prediction)."""
+    _check_grids(a, b)
+    if predictor == "default":
+        from . import learned
+        predictor = learned.get_default()
+    h = context(a.device).use_current_stream()
+    out, trp, toff = _out_grid(a, b)
+    plan = ctypes.c_void_p()
+    nnz = ctypes.c_int64()
+    ag, bg = a.spgrid(), b.spgrid()
+    prm = ctypes.c_void_p(predictor.params.data_ptr()) if predictor is not None else None
+    call("bclx_spgemm_learned_run", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), prm,
+         ctypes.byref(plan), ctypes.byref(nnz))
+    pl = SpgemmPlan(plan)
+    k = int(nnz.value)
+    td = a.tile_row_ptr.device
+    ci = torch.empty(max(k, 1), dtype=torch.int32, device=td)
+    v = torch.empty(max(k, 1), dtype=_TORCH_OF[_NP_TO_DT[a.dtype]], device=td)
+    out.col_ind, out.vals = ci.data_ptr(), v.data_ptr()
+    call("bclx_spgemm_learned_finish", h, pl.h, ctypes.byref(out))
+    c = SPMatrix(a.m, b.n, a.tm, b.tn, a.dtype, a.device, trp, toff, ci, v)
+    if keep_plan:
+        return c, pl
+    pl.close()
+    return c
+
+
+def learned_stats(plan: "SpgemmPlan") -> dict:
+    arr = (ctypes.c_int64 * 6)()
+    call("bclx_spgemm_learned_stats", plan.h, arr)
+    keys = ["heavy_rows", "heavy_items", "rows_redone", "temp_entries", "nnz", "redo_items"]
+    return dict(zip(keys, [int(x) for x in arr]))
 
 
 def spgemm_numeric(plan: SpgemmPlan, a: SPMatrix, b: SPMatrix, out: SpGridOut, stages: str = "fused"):

@@ -308,22 +308,82 @@ __device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridVi
   }
 }
 
+// Order-free walk over the products of C-tile row `x` whose columns lie in
+// fine blocks [fb_lo, fb_hi) (B-row table `tab`): calls fs(j) for each.
+template <typename FS>
+__device__ __forceinline__ void walk_columns_ranged(const SpGridView& A, const SpGridView& B, const Geom& g,
+                                                    const RowInfo& x, int fb_lo, int fb_hi,
+                                                    const int32_t* __restrict__ tab, FS&& fs) {
+  const int lane = lane_id();
+  for (int g0 = 0; g0 < g.gk; g0 += 32) {
+    const int kk = g0 + lane;
+    int32_t as = 0, alen = 0;
+    const int32_t* acol = nullptr;
+    const int32_t* trows = nullptr;
+    const int32_t* bci = nullptr;
+    if (kk < g.gk) {
+      const bclx_csr_t At = A.tile(x.ti, kk);
+      as = __ldg(At.row_ptr + x.r);
+      alen = __ldg(At.row_ptr + x.r + 1) - as;
+      acol = At.col_ind;
+      trows = tab + ((int64_t)kk * g.gn + x.tj) * g.tk * (g.nfb + 1);
+      bci = B.tile(kk, x.tj).col_ind;
+    }
+    const int32_t aincl = warp_inclusive_scan(alen);
+    const int32_t atot = __shfl_sync(kFull, aincl, 31);
+    const int32_t aexcl = aincl - alen;
+    for (int32_t e0 = 0; e0 < atot; e0 += 32) {
+      const int32_t e = e0 + lane;
+      const int sl = warp_search(aincl, e);
+      const int32_t sas = __shfl_sync(kFull, as, sl);
+      const int32_t sax = __shfl_sync(kFull, aexcl, sl);
+      const int32_t* sacol = shfl_ptr(acol, sl);
+      const int32_t* strows = shfl_ptr(trows, sl);
+      const int32_t* sbci = shfl_ptr(bci, sl);
+      int32_t bs = 0, be = 0;
+      if (e < atot) {
+        const int32_t kc = __ldg(sacol + sas + (e - sax));
+        const int32_t* trow = strows + (int64_t)kc * (g.nfb + 1);
+        bs = __ldg(trow + fb_lo);
+        be = __ldg(trow + fb_hi);
+      }
+      const bool lng = be - bs >= 32;
+      if (!lng)
+        for (int32_t q = bs; q < be; q++) fs(__ldg(sbci + q));
+      unsigned longm = __ballot_sync(kFull, lng);
+      while (longm) {
+        const int src = __ffs(longm) - 1;
+        longm &= longm - 1;
+        const int32_t lb = __shfl_sync(kFull, bs, src), le = __shfl_sync(kFull, be, src);
+        const int32_t* lci = shfl_ptr(sbci, src);
+        for (int32_t q = lb + lane; q < le; q += 32) fs(__ldg(lci + q));
+      }
+    }
+  }
+}
+
 // ---- planning --------------------------------------------------------------------
 
 // Per row: intermediate products; light/heavy classification into two lists.
 // One warp per row: one lane per stage reads the A-row segment, then the
 // flattened entries are read 32 at a time.
+// With FEATURES it also writes, per row, the predictor's five features
+// X[ri*5 + 0..4] = log2(1 + A-row nnz over all stages), log2(1 + products),
+// log2(1 + longest referenced B row), (i + 1/2)/grid_m, (j + 1/2)/grid_n,
+// and the row's product count (capped at 2^31-1) to ub_out[ri].
+template <bool FEATURES>
 __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restrict__ light_list,
                            int32_t* __restrict__ heavy_list, int32_t* __restrict__ vheavy_list,
                            int32_t* __restrict__ counters, unsigned long long* __restrict__ products,
-                           int heavy_min_cols) {
+                           int heavy_min_cols, float* __restrict__ X, int32_t* __restrict__ ub_out) {
   const int lane = lane_id();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long mine = 0;
   for (int64_t ri = warp; ri < g.n_row_items; ri += nwarps) {
     const RowInfo x = decode_row(g, ri);
-    int64_t tot = 0;
+    int64_t tot = 0, annz = 0;
+    int32_t bmax = 0;
     if (x.r < A.rows_of(x.ti)) {
       for (int g0 = 0; g0 < g.gk; g0 += 32) {
         const int kk = g0 + lane;
@@ -348,11 +408,27 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
           const int32_t* sbrp = shfl_ptr(brp, sl);
           if (e < atot) {
             const int32_t kc = __ldg(sacol + sas + (e - sax));
-            tot += __ldg(sbrp + kc + 1) - __ldg(sbrp + kc);
+            const int32_t bl = __ldg(sbrp + kc + 1) - __ldg(sbrp + kc);
+            tot += bl;
+            if (FEATURES) bmax = max(bmax, bl);
           }
         }
+        if (FEATURES) annz += atot;
       }
       tot = warp_sum(tot);
+      if (FEATURES) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) bmax = max(bmax, __shfl_xor_sync(kFull, bmax, d));
+      }
+    }
+    if (FEATURES && lane == 0) {
+      float* xr = X + ri * 5;
+      xr[0] = log2f(1.f + (float)annz);
+      xr[1] = log2f(1.f + (float)tot);
+      xr[2] = log2f(1.f + (float)bmax);
+      xr[3] = ((float)x.ti + 0.5f) / (float)g.gm;
+      xr[4] = ((float)x.tj + 0.5f) / (float)g.gn;
+      ub_out[ri] = (int32_t)(tot < INT32_MAX ? tot : INT32_MAX);
     }
     if (lane == 0 && tot > 0) {
       mine += (unsigned long long)tot;
@@ -536,10 +612,17 @@ struct WarpSmem {
   int32_t ss[32];
 };
 
-template <typename VT, int WORDS>
 #ifndef BCLX_NUMERIC_MIN_BLOCKS
 #define BCLX_NUMERIC_MIN_BLOCKS 4
 #endif
+// LEARNED: the learned product's single pass.  Heavy items come from the
+// predicted cut (their counts are unknown): each builds its bitmap from its
+// own products, and an item with more than kVcap outputs marks its row in
+// row_failed and stops (that row is redone by the exact path).  Outputs go
+// to temp slots (light row l at light_slot[l], heavy item idx at
+// heavy_slot_base + idx*kVcap, after all light slots),
+// counts to item_count / row_count_w.
+template <typename VT, int WORDS, bool LEARNED>
 __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     k_numeric(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
               const int32_t* __restrict__ heavy_list, int n_light, int64_t n_heavy_items,
@@ -547,7 +630,9 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
               const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, const int32_t* __restrict__ tab,
               const int32_t* __restrict__ row_count, const int64_t* __restrict__ row_offset,
               int32_t* __restrict__ out_col, VT* __restrict__ out_val, int s0, int s1,
-              unsigned long long* __restrict__ queue, int grab, int long_seg) {
+              unsigned long long* __restrict__ queue, int grab, int long_seg,
+              const int64_t* __restrict__ light_slot, int32_t* __restrict__ item_count,
+              int32_t* __restrict__ row_count_w, int32_t* __restrict__ row_failed, int64_t heavy_slot_base) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem<VT, WORDS>& S = reinterpret_cast<WarpSmem<VT, WORDS>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = lane_id();
@@ -567,21 +652,30 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     // heavy items first (they are the larger ones)
     const bool heavy = idx < n_heavy_items;
     int64_t ri;
-    int cnt, fb_lo = 0, fb_hi = 0, lo = 0, hi;
+    int cnt = 0, fb_lo = 0, fb_hi = 0, lo = 0, hi, hslot = 0;
     int64_t off;
     const uint32_t* hb = nullptr;
     if (heavy) {
       const HeavyItem it = heavy_items[idx];
       ri = heavy_list[it.h];
-      cnt = it.count;
+      hslot = it.h;
       fb_lo = it.fb_lo;
       fb_hi = it.fb_hi;
-      off = row_offset[ri] + it.rel;
-      hb = heavy_bitmaps + (int64_t)it.h * hbm_words;
+      if (LEARNED) {
+        off = heavy_slot_base + idx * kVcap;
+      } else {
+        cnt = it.count;
+        off = row_offset[ri] + it.rel;
+        hb = heavy_bitmaps + (int64_t)it.h * hbm_words;
+      }
     } else {
       ri = light_list[idx - n_heavy_items];
-      cnt = row_count[ri];
-      off = row_offset[ri];
+      if (LEARNED) {
+        off = light_slot[idx - n_heavy_items];
+      } else {
+        cnt = row_count[ri];
+        off = row_offset[ri];
+      }
     }
     const RowInfo x = decode_row(g, ri);
     if (heavy) {
@@ -594,7 +688,14 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     const int words = ((hi - lo) + 31) >> 5;
 
     // 1. column bitmap of the item (word w covers columns lo + 32w ..)
-    if (heavy) {
+    if (heavy && LEARNED) {
+      for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
+      __syncwarp();
+      walk_columns_ranged(A, B, g, x, fb_lo, fb_hi, tab, [&](int32_t j) {
+        const int xx = j - lo;
+        atomicOr(&S.bm[xx >> 5], 1u << (xx & 31));
+      });
+    } else if (heavy) {
       for (int w = lane; w < words; w += 32) S.bm[w] = __ldg(hb + w0 + w);
     } else {
       for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
@@ -616,13 +717,29 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
       const int wa = lane * per;
       int loc = 0;
       for (int w = wa; w < wa + per && w < words; w++) loc += __popc(S.bm[w]);
-      int ex = warp_inclusive_scan(loc) - loc;
+      const int inc = warp_inclusive_scan(loc);
+      int ex = inc - loc;
       for (int w = wa; w < wa + per && w < words; w++) {
         S.pre[w] = (uint16_t)ex;
         ex += __popc(S.bm[w]);
       }
+      if (LEARNED) cnt = __shfl_sync(kFull, inc, 31);
     }
     __syncwarp();
+    if (LEARNED) {
+      if (heavy && cnt > kVcap) {  // the prediction cut this item too wide
+        if (lane == 0) row_failed[hslot] = 1;
+        continue;
+      }
+      if (lane == 0) {
+        if (heavy) {
+          item_count[idx] = cnt;
+          atomicAdd(&row_count_w[ri], cnt);
+        } else {
+          row_count_w[ri] = cnt;
+        }
+      }
+    }
 
     // 3. sorted columns (first stage range only) and the accumulators
     if (s0 == 0) {
@@ -718,6 +835,163 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
   }
 }
 
+// ---- learned product ---------------------------------------------------------------------
+
+constexpr float kLearnTarget = 320.f;  // outputs aimed at per heavy item (the accumulator holds 512)
+constexpr float kLearnMargin = 1.15f;  // head room on the predicted count
+
+// Products of every heavy row per fine column block: bub[h*nfb + b] (one warp
+// per heavy row, lanes over blocks, the A entries of all stages in turn).
+__global__ void k_heavy_block_ub(SpGridView A, Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
+                                 const int32_t* __restrict__ tab, int32_t* __restrict__ bub) {
+  const int lane = lane_id();
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int nfb = (int)g.nfb;
+  for (int64_t h = warp; h < n_heavy; h += nwarps) {
+    const RowInfo x = decode_row(g, heavy_list[h]);
+    int32_t acc0 = 0, acc1 = 0;  // blocks lane and lane + 32 (nfb <= 64)
+    for (int64_t k = 0; k < g.gk; k++) {
+      const bclx_csr_t At = A.tile(x.ti, k);
+      const int32_t a0 = __ldg(At.row_ptr + x.r), a1 = __ldg(At.row_ptr + x.r + 1);
+      const int32_t* trows = tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1);
+      for (int32_t c0 = a0; c0 < a1; c0 += 32) {
+        const int32_t kc_l = c0 + lane < a1 ? __ldg(At.col_ind + c0 + lane) : 0;
+        const int ne = min(32, a1 - c0);
+        for (int e = 0; e < ne; e++) {
+          const int32_t kc = __shfl_sync(kFull, kc_l, e);
+          const int32_t* trow = trows + (int64_t)kc * (g.nfb + 1);
+          if (lane < nfb) acc0 += __ldg(trow + lane + 1) - __ldg(trow + lane);
+          if (lane + 32 < nfb) acc1 += __ldg(trow + lane + 33) - __ldg(trow + lane + 32);
+        }
+      }
+    }
+    if (lane < nfb) bub[h * nfb + lane] = acc0;
+    if (lane + 32 < nfb) bub[h * nfb + lane + 32] = acc1;
+  }
+}
+
+// Heavy rows cut into fine-block ranges of about kLearnTarget expected
+// outputs, greedy left to right.  A block of width w receiving p products is
+// expected to hold w*(1 - exp(-p/w)) distinct columns (p products spread over
+// w columns); the network's predicted row count (pred = log2(1 + count))
+// rescales these block estimates so that they add up to the prediction.
+// Without a network a block's product count (capped at its width) is used:
+// an upper bound, so no item can overflow.  FILL = false counts the items,
+// FILL = true writes them.
+template <bool FILL>
+__global__ void k_learned_cut(Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
+                              const float* __restrict__ pred, const int32_t* __restrict__ ub,
+                              const int32_t* __restrict__ bub, int32_t* __restrict__ n_items,
+                              const int64_t* __restrict__ first, HeavyItem* __restrict__ items) {
+  const int nfb_g = (int)g.nfb;
+  for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n_heavy; h += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ri = heavy_list[h];
+    const RowInfo x = decode_row(g, ri);
+    const int nfb = (x.w + kFineCols - 1) / kFineCols;
+    const int32_t* bu = bub + h * nfb_g;
+    float kappa = 1.f;
+    if (pred) {
+      float est = 0.f;
+      for (int b = 0; b < nfb; b++) {
+        const float w = (float)min(kFineCols, x.w - b * kFineCols);
+        est += w * (1.f - __expf(-(float)bu[b] / w));
+      }
+      const float c = exp2f(pred[ri]) - 1.f;
+      kappa = fminf(fmaxf(c * kLearnMargin / fmaxf(est, 1.f), 0.25f), 4.f);
+    }
+    int n = 0, start = 0;
+    float cur = 0.f;
+    int64_t out = FILL ? first[h] : 0;
+    for (int b = 0; b < nfb; b++) {
+      const float w = (float)min(kFineCols, x.w - b * kFineCols);
+      const float p = (float)bu[b];
+      const float e = pred ? fminf(w, kappa * w * (1.f - __expf(-p / w))) : fminf(w, p);
+      if (b > start && cur + e > kLearnTarget) {
+        if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)b, 0, 0};
+        n++;
+        start = b;
+        cur = 0.f;
+      }
+      cur += e;
+    }
+    if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)nfb, 0, 0};
+    n++;
+    if (!FILL) n_items[h] = n;
+  }
+}
+
+__global__ void k_gather_ub(const int32_t* __restrict__ list, int n, const int32_t* __restrict__ ub,
+                            int32_t* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = ub[list[i]];
+}
+
+// Failed heavy rows -> their row indices, and their heavy-list slots marked.
+__global__ void k_collect_failed(const int32_t* __restrict__ heavy_list, int n_heavy,
+                                 const int32_t* __restrict__ row_failed, int32_t* __restrict__ failed_list,
+                                 int32_t* __restrict__ n_failed) {
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < n_heavy; h += gridDim.x * blockDim.x)
+    if (row_failed[h]) failed_list[atomicAdd(n_failed, 1)] = heavy_list[h];
+}
+
+__global__ void k_take_counts(const int32_t* __restrict__ failed_list, int n_failed,
+                              const int32_t* __restrict__ redo_count, int32_t* __restrict__ row_count) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n_failed; f += gridDim.x * blockDim.x) {
+    const int ri = failed_list[f];
+    row_count[ri] = redo_count[ri];
+  }
+}
+
+// Compaction into the final CSR: one warp per light row, heavy item (of a row
+// that did not fail) and failed row; lanes copy the contiguous run.
+template <typename VT>
+__global__ void k_compact(Geom g, const int32_t* __restrict__ light_list, int n_light,
+                          const int64_t* __restrict__ light_slot, const int32_t* __restrict__ heavy_list,
+                          const HeavyItem* __restrict__ items, int64_t n_items, const int64_t* __restrict__ first,
+                          const int32_t* __restrict__ item_count, const int64_t* __restrict__ item_pos,
+                          const int32_t* __restrict__ row_failed, const int32_t* __restrict__ failed_list,
+                          int n_failed, int64_t heavy_slot_base, const int64_t* __restrict__ redo_off,
+                          const int32_t* __restrict__ row_count,
+                          const int64_t* __restrict__ row_offset, const int32_t* __restrict__ tcol,
+                          const VT* __restrict__ tval, const int32_t* __restrict__ rcol, const VT* __restrict__ rval,
+                          int32_t* __restrict__ out_col, VT* __restrict__ out_val) {
+  const int lane = lane_id();
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t total = (int64_t)n_light + n_items + n_failed;
+  for (int64_t u = warp; u < total; u += nwarps) {
+    int64_t src, dst;
+    int cnt;
+    const int32_t* sc = tcol;
+    const VT* sv = tval;
+    if (u < n_light) {
+      const int ri = light_list[u];
+      src = light_slot[u];
+      dst = row_offset[ri];
+      cnt = row_count[ri];
+    } else if (u < n_light + n_items) {
+      const int64_t idx = u - n_light;
+      const HeavyItem it = items[idx];
+      if (row_failed[it.h]) continue;
+      const int ri = heavy_list[it.h];
+      src = heavy_slot_base + idx * kVcap;
+      dst = row_offset[ri] + (item_pos[idx] - item_pos[first[it.h]]);
+      cnt = item_count[idx];
+    } else {
+      const int ri = failed_list[u - n_light - n_items];
+      src = redo_off[ri];
+      dst = row_offset[ri];
+      cnt = row_count[ri];
+      sc = rcol;
+      sv = rval;
+    }
+    for (int q = lane; q < cnt; q += 32) {
+      out_col[dst + q] = sc[src + q];
+      out_val[dst + q] = sv[src + q];
+    }
+  }
+}
+
 // ---- identity tiles (tile accumulation as a product) ------------------------------
 
 template <typename VT>
@@ -766,6 +1040,25 @@ struct bclx_spgemm_plan_s {
   const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaStream_t gstream = nullptr;  // capture/replay stream (the caller's may be the legacy default stream)
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // learned product (bclx_spgemm_learned_run / _finish)
+  bool learned = false;
+  float* feat = nullptr;            // [nri*5]
+  int32_t* ub = nullptr;            // [nri]
+  float* pred = nullptr;            // [nri]
+  int64_t* light_slot = nullptr;    // [n_light+1]
+  int32_t* light_ub = nullptr;      // [n_light]
+  int32_t* item_count = nullptr;    // [n_heavy_items]
+  int64_t* item_pos = nullptr;      // [n_heavy_items+1]
+  int32_t* row_failed = nullptr;    // [n_heavy]
+  int32_t* block_ub = nullptr;      // [n_heavy*nfb] products per fine block
+  int32_t* failed_list = nullptr;   // [n_heavy] row indices of failed rows
+  int32_t* temp_col = nullptr;
+  void* temp_val = nullptr;
+  int64_t temp_entries = 0, n_failed = 0, heavy_slot_base = 0;
+  bclx_spgemm_plan_s* redo = nullptr;  // exact plan over the failed rows
+  int64_t* redo_off = nullptr;         // [nri+1]
+  int32_t* redo_col = nullptr;
+  void* redo_val = nullptr;
   // tile accumulation: identity A tiles and their descriptors, 1x1 C offsets
   int32_t* id_rp = nullptr;
   int32_t* id_ci = nullptr;
@@ -786,6 +1079,23 @@ struct bclx_spgemm_plan_s {
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
     ev_in = ev_out = nullptr;
+    if (redo) {
+      redo->heavy_list = nullptr;  // borrowed from this plan
+      redo->light_list = nullptr;
+      redo->row_offset = nullptr;
+      redo->tab = nullptr;
+      redo->release();
+      delete redo;
+      redo = nullptr;
+    }
+    void* lp[] = {feat, ub, pred, light_slot, light_ub, item_count, item_pos, row_failed, block_ub, failed_list,
+                  temp_col,
+                  temp_val, redo_off, redo_col, redo_val};
+    for (void* p : lp) scratch_free(ctx, p);
+    feat = pred = nullptr;
+    ub = light_ub = item_count = row_failed = block_ub = failed_list = temp_col = redo_col = nullptr;
+    light_slot = item_pos = redo_off = nullptr;
+    temp_val = redo_val = nullptr;
     void* ps[] = {queue, light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
                   heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset};
     for (void* p : ps) scratch_free(ctx, p);
@@ -854,11 +1164,11 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
   return BCLX_OK;
 }
 
-template <typename VT, int WORDS>
+template <typename VT, int WORDS, bool LEARNED = false>
 static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P,
                             int32_t* out_col, void* out_val, int s0, int s1) {
   constexpr size_t smem = sizeof(WarpSmem<VT, WORDS>) * kWarpsNum;
-  auto kern = k_numeric<VT, WORDS>;
+  auto kern = k_numeric<VT, WORDS, LEARNED>;
   static std::atomic<unsigned long long> configured{0};  // one bit per device
   const unsigned long long bit = 1ull << (ctx->device & 63);
   if (!(configured.load() & bit)) {
@@ -872,7 +1182,9 @@ static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView&
   kern<<<grid_for(ctx, n_total, kWarpsNum, bps), kWarpsNum * 32, smem, ctx->stream>>>(
       A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, P->n_heavy_items, P->heavy_items, P->heavy_bitmaps,
       P->hbm_words, P->tab, P->row_count, P->row_offset, out_col, reinterpret_cast<VT*>(out_val), s0, s1, q,
-      P->grab < 1 ? 1 : P->grab, P->long_seg < 1 ? 1 : P->long_seg);
+      P->grab < 1 ? 1 : P->grab, P->long_seg < 1 ? 1 : P->long_seg, LEARNED ? P->light_slot : nullptr,
+      LEARNED ? P->item_count : nullptr, LEARNED ? P->row_count : nullptr, LEARNED ? P->row_failed : nullptr,
+      P->heavy_slot_base);
   note_launch();
   BCLX_CK_LAUNCH();
   return BCLX_OK;
@@ -907,9 +1219,9 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   // rows of tiles wider than 8192 columns always take the block path
   const int heavy_min_cols = 8192 + 1;
   if (nri > 0) {
-    k_classify<<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P->light_list, P->heavy_tmp,
-                                                                   P->vheavy_list, P->counters, P->products_dev,
-                                                                   heavy_min_cols);
+    k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
+        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, heavy_min_cols, nullptr,
+        nullptr);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1310,8 +1622,8 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
   BCLX_CK(cudaMemsetAsync(P.counters, 0, 4 * sizeof(int32_t), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P.products_dev, 0, sizeof(unsigned long long), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P.row_count, 0, sizeof(int32_t) * nri, ctx->stream));
-  k_classify<<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P.light_list, P.heavy_tmp, P.vheavy_list,
-                                                                 P.counters, P.products_dev, 8192 + 1);
+  k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
+      A, B, g, P.light_list, P.heavy_tmp, P.vheavy_list, P.counters, P.products_dev, 8192 + 1, nullptr, nullptr);
   note_launch();
   BCLX_CK_LAUNCH();
   int32_t cnts[4];
@@ -1422,3 +1734,317 @@ extern "C" int bclx_spgemm_tile_noalloc(const bclx_csr_t* a, const bclx_csr_t* b
   ScratchArena ar{reinterpret_cast<unsigned char*>(base), kNoAllocScratchBytes};
   return noalloc_product(&ctx, ar, a, b, c_row_ptr, c_col_ind, c_vals, c_capacity, c_nnz);
 }
+
+// ---- learned product: orchestration ---------------------------------------------------
+
+namespace bclx {
+
+template <typename VT>
+static int learned_numeric(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P) {
+  if (P->g.tn <= 8192) return launch_numeric_w<VT, 256, true>(ctx, A, B, P, P->temp_col, P->temp_val, 0, (int)P->g.gk);
+  return launch_numeric_w<VT, kMaxWords, true>(ctx, A, B, P, P->temp_col, P->temp_val, 0, (int)P->g.gk);
+}
+
+template <typename VT>
+static int exact_numeric_into(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* R,
+                              int32_t* col, void* val) {
+  if (R->g.tn <= 8192) return launch_numeric_w<VT, 256>(ctx, A, B, R, col, val, 0, (int)R->g.gk);
+  return launch_numeric_w<VT, kMaxWords>(ctx, A, B, R, col, val, 0, (int)R->g.gk);
+}
+
+// Everything up to the final offsets: predict, cut, one numeric pass into
+// temp slots, redo the failed rows exactly, row offsets.  nnz in P->nnz.
+static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, const Geom& g, int dtype,
+                        const float* params, int32_t* tile_row_ptr, int64_t* tile_offset, bclx_spgemm_plan_s* P) {
+  P->learned = true;
+  P->g = g;
+  P->dtype = dtype;
+  P->hbm_words = (g.tn + 31) / 32;
+  const int64_t nri = g.n_row_items;
+  BCLX_TRY(scratch_alloc_n(ctx, &P->light_list, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_list, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->vheavy_list, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_tmp, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->counters, 4));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->products_dev, 1));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->row_count, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->row_offset, nri + 1));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->queue, kQueueSlots));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->feat, (size_t)nri * 5));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->ub, nri));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->pred, nri));
+  BCLX_CK(cudaMemsetAsync(P->counters, 0, 4 * sizeof(int32_t), ctx->stream));
+  BCLX_CK(cudaMemsetAsync(P->products_dev, 0, sizeof(unsigned long long), ctx->stream));
+  BCLX_CK(cudaMemsetAsync(P->row_count, 0, sizeof(int32_t) * (nri > 0 ? nri : 1), ctx->stream));
+  if (nri > 0) {
+    k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
+        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, 8192 + 1, P->feat, P->ub);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+  int32_t cnts[4];
+  int64_t prod = 0;
+  BCLX_CK(cudaMemcpyAsync(cnts, P->counters, sizeof(cnts), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(&prod, P->products_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
+  P->n_light = cnts[0];
+  P->n_vheavy = 0;  // the learned cut treats every heavy row alike
+  P->n_heavy = cnts[1] + cnts[3];
+  P->products = prod;
+  if (cnts[3] > 0)
+    BCLX_CK(cudaMemcpyAsync(P->heavy_list, P->vheavy_list, sizeof(int32_t) * cnts[3], cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+  if (cnts[1] > 0)
+    BCLX_CK(cudaMemcpyAsync(P->heavy_list + cnts[3], P->heavy_tmp, sizeof(int32_t) * cnts[1],
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+  if (params && P->n_heavy > 0)
+    BCLX_TRY(bclx_mlp_predict(reinterpret_cast<bclx_context_t>(ctx), P->feat, nri, params, P->pred));
+
+  // heavy rows: predicted cut; light rows: slots of their product count
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_nitems, P->n_heavy));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_first, P->n_heavy + 1));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->light_ub, P->n_light));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->light_slot, P->n_light + 1));
+  const unsigned hb = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
+  if (P->n_heavy > 0) {
+    const int64_t nbrows = g.gk * g.gn * g.tk;
+    BCLX_TRY(scratch_alloc_n(ctx, &P->tab, (size_t)nbrows * (g.nfb + 1)));
+    k_btable<<<grid_for(ctx, nbrows / 32 + 1, 8, 16), 256, 0, ctx->stream>>>(B, g, P->tab);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    BCLX_TRY(scratch_alloc_n(ctx, &P->block_ub, (size_t)P->n_heavy * g.nfb));
+    k_heavy_block_ub<<<grid_for(ctx, P->n_heavy, 8, 8), 256, 0, ctx->stream>>>(A, g, P->heavy_list,
+                                                                               (int)P->n_heavy, P->tab, P->block_ub);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    k_learned_cut<false><<<hb, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, params ? P->pred : nullptr,
+                                                      P->ub, P->block_ub, P->heavy_nitems, nullptr, nullptr);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+  BCLX_TRY(exclusive_scan_i32(ctx, P->heavy_nitems, P->heavy_first, P->n_heavy));
+  if (P->n_light > 0) {
+    k_gather_ub<<<grid_for(ctx, P->n_light / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(P->light_list, (int)P->n_light,
+                                                                                    P->ub, P->light_ub);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+  BCLX_TRY(exclusive_scan_i32(ctx, P->light_ub, P->light_slot, P->n_light));
+  int64_t tails[2];
+  BCLX_CK(cudaMemcpyAsync(&tails[0], P->heavy_first + P->n_heavy, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(&tails[1], P->light_slot + P->n_light, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
+  P->n_heavy_items = tails[0];
+  const int64_t light_total = tails[1];
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_items, P->n_heavy_items));
+  if (P->n_heavy > 0) {
+    k_learned_cut<true><<<hb, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, params ? P->pred : nullptr,
+                                                     P->ub, P->block_ub, nullptr, P->heavy_first, P->heavy_items);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+
+  // one numeric pass into temp slots
+  P->heavy_slot_base = light_total;  // heavy item slots follow the light rows' slots
+  P->temp_entries = light_total + P->n_heavy_items * (int64_t)kVcap;
+  BCLX_TRY(scratch_alloc_n(ctx, &P->temp_col, P->temp_entries));
+  BCLX_TRY(scratch_alloc(ctx, &P->temp_val, 4 * (size_t)(P->temp_entries > 0 ? P->temp_entries : 1)));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->item_count, P->n_heavy_items));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->row_failed, P->n_heavy));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->failed_list, P->n_heavy));
+  BCLX_CK(cudaMemsetAsync(P->item_count, 0, sizeof(int32_t) * (P->n_heavy_items > 0 ? P->n_heavy_items : 1),
+                          ctx->stream));
+  BCLX_CK(cudaMemsetAsync(P->row_failed, 0, sizeof(int32_t) * (P->n_heavy > 0 ? P->n_heavy : 1), ctx->stream));
+  if (P->n_light + P->n_heavy_items > 0) {
+    if (dtype == BCLX_F32) BCLX_TRY(learned_numeric<float>(ctx, A, B, P));
+    else BCLX_TRY(learned_numeric<int32_t>(ctx, A, B, P));
+  }
+  BCLX_CK(cudaMemsetAsync(P->counters + 2, 0, sizeof(int32_t), ctx->stream));
+  if (P->n_heavy > 0) {
+    k_collect_failed<<<hb, 256, 0, ctx->stream>>>(P->heavy_list, (int)P->n_heavy, P->row_failed, P->failed_list,
+                                                  P->counters + 2);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+  int32_t nf = 0;
+  BCLX_CK(cudaMemcpyAsync(&nf, P->counters + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
+  P->n_failed = nf;
+
+  // the exact two-phase path for the failed rows (symbolic, cut, numeric)
+  if (nf > 0) {
+    auto* R = new bclx_spgemm_plan_s();
+    P->redo = R;
+    R->ctx = ctx;
+    R->g = g;
+    R->dtype = dtype;
+    R->hbm_words = P->hbm_words;
+    R->grab = P->grab;
+    R->blocks_per_sm = P->blocks_per_sm;
+    R->long_seg = P->long_seg;
+    R->heavy_list = P->failed_list;  // borrowed
+    R->light_list = P->light_list;   // borrowed (unused: no light rows)
+    R->n_light = 0;
+    R->n_vheavy = 0;
+    R->n_heavy = nf;
+    BCLX_TRY(scratch_alloc_n(ctx, &R->row_count, nri));
+    BCLX_TRY(scratch_alloc_n(ctx, &R->heavy_bitmaps, (size_t)nf * R->hbm_words));
+    BCLX_TRY(scratch_alloc_n(ctx, &R->heavy_nitems, nf));
+    BCLX_TRY(scratch_alloc_n(ctx, &R->heavy_first, nf + 1));
+    BCLX_TRY(scratch_alloc_n(ctx, &R->queue, kQueueSlots));
+    BCLX_TRY(scratch_alloc_n(ctx, &P->redo_off, nri + 1));
+    BCLX_CK(cudaMemsetAsync(R->row_count, 0, sizeof(int32_t) * nri, ctx->stream));
+    BCLX_TRY(launch_symbolic(ctx, A, B, R));
+    BCLX_TRY(exclusive_scan_i32(ctx, R->row_count, P->redo_off, nri));
+    R->row_offset = P->redo_off;  // borrowed
+    const unsigned rb = grid_for(ctx, nf / 32 + 1, 8, 8);
+    k_cut_heavy<false><<<rb, 256, 0, ctx->stream>>>(g, R->heavy_list, nf, R->heavy_bitmaps, R->hbm_words,
+                                                    R->heavy_nitems, nullptr, nullptr);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    BCLX_TRY(exclusive_scan_i32(ctx, R->heavy_nitems, R->heavy_first, nf));
+    int64_t rt[2];
+    BCLX_CK(cudaMemcpyAsync(&rt[0], R->heavy_first + nf, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    BCLX_CK(cudaMemcpyAsync(&rt[1], P->redo_off + nri, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    BCLX_CK(cudaStreamSynchronize(ctx->stream));
+    R->n_heavy_items = rt[0];
+    BCLX_TRY(scratch_alloc_n(ctx, &R->heavy_items, R->n_heavy_items));
+    k_cut_heavy<true><<<rb, 256, 0, ctx->stream>>>(g, R->heavy_list, nf, R->heavy_bitmaps, R->hbm_words, nullptr,
+                                                   R->heavy_first, R->heavy_items);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    R->tab = P->tab;  // borrowed
+    BCLX_TRY(scratch_alloc_n(ctx, &P->redo_col, rt[1]));
+    BCLX_TRY(scratch_alloc(ctx, &P->redo_val, 4 * (size_t)(rt[1] > 0 ? rt[1] : 1)));
+    if (R->n_heavy_items > 0) {
+      if (dtype == BCLX_F32) BCLX_TRY(exact_numeric_into<float>(ctx, A, B, R, P->redo_col, P->redo_val));
+      else BCLX_TRY(exact_numeric_into<int32_t>(ctx, A, B, R, P->redo_col, P->redo_val));
+    }
+    k_take_counts<<<rb, 256, 0, ctx->stream>>>(P->failed_list, nf, R->row_count, P->row_count);
+    note_launch();
+    BCLX_CK_LAUNCH();
+  }
+
+  // final row offsets and the C tile pointers (counters[3] becomes the overflow flag)
+  BCLX_TRY(exclusive_scan_i32(ctx, P->row_count, P->row_offset, nri));
+  BCLX_CK(cudaMemsetAsync(P->counters + 3, 0, sizeof(int32_t), ctx->stream));
+  const int64_t ntiles = g.gm * g.gn;
+  k_tile_ptrs<<<grid_for(ctx, ntiles * (g.tm + 1) / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
+      g, P->row_offset, tile_row_ptr, tile_offset, P->counters + 3);
+  note_launch();
+  BCLX_CK_LAUNCH();
+  BCLX_TRY(scratch_alloc_n(ctx, &P->item_pos, P->n_heavy_items + 1));
+  BCLX_TRY(exclusive_scan_i32(ctx, P->item_count, P->item_pos, P->n_heavy_items));
+  int64_t nnz = 0;
+  int32_t ovf = 0;
+  BCLX_CK(cudaMemcpyAsync(&nnz, P->row_offset + nri, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaMemcpyAsync(&ovf, P->counters + 3, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
+  if (ovf) {
+    set_last_error("a C tile has more than 2^31-1 nonzeros; use a finer tile grid");
+    return BCLX_ERR_INDEX_OVERFLOW;
+  }
+  P->nnz = nnz;
+  return BCLX_OK;
+}
+
+template <typename VT>
+static int learned_finish_impl(Context* ctx, bclx_spgemm_plan_s* P, int32_t* out_col, void* out_val) {
+  const int64_t units = P->n_light + P->n_heavy_items + P->n_failed;
+  if (units == 0) return BCLX_OK;
+  k_compact<VT><<<grid_for(ctx, units, 8, 8), 256, 0, ctx->stream>>>(
+      P->g, P->light_list, (int)P->n_light, P->light_slot, P->heavy_list, P->heavy_items, P->n_heavy_items,
+      P->heavy_first, P->item_count, P->item_pos, P->row_failed, P->failed_list, (int)P->n_failed,
+      P->heavy_slot_base, P->redo_off,
+      P->row_count, P->row_offset, P->temp_col, reinterpret_cast<const VT*>(P->temp_val), P->redo_col,
+      reinterpret_cast<const VT*>(P->redo_val), out_col, reinterpret_cast<VT*>(out_val));
+  note_launch();
+  BCLX_CK_LAUNCH();
+  return BCLX_OK;
+}
+
+}  // namespace bclx
+
+extern "C" {
+
+int bclx_spgemm_learned_run(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b, bclx_spgrid_out_t* out,
+                            const float* mlp_params, bclx_spgemm_plan_t* plan, int64_t* nnz) {
+  Context* ctx = reinterpret_cast<Context*>(c);
+  if (!ctx || !plan || !nnz) return BCLX_ERR_INVALID;
+  *plan = nullptr;
+  BCLX_TRY(check_grids(a, b, out));
+  if (!out->tile_row_ptr || !out->tile_offset) return BCLX_ERR_INVALID;
+  BCLX_CK(cudaSetDevice(ctx->device));
+  auto* P = new bclx_spgemm_plan_s();
+  P->ctx = ctx;
+  int rc = learned_impl(ctx, make_view(*a), make_view(*b), make_geom(out, a->grid_n, a->tile_n), a->dtype, mlp_params,
+                        out->tile_row_ptr, out->tile_offset, P);
+  if (rc != BCLX_OK) {
+    P->release();
+    delete P;
+    return rc;
+  }
+  *nnz = P->nnz;
+  *plan = P;
+  return BCLX_OK;
+}
+
+int bclx_spgemm_learned_finish(bclx_context_t c, bclx_spgemm_plan_t P, bclx_spgrid_out_t* out) {
+  Context* ctx = reinterpret_cast<Context*>(c);
+  if (!ctx || !P || !out || !P->learned) return BCLX_ERR_INVALID;
+  if (P->nnz > 0 && (!out->col_ind || !out->vals)) return BCLX_ERR_INVALID;
+  BCLX_CK(cudaSetDevice(ctx->device));
+  if (P->dtype == BCLX_F32) return learned_finish_impl<float>(ctx, P, out->col_ind, out->vals);
+  return learned_finish_impl<int32_t>(ctx, P, out->col_ind, out->vals);
+}
+
+int bclx_spgemm_learned_stats(bclx_spgemm_plan_t P, int64_t* out6) {
+  if (!P || !out6 || !P->learned) return BCLX_ERR_INVALID;
+  out6[0] = P->n_heavy;
+  out6[1] = P->n_heavy_items;
+  out6[2] = P->n_failed;
+  out6[3] = P->temp_entries;
+  out6[4] = P->nnz;
+  out6[5] = P->redo ? P->redo->n_heavy_items : 0;
+  return BCLX_OK;
+}
+
+int bclx_spgemm_row_features(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b,
+                             const bclx_spgrid_out_t* out, float* X, int32_t* ub) {
+  Context* ctx = reinterpret_cast<Context*>(c);
+  if (!ctx || !X || !ub) return BCLX_ERR_INVALID;
+  BCLX_TRY(check_grids(a, b, out));
+  BCLX_CK(cudaSetDevice(ctx->device));
+  const Geom g = make_geom(out, a->grid_n, a->tile_n);
+  const int64_t nri = g.n_row_items;
+  if (nri == 0) return BCLX_OK;
+  int32_t* lists = nullptr;
+  int32_t* cnt = nullptr;
+  unsigned long long* prod = nullptr;
+  BCLX_TRY(scratch_alloc_n(ctx, &lists, 3 * (size_t)nri));
+  int rc = scratch_alloc_n(ctx, &cnt, 4);
+  if (rc == BCLX_OK) rc = scratch_alloc_n(ctx, &prod, 1);
+  if (rc == BCLX_OK) {
+    cudaMemsetAsync(cnt, 0, 4 * sizeof(int32_t), ctx->stream);
+    k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
+        make_view(*a), make_view(*b), g, lists, lists + nri, lists + 2 * nri, cnt, prod, 8192 + 1, X, ub);
+    note_launch();
+    if (cudaGetLastError() != cudaSuccess) rc = BCLX_ERR_CUDA;
+  }
+  scratch_free(ctx, lists);
+  scratch_free(ctx, cnt);
+  scratch_free(ctx, prod);
+  return rc;
+}
+
+int bclx_spgemm_plan_row_counts(bclx_spgemm_plan_t P, int32_t* counts) {
+  if (!P || !counts || !P->row_count) return BCLX_ERR_INVALID;
+  Context* ctx = P->ctx;
+  BCLX_CK(cudaMemcpyAsync(counts, P->row_count, sizeof(int32_t) * P->g.n_row_items, cudaMemcpyDeviceToDevice,
+                          ctx->stream));
+  return BCLX_OK;
+}
+
+}  // extern "C"

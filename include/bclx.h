@@ -183,6 +183,52 @@ BCLX_API int bclx_spgemm_plan_tune(bclx_spgemm_plan_t plan, int32_t grab, int32_
  * [3] work items in the large-accumulator class, [4] stages, [5] output nnz. */
 BCLX_API int bclx_spgemm_plan_stats(bclx_spgemm_plan_t plan, int64_t* out6);
 
+/* ---- learned product --------------------------------------------------------
+ * The same product without a separate symbolic pass: a row-nnz predictor
+ * (bclx_mlp_*) sizes the work.  run: classifies rows and computes their
+ * features, predicts each heavy row's output count, cuts heavy rows into
+ * column items from the prediction, runs one numeric pass that also builds
+ * every item's structure (outputs to plan-owned temp slots), redoes every row
+ * with an item whose real count exceeded the accumulator by the exact
+ * two-phase path, and writes c->tile_row_ptr / tile_offset and *nnz.  The
+ * caller then provides c->col_ind / c->vals and finish compacts the result
+ * into them.  Output bit-identical to bclx_spgemm_symbolic/_numeric.
+ * mlp_params: device array of bclx_mlp_num_params() floats, or NULL to size
+ * items from the product count (an upper bound) instead of a prediction.
+ * Destroy the plan with bclx_spgemm_plan_destroy.  No reference counterpart
+ * (the reference has no predictor); it replaces spgemm.hpp:182-242 as the
+ * symbolic/numeric pair does. */
+BCLX_API int bclx_spgemm_learned_run(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_spgrid_t* b,
+                                     bclx_spgrid_out_t* c, const float* mlp_params, bclx_spgemm_plan_t* plan,
+                                     int64_t* nnz);
+BCLX_API int bclx_spgemm_learned_finish(bclx_context_t ctx, bclx_spgemm_plan_t plan, bclx_spgrid_out_t* c);
+/* [0] heavy rows, [1] predicted heavy items, [2] rows redone exactly
+ * (mispredictions), [3] temp entries allocated, [4] nnz, [5] redo items. */
+BCLX_API int bclx_spgemm_learned_stats(bclx_spgemm_plan_t plan, int64_t* out6);
+/* Per C-tile row (grid_m*grid_n*tile_m rows, tile-major): the predictor's
+ * features X[row*5 + 0..4] (log2(1+A-row nnz), log2(1+products),
+ * log2(1+longest referenced B row), tile-row and tile-column coordinate in
+ * (0,1)) and the product count ub[row] (device arrays). */
+BCLX_API int bclx_spgemm_row_features(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_spgrid_t* b,
+                                      const bclx_spgrid_out_t* c, float* X, int32_t* ub);
+/* The exact per-row output counts of a symbolic plan (device array of
+ * grid_m*grid_n*tile_m int32): the predictor's training targets. */
+BCLX_API int bclx_spgemm_plan_row_counts(bclx_spgemm_plan_t plan, int32_t* counts);
+
+/* ---- row-nnz predictor: 5 -> 64 -> 64 -> 1 MLP (ReLU, FP32) -------------------
+ * No reference counterpart.  Parameters: device float array of
+ * bclx_mlp_num_params() values, layout W1[5][64] b1[64] W2[64][64] b2[64]
+ * w3[64] b3.  X: device [n][5]; y: device [n] targets log2(1 + row nnz). */
+BCLX_API int bclx_mlp_num_params(void);
+BCLX_API int bclx_mlp_predict(bclx_context_t ctx, const float* X, int64_t n, const float* params, float* out);
+/* grad[0..P) = dL/dparams of L = mean (yhat - y)^2, grad[P] = sum of squared errors. */
+BCLX_API int bclx_mlp_gradient(bclx_context_t ctx, const float* X, const float* y, int64_t n, const float* params,
+                               float* grad);
+/* `steps` full-batch Adam steps on (X, y) from `params` (updated in place);
+ * loss_host (host, may be NULL) receives the loss before each step. */
+BCLX_API int bclx_mlp_train(bclx_context_t ctx, const float* X, const float* y, int64_t n, float* params,
+                            int32_t steps, float lr, float* loss_host);
+
 /* ---- tile accumulation ---------------------------------------------------
  * C = parts[0] + parts[1] + ... (all m x n), per entry summed in list order
  * from 0, union structure (SparseHashAccumulator::get_matrix,
