@@ -840,34 +840,41 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
 constexpr float kLearnTarget = 320.f;  // outputs aimed at per heavy item (the accumulator holds 512)
 constexpr float kLearnMargin = 1.15f;  // head room on the predicted count
 
-// Products of every heavy row per fine column block: bub[h*nfb + b] (one warp
-// per heavy row, lanes over blocks, the A entries of all stages in turn).
-__global__ void k_heavy_block_ub(SpGridView A, Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
-                                 const int32_t* __restrict__ tab, int32_t* __restrict__ bub) {
+// Products of every heavy row per fine column block: bub[h*nfb + b].  One
+// warp per heavy row; lanes take A entries (all stages) and add each entry's
+// per-block segment lengths (from the B-row table) into shared counters.
+__global__ void __launch_bounds__(256) k_heavy_block_ub(SpGridView A, Geom g, const int32_t* __restrict__ heavy_list,
+                                                        int n_heavy, const int32_t* __restrict__ tab,
+                                                        int32_t* __restrict__ bub) {
+  __shared__ int32_t cnt_all[8][64];
+  int32_t* cnt = cnt_all[threadIdx.x >> 5];
   const int lane = lane_id();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int nfb = (int)g.nfb;
   for (int64_t h = warp; h < n_heavy; h += nwarps) {
     const RowInfo x = decode_row(g, heavy_list[h]);
-    int32_t acc0 = 0, acc1 = 0;  // blocks lane and lane + 32 (nfb <= 64)
+    cnt[lane] = 0;
+    cnt[lane + 32] = 0;
+    __syncwarp();
     for (int64_t k = 0; k < g.gk; k++) {
       const bclx_csr_t At = A.tile(x.ti, k);
       const int32_t a0 = __ldg(At.row_ptr + x.r), a1 = __ldg(At.row_ptr + x.r + 1);
       const int32_t* trows = tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1);
-      for (int32_t c0 = a0; c0 < a1; c0 += 32) {
-        const int32_t kc_l = c0 + lane < a1 ? __ldg(At.col_ind + c0 + lane) : 0;
-        const int ne = min(32, a1 - c0);
-        for (int e = 0; e < ne; e++) {
-          const int32_t kc = __shfl_sync(kFull, kc_l, e);
-          const int32_t* trow = trows + (int64_t)kc * (g.nfb + 1);
-          if (lane < nfb) acc0 += __ldg(trow + lane + 1) - __ldg(trow + lane);
-          if (lane + 32 < nfb) acc1 += __ldg(trow + lane + 33) - __ldg(trow + lane + 32);
+      for (int32_t p = a0 + lane; p < a1; p += 32) {
+        const int32_t* trow = trows + (int64_t)__ldg(At.col_ind + p) * (g.nfb + 1);
+        int32_t prev = __ldg(trow);
+        for (int b = 0; b < nfb; b++) {
+          const int32_t nx = __ldg(trow + b + 1);
+          if (nx != prev) atomicAdd(&cnt[b], nx - prev);
+          prev = nx;
         }
       }
     }
-    if (lane < nfb) bub[h * nfb + lane] = acc0;
-    if (lane + 32 < nfb) bub[h * nfb + lane + 32] = acc1;
+    __syncwarp();
+    if (lane < nfb) bub[h * nfb + lane] = cnt[lane];
+    if (lane + 32 < nfb) bub[h * nfb + lane + 32] = cnt[lane + 32];
+    __syncwarp();
   }
 }
 
@@ -919,6 +926,20 @@ __global__ void k_learned_cut(Geom g, const int32_t* __restrict__ heavy_list, in
     n++;
     if (!FILL) n_items[h] = n;
   }
+}
+
+__global__ void k_gather_features(const int32_t* __restrict__ list, int n, const float* __restrict__ feat,
+                                  float* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int64_t ri = list[i];
+#pragma unroll
+    for (int f = 0; f < 5; f++) out[(int64_t)i * 5 + f] = feat[ri * 5 + f];
+  }
+}
+
+__global__ void k_scatter_pred(const int32_t* __restrict__ list, int n, const float* __restrict__ pred_in,
+                               float* __restrict__ pred) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) pred[list[i]] = pred_in[i];
 }
 
 __global__ void k_gather_ub(const int32_t* __restrict__ list, int n, const int32_t* __restrict__ ub,
@@ -1797,8 +1818,23 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   if (cnts[1] > 0)
     BCLX_CK(cudaMemcpyAsync(P->heavy_list + cnts[3], P->heavy_tmp, sizeof(int32_t) * cnts[1],
                             cudaMemcpyDeviceToDevice, ctx->stream));
-  if (params && P->n_heavy > 0)
-    BCLX_TRY(bclx_mlp_predict(reinterpret_cast<bclx_context_t>(ctx), P->feat, nri, params, P->pred));
+  if (params && P->n_heavy > 0) {
+    // predictions are needed for the heavy rows only
+    float* hx = nullptr;
+    BCLX_TRY(scratch_alloc_n(ctx, &hx, (size_t)P->n_heavy * 6));
+    k_gather_features<<<grid_for(ctx, P->n_heavy / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
+        P->heavy_list, (int)P->n_heavy, P->feat, hx);
+    note_launch();
+    int rc = bclx_mlp_predict(reinterpret_cast<bclx_context_t>(ctx), hx, P->n_heavy, params, hx + 5 * P->n_heavy);
+    if (rc == BCLX_OK) {
+      k_scatter_pred<<<grid_for(ctx, P->n_heavy / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
+          P->heavy_list, (int)P->n_heavy, hx + 5 * P->n_heavy, P->pred);
+      note_launch();
+    }
+    scratch_free(ctx, hx);
+    BCLX_TRY(rc);
+    BCLX_CK_LAUNCH();
+  }
 
   // heavy rows: predicted cut; light rows: slots of their product count
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_nitems, P->n_heavy));
@@ -1813,7 +1849,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
     note_launch();
     BCLX_CK_LAUNCH();
     BCLX_TRY(scratch_alloc_n(ctx, &P->block_ub, (size_t)P->n_heavy * g.nfb));
-    k_heavy_block_ub<<<grid_for(ctx, P->n_heavy, 8, 8), 256, 0, ctx->stream>>>(A, g, P->heavy_list,
+    k_heavy_block_ub<<<grid_for(ctx, P->n_heavy, 8, 16), 256, 0, ctx->stream>>>(A, g, P->heavy_list,
                                                                                (int)P->n_heavy, P->tab, P->block_ub);
     note_launch();
     BCLX_CK_LAUNCH();
