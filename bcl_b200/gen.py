@@ -67,6 +67,17 @@ def _csr_from_sorted_keys(keys: np.ndarray, m: int, n: int, vals: np.ndarray) ->
     return CSR(m, n, row_ptr.astype(np.int32), cols, vals)
 
 
+def _sorted_unique(keys: np.ndarray) -> np.ndarray:
+    """Sorted distinct values (np.unique, without its slow path on large int64 arrays)."""
+    keys.sort()
+    if keys.size == 0:
+        return keys
+    keep = np.empty(keys.size, dtype=bool)
+    keep[0] = True
+    np.not_equal(keys[1:], keys[:-1], out=keep[1:])
+    return keys[keep]
+
+
 def _values(rng: np.random.Generator, count: int, value_type: str) -> np.ndarray:
     if value_type == "f32":
         return rng.uniform(-1.0, 1.0, count).astype(np.float32)
@@ -89,19 +100,26 @@ def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c:
     rng = np.random.default_rng(seed)
     keys = np.empty(n_edges, dtype=np.int64)
     ab, abc = a + b, a + b + c
+    r = np.empty(chunk, dtype=np.float64)
+    m1 = np.empty(chunk, dtype=bool)
+    m2 = np.empty(chunk, dtype=bool)
     for start in range(0, n_edges, chunk):
         cnt = min(chunk, n_edges - start)
         rows = np.zeros(cnt, dtype=np.int64)
         cols = np.zeros(cnt, dtype=np.int64)
+        rr, d, rt = r[:cnt], m1[:cnt], m2[:cnt]
         for level in range(scale):
-            r = rng.random(cnt)
+            rng.random(out=rr)
             bit = np.int64(1) << np.int64(scale - 1 - level)
-            down = r >= ab
-            right = ((r >= a) & (r < ab)) | (r >= abc)
-            rows |= down.astype(np.int64) * bit
-            cols |= right.astype(np.int64) * bit
+            # quadrant: [0,a) top-left, [a,a+b) top-right, [a+b,a+b+c) bottom-left, rest bottom-right
+            np.greater_equal(rr, ab, out=d)
+            np.add(rows, bit, out=rows, where=d)
+            np.greater_equal(rr, a, out=rt)
+            rt &= ~d
+            rt |= rr >= abc
+            np.add(cols, bit, out=cols, where=rt)
         keys[start:start + cnt] = rows * n + cols
-    keys = np.unique(keys)
+    keys = _sorted_unique(keys)
     return _csr_from_sorted_keys(keys, n, n, _values(rng, keys.size, value_type))
 
 
