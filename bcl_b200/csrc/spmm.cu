@@ -41,6 +41,10 @@ struct Vec<float> {
   }
   __device__ __forceinline__ static float to_f(float x) { return x; }
   __device__ __forceinline__ static float from_f(float x) { return x; }
+  __device__ __forceinline__ static void unpack_raw(uint4 v, float* out) {
+    out[0] = __uint_as_float(v.x); out[1] = __uint_as_float(v.y);
+    out[2] = __uint_as_float(v.z); out[3] = __uint_as_float(v.w);
+  }
 };
 
 template <>
@@ -72,95 +76,192 @@ struct Vec<__nv_bfloat16> {
   }
   __device__ __forceinline__ static float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
   __device__ __forceinline__ static __nv_bfloat16 from_f(float x) { return __float2bfloat16_rn(x); }
+  __device__ __forceinline__ static void unpack_raw(uint4 v, float* out) { unpack(v, out); }
 };
 
-// One (C row, panel) with all loads of B and C as 16-byte vectors.
-template <typename ST, int CH, bool VECTOR>
-__device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
-                                         int64_t tj, int64_t r, int c0, int W) {
-  using V = Vec<ST>;
-  constexpr int VN = V::N;
-  // entries whose B loads are in flight together: 16 floats of B per lane
-  constexpr int kUnroll = VN * CH >= 16 ? 1 : (VN * CH >= 8 ? 2 : 4);
-  const int lane = lane_id();
-  ST* __restrict__ crow = reinterpret_cast<ST*>(C.tile(ti, tj)) + r * C.ld;
-  float acc[CH][VN];
-  bool own[CH];
-#pragma unroll
-  for (int q = 0; q < CH; q++) {
-    const int col = c0 + (q * 32 + lane) * VN;
-    own[q] = col < W;
-    if (VECTOR) {
-      if (own[q]) V::load_c(crow + col, acc[q]);
-    } else {
-#pragma unroll
-      for (int x = 0; x < VN; x++) acc[q][x] = (col + x < W) ? V::to_f(crow[col + x]) : 0.f;
-    }
-  }
+constexpr int kSpmmUnroll = 8;  // B-row loads in flight per lane
+
+// Ask L2 for the 128-byte lines of [p, p + bytes) (no-op for null).
+__device__ __forceinline__ void l2_prefetch_slice(const void* p, int bytes) {
+  if (p == nullptr) return;
+  const char* q = reinterpret_cast<const char*>(p);
+  for (int o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(q + o));
+}
+
+// Per-warp entry tables (two 32-entry buffers of 16 bytes per warp).
+__shared__ uint4 spmm_tables[kSpmmWarps * 64];
+
+// The stages of C-tile row (ti, tj, r), one lane per stage of the group
+// [g0, g0+32), in the reference's rotated order k = (k_ + ti + tj) mod gk:
+// the A-row segment of that stage and its B tile.
+template <typename ST>
+struct StageLane {
+  int32_t alen;
+  const int32_t* acol;
+  const float* aval;
+  const ST* bt;
+};
+
+template <typename ST>
+__device__ __forceinline__ StageLane<ST> stage_lane(const SpGridView& A, const DGridView& B, int64_t ti, int64_t tj,
+                                                    int64_t r, int64_t g0) {
+  StageLane<ST> s{0, nullptr, nullptr, nullptr};
+  const int64_t kk = g0 + lane_id();
   const int64_t gk = A.gn;
-  for (int64_t kk = 0; kk < gk; kk++) {
+  if (kk < gk) {
     const int64_t k = (kk + ti + tj) % gk;
     const bclx_csr_t At = A.tile(ti, k);
-    const int32_t a0 = __ldg(At.row_ptr + r), a1 = __ldg(At.row_ptr + r + 1);
-    if (a0 == a1) continue;
-    const ST* __restrict__ bt = reinterpret_cast<const ST*>(B.tile(k, tj));
-    const bool bvec = VECTOR && (reinterpret_cast<uintptr_t>(bt) & 15) == 0;
-    const float* __restrict__ av = reinterpret_cast<const float*>(At.vals);
-    for (int32_t cb = a0; cb < a1; cb += 32) {
-      const int32_t p = cb + lane;
-      const int32_t kc = p < a1 ? __ldg(At.col_ind + p) : 0;
-      const float vv = p < a1 ? __ldg(av + p) : 0.f;
-      const int ne = min(32, a1 - cb);
-      for (int e = 0; e < ne; e += kUnroll) {
-        float bvals[kUnroll][CH][VN];
-        float vs[kUnroll];
+    const int32_t as = __ldg(At.row_ptr + r);
+    s.alen = __ldg(At.row_ptr + r + 1) - as;
+    s.acol = At.col_ind + as;
+    s.aval = reinterpret_cast<const float*>(At.vals) + as;
+    s.bt = reinterpret_cast<const ST*>(B.tile(k, tj));
+  }
+  return s;
+}
+
+// C tile (ti, tj) and every B tile of its column start on 16 bytes.
+__device__ __forceinline__ bool tiles_aligned(const DGridView& B, const DGridView& C, int64_t ti, int64_t tj) {
+  bool ok = (reinterpret_cast<uintptr_t>(C.tile(ti, tj)) & 15) == 0;
+  for (int64_t k = lane_id(); k < B.gm; k += 32) ok &= (reinterpret_cast<uintptr_t>(B.tile(k, tj)) & 15) == 0;
+  return __all_sync(kFull, ok);
+}
+
+// One warp per (C row, panel of 32 16-byte vectors).  The A entries of all
+// stages are taken 32 at a time (one lane each finds its B row), then
+// broadcast kSpmmUnroll at a time so that that many B-row loads (raw
+// 16-byte vectors) are in flight before their multiply-adds are applied in
+// entry order.  `vec`: every B and C row slice of this tile pair is 16-byte
+// aligned; otherwise element-wise access.
+template <typename ST>
+__device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
+                                         int64_t tj, int64_t r, int c0, int W, bool vec) {
+  using V = Vec<ST>;
+  constexpr int VN = V::N;
+  const int lane = lane_id();
+  ST* __restrict__ crow = reinterpret_cast<ST*>(C.tile(ti, tj)) + r * C.ld;
+  const int col = c0 + lane * VN;
+  const bool own = col < W;
+  float acc[VN];
+  if (vec) {
+    if (own) V::load_c(crow + col, acc);
+  } else {
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
-          const int32_t kr = __shfl_sync(kFull, kc, (e + u) & 31);
-          vs[u] = __shfl_sync(kFull, vv, (e + u) & 31);
-          const ST* brow = bt + (int64_t)kr * B.ld;
+    for (int x = 0; x < VN; x++) acc[x] = (col + x < W) ? V::to_f(crow[col + x]) : 0.f;
+  }
+  // Entry table of one 32-entry chunk per buffer: B row address (column 0
+  // of the tile) and A value, written lane-parallel one chunk ahead and read
+  // back with broadcast 16-byte shared loads.
+  uint4* tb = spmm_tables + (threadIdx.x >> 5) * 64;
+  // bytes of this warp's panel in one B row
+  const int pbytes = min(32 * VN, W - c0) * (int)sizeof(ST);
+  for (int64_t g0 = 0; g0 < A.gn; g0 += 32) {
+    const StageLane<ST> sl = stage_lane<ST>(A, B, ti, tj, r, g0);
+    const int32_t aincl = warp_inclusive_scan(sl.alen);
+    const int32_t atot = __shfl_sync(kFull, aincl, 31);
+    const int32_t aexcl = aincl - sl.alen;
+    // entry e0 + lane of the flattened stages: its A value and B row
+    auto chunk = [&](int32_t e0, float& v, const ST*& brow) {
+      const int32_t e = e0 + lane;
+      int src = 0;
 #pragma unroll
-          for (int q = 0; q < CH; q++) {
-            const int col = c0 + (q * 32 + lane) * VN;
-            if (e + u < ne && own[q]) {
-              if (bvec) {
-                V::load(brow + col, bvals[u][q]);
-              } else {
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int32_t t = __shfl_sync(kFull, aincl, src + step - 1);
+        if (t <= e) src += step;
+      }
+      src = min(src, 31);
+      const int32_t off = e - __shfl_sync(kFull, aexcl, src);
+      const int32_t* sacol = reinterpret_cast<const int32_t*>(
+          __shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.acol), src));
+      const float* saval = reinterpret_cast<const float*>(
+          __shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.aval), src));
+      const ST* sbt = reinterpret_cast<const ST*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.bt), src));
+      v = 0.f;
+      brow = sbt;
+      if (e < atot) {
+        v = __ldg(saval + off);
+        brow = sbt + (int64_t)__ldg(sacol + off) * B.ld;
+      }
+    };
+    auto put = [&](int buf, float v, const ST* brow) {
+      const uint64_t pa = reinterpret_cast<uint64_t>(brow);
+      tb[buf * 32 + lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), __float_as_uint(v), 0u);
+    };
+    // Chunk c is applied from the table while the rows of chunk c+2 are
+    // asked into L2 (each lane its own entry's panel slice) and the A loads
+    // of chunk c+3 are in flight.
+    float v0, v1, v2, v3;
+    const ST *b0, *b1, *b2, *b3;
+    chunk(0, v0, b0);
+    chunk(32, v1, b1);
+    chunk(64, v2, b2);
+    put(0, v0, b0);
+    l2_prefetch_slice(vec && lane < atot ? b0 + c0 : nullptr, pbytes);
+    l2_prefetch_slice(vec && 32 + lane < atot ? b1 + c0 : nullptr, pbytes);
+    __syncwarp();
+    int buf = 0;
+    for (int32_t e0 = 0; e0 < atot; e0 += 32) {
+      const bool more = e0 + 32 < atot;
+      if (e0 + 96 < atot) chunk(e0 + 96, v3, b3);  // A loads three chunks ahead
+      l2_prefetch_slice(vec && e0 + 64 + lane < atot ? b2 + c0 : nullptr, pbytes);
+      const int ne = min(32, atot - e0);
+      const uint4* t = tb + buf * 32;
+      if (vec) {
+        for (int u0 = 0; u0 < ne; u0 += kSpmmUnroll) {
+          uint4 ent[kSpmmUnroll];
+          uint4 raw[kSpmmUnroll];
 #pragma unroll
-                for (int x = 0; x < VN; x++) bvals[u][q][x] = (col + x < W) ? V::to_f(brow[col + x]) : 0.f;
-              }
+          for (int u = 0; u < kSpmmUnroll; u++) ent[u] = t[(u0 + u) & 31];
+#pragma unroll
+          for (int u = 0; u < kSpmmUnroll; u++) {
+            const ST* rp = reinterpret_cast<const ST*>((uint64_t)ent[u].x | ((uint64_t)ent[u].y << 32));
+            if (u0 + u < ne && own) raw[u] = __ldg(reinterpret_cast<const uint4*>(rp + col));
+          }
+#pragma unroll
+          for (int u = 0; u < kSpmmUnroll; u++) {
+            if (u0 + u < ne && own) {
+              float b[VN];
+              V::unpack_raw(raw[u], b);
+              const float vs = __uint_as_float(ent[u].z);
+#pragma unroll
+              for (int x = 0; x < VN; x++) acc[x] = __fmaf_rn(vs, b[x], acc[x]);
             }
           }
         }
+      } else {
+        for (int u = 0; u < ne; u++) {
+          const uint4 en = t[u];
+          const ST* rp = reinterpret_cast<const ST*>((uint64_t)en.x | ((uint64_t)en.y << 32));
+          const float vs = __uint_as_float(en.z);
 #pragma unroll
-        for (int u = 0; u < kUnroll; u++) {
-          if (e + u < ne) {
-#pragma unroll
-            for (int q = 0; q < CH; q++)
-#pragma unroll
-              for (int x = 0; x < VN; x++) acc[q][x] = __fmaf_rn(vs[u], bvals[u][q][x], acc[q][x]);
-          }
+          for (int x = 0; x < VN; x++)
+            if (col + x < W) acc[x] = __fmaf_rn(vs, V::to_f(rp[col + x]), acc[x]);
         }
       }
+      if (more) {
+        buf ^= 1;
+        put(buf, v1, b1);
+      }
+      __syncwarp();
+      v1 = v2;
+      b1 = b2;
+      v2 = v3;
+      b2 = b3;
     }
   }
+  if (vec) {
+    if (own) V::store(crow + col, acc);
+  } else {
 #pragma unroll
-  for (int q = 0; q < CH; q++) {
-    const int col = c0 + (q * 32 + lane) * VN;
-    if (VECTOR) {
-      if (own[q]) V::store(crow + col, acc[q]);
-    } else {
-#pragma unroll
-      for (int x = 0; x < VN; x++)
-        if (col + x < W) crow[col + x] = V::from_f(acc[q][x]);
-    }
+    for (int x = 0; x < VN; x++)
+      if (col + x < W) crow[col + x] = V::from_f(acc[x]);
   }
 }
 
-template <typename ST, int CH>
+template <typename ST>
 __global__ void __launch_bounds__(kSpmmWarps * 32)
     k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int row_align_ok) {
-  constexpr int PW = 32 * Vec<ST>::N * CH;
+  constexpr int PW = 32 * Vec<ST>::N;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t item = warp; item < n_items; item += nwarps) {
@@ -173,36 +274,21 @@ __global__ void __launch_bounds__(kSpmmWarps * 32)
     const int W = (int)C.cols_of(tj);
     const int c0 = panel * PW;
     if (c0 >= W) continue;
-    bool vec = row_align_ok && (W % Vec<ST>::N) == 0;
-    if (vec) {
-      const uintptr_t pc = reinterpret_cast<uintptr_t>(C.tile(ti, tj));
-      vec = (pc & 15) == 0;
-    }
-    // (a B tile that is not 16-byte aligned is read with scalar loads)
-    if (vec)
-      spmm_row<ST, CH, true>(A, B, C, ti, tj, r, c0, W);
-    else
-      spmm_row<ST, CH, false>(A, B, C, ti, tj, r, c0, W);
+    const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
+    spmm_row<ST>(A, B, C, ti, tj, r, c0, W, vec);
   }
 }
 
 template <typename ST>
 static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, const DGridView& C, int align_ok) {
   constexpr int VN = Vec<ST>::N;
-  const int64_t W = C.tn;
-  int ch = W <= 32 * VN ? 1 : (W <= 64 * VN ? 2 : 4);
-  const int64_t pw = 32 * VN * ch;
-  const int npanels = (int)ceil_div(W, pw);
+  const int npanels = (int)ceil_div(C.tn, 32 * VN);
   const int64_t n_items = C.gm * C.gn * C.tm * npanels;
   if (n_items == 0) return BCLX_OK;
-  int64_t want = ceil_div(n_items, kSpmmWarps);
-  int64_t cap = (int64_t)ctx->num_sms * 8;
-  const unsigned blocks = (unsigned)(want < cap ? want : cap);
-  switch (ch) {
-    case 1: k_spmm<ST, 1><<<blocks, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, align_ok); break;
-    case 2: k_spmm<ST, 2><<<blocks, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, align_ok); break;
-    default: k_spmm<ST, 4><<<blocks, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, align_ok); break;
-  }
+  const int64_t want = ceil_div(n_items, kSpmmWarps);
+  const int64_t cap = (int64_t)ctx->num_sms * 8;
+  k_spmm<ST><<<(unsigned)(want < cap ? want : cap), kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels,
+                                                                                        align_ok);
   note_launch();
   BCLX_CK_LAUNCH();
   return BCLX_OK;
