@@ -59,6 +59,7 @@ SIGNATURES = {
     "bclx_context_destroy": [vp],
     "bclx_context_set_stream": [vp, vp],
     "bclx_context_synchronize": [vp],
+    "bclx_context_release_cached": [vp],
     "bclx_last_error": [],
     "bclx_version": [],
     "bclx_launch_count": [],

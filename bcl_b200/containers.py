@@ -58,6 +58,10 @@ class Context:
         call("bclx_context_set_stream", self.h, ctypes.c_void_p(s))
         return self.h
 
+    def release_cached(self):
+        """Return the scratch pool's cached device memory to the driver."""
+        call("bclx_context_release_cached", self.use_current_stream())
+
     def __del__(self):
         try:
             if getattr(self, "h", None):

@@ -214,6 +214,17 @@ int bclx_context_set_stream(bclx_context_t c, void* stream) {
   return BCLX_OK;
 }
 
+int bclx_context_release_cached(bclx_context_t c) {
+  Context* ctx = reinterpret_cast<Context*>(c);
+  if (!ctx) return BCLX_ERR_INVALID;
+  BCLX_CK(cudaSetDevice(ctx->device));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
+  cudaMemPool_t pool;
+  BCLX_CK(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+  BCLX_CK(cudaMemPoolTrimTo(pool, 0));
+  return BCLX_OK;
+}
+
 int bclx_context_synchronize(bclx_context_t c) {
   Context* ctx = reinterpret_cast<Context*>(c);
   if (!ctx) return BCLX_ERR_INVALID;

@@ -38,6 +38,8 @@
 // uses wrapping arithmetic and is exact.
 #include "common.cuh"
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <atomic>
 #include <cstring>
@@ -64,7 +66,60 @@ struct Geom {
   int64_t m, n;         // C shape
   int64_t n_row_items;  // gm * gn * tm
   int64_t nfb;          // fine blocks per (full) tile width: ceil(tn / kFineCols)
+  // Stage map (or null: every stage): for C tile t = ti*gn + tj, scount[t]
+  // positions kk (ascending) of the rotated order k = (kk + ti + tj) mod gk
+  // whose A_ik and B_kj tiles both have entries, in smap[t*gk ...].
+  const int32_t* smap = nullptr;
+  const int32_t* scount = nullptr;
 };
+
+__device__ __forceinline__ int stage_count(const Geom& g, int64_t ti, int64_t tj) {
+  return g.scount ? __ldg(g.scount + ti * g.gn + tj) : (int)g.gk;
+}
+__device__ __forceinline__ int stage_at(const Geom& g, int64_t ti, int64_t tj, int s) {
+  return g.smap ? __ldg(g.smap + (ti * g.gn + tj) * g.gk + s) : s;
+}
+// Stage-list window [lo, hi) of the positions kk in [s0, s1) (warp-uniform).
+__device__ __forceinline__ void stage_window(const Geom& g, int64_t ti, int64_t tj, int s0, int s1, int& lo,
+                                             int& hi) {
+  if (!g.smap) {
+    lo = s0;
+    hi = s1;
+    return;
+  }
+  const int ns = stage_count(g, ti, tj);
+  if (s0 <= 0 && s1 >= g.gk) {
+    lo = 0;
+    hi = ns;
+    return;
+  }
+  int c0 = 0, c1 = 0;
+  for (int b = 0; b < ns; b += 32) {
+    const int si = b + (int)(threadIdx.x & 31);
+    const int kk = si < ns ? stage_at(g, ti, tj, si) : INT_MAX;
+    c0 += __popc(__ballot_sync(0xffffffffu, kk < s0));
+    c1 += __popc(__ballot_sync(0xffffffffu, kk < s1));
+  }
+  lo = c0;
+  hi = c1;
+}
+
+// Entries [bs, be) of B row kc whose columns lie in fine blocks
+// [fb_lo, fb_hi): from the B-row table rows `trows` of the tile when there is
+// one, otherwise by binary search of the row's sorted columns.
+__device__ __forceinline__ void b_block_range(const int32_t* trows, const int32_t* brp, const int32_t* bci,
+                                              int32_t kc, int fb_lo, int fb_hi, int64_t nfb, int32_t& bs,
+                                              int32_t& be) {
+  if (trows) {
+    const int32_t* trow = trows + (int64_t)kc * (nfb + 1);
+    bs = __ldg(trow + fb_lo);
+    be = __ldg(trow + fb_hi);
+  } else {
+    const int32_t b0 = __ldg(brp + kc), b1 = __ldg(brp + kc + 1);
+    bs = fb_lo == 0 ? b0 : lower_bound_i32(bci, b0, b1, fb_lo * kFineCols);
+    be = fb_hi >= nfb ? b1 : lower_bound_i32(bci, bs, b1, fb_hi * kFineCols);
+  }
+}
 
 struct RowInfo {
   int64_t ti, tj, r;
@@ -125,16 +180,21 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
                                               const RowInfo& x, int s0, int s1, int fb_lo, int fb_hi,
                                               const int32_t* __restrict__ tab, int long_seg, F&& f, FD&& fd) {
   const int lane = lane_id();
-  for (int g0 = s0; g0 < s1; g0 += 32) {
+  int w0, w1;
+  stage_window(g, x.ti, x.tj, s0, s1, w0, w1);
+  for (int g0 = w0; g0 < w1; g0 += 32) {
     // one lane per stage: its A-row segment and its B tile
-    const int kk = g0 + lane;
+    const int si = g0 + lane;
+    int kk = 0;
     int32_t as = 0, alen = 0;
     const int32_t* acol = nullptr;
     const VT* aval = nullptr;
-    const int32_t* brow = nullptr;  // B row_ptr, or the stage's table block when RANGED
+    const int32_t* brow = nullptr;   // B row_ptr
+    const int32_t* btrows = nullptr;  // the stage's B-row table block (RANGED, when there is a table)
     const int32_t* bci = nullptr;
     const VT* bva = nullptr;
-    if (kk < s1) {
+    if (si < w1) {
+      kk = stage_at(g, x.ti, x.tj, si);
       const int64_t k = (kk + x.ti + x.tj) % g.gk;
       const bclx_csr_t At = A.tile(x.ti, k);
       as = __ldg(At.row_ptr + x.r);
@@ -142,7 +202,8 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
       acol = At.col_ind + as;
       aval = reinterpret_cast<const VT*>(At.vals) + as;
       const bclx_csr_t Bt = B.tile(k, x.tj);
-      brow = RANGED ? tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1) : Bt.row_ptr;
+      brow = Bt.row_ptr;
+      if (RANGED && tab) btrows = tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1);
       bci = Bt.col_ind;
       bva = reinterpret_cast<const VT*>(Bt.vals);
     }
@@ -159,7 +220,8 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
       const int32_t* sbrow = shfl_ptr(brow, sl);
       const int32_t* sbci = shfl_ptr(bci, sl);
       const VT* sbva = shfl_ptr(bva, sl);
-      const int stage = g0 + sl;
+      const int32_t* sbtr = RANGED ? shfl_ptr(btrows, sl) : nullptr;
+      const int stage = __shfl_sync(kFull, kk, sl);
       int32_t len = 0;
       VT av = VT(0);
       const int32_t* bcol = nullptr;
@@ -169,9 +231,7 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
         av = __ldg(saval + off);
         int32_t bs, be;
         if (RANGED) {
-          const int32_t* trow = sbrow + (int64_t)kc * (g.nfb + 1);
-          bs = __ldg(trow + fb_lo);
-          be = __ldg(trow + fb_hi);
+          b_block_range(sbtr, sbrow, sbci, kc, fb_lo, fb_hi, g.nfb, bs, be);
         } else {
           bs = __ldg(sbrow + kc);
           be = __ldg(sbrow + kc + 1);
@@ -251,18 +311,20 @@ template <typename FS>
 __device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridView& B, const Geom& g,
                                              const RowInfo& x, int part, int nparts, FS&& fs) {
   const int lane = lane_id();
-  for (int g0 = 0; g0 < g.gk; g0 += 32) {
-    const int kk = g0 + lane;
+  const int ns = stage_count(g, x.ti, x.tj);
+  for (int g0 = 0; g0 < ns; g0 += 32) {
+    const int si = g0 + lane;
     int32_t as = 0, alen = 0;
     const int32_t* acol = nullptr;
     const int32_t* brp = nullptr;
     const int32_t* bci = nullptr;
-    if (kk < g.gk) {
-      const bclx_csr_t At = A.tile(x.ti, kk);
+    if (si < ns) {
+      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.ti + x.tj) % g.gk;
+      const bclx_csr_t At = A.tile(x.ti, k);
       as = __ldg(At.row_ptr + x.r);
       alen = __ldg(At.row_ptr + x.r + 1) - as;
       acol = At.col_ind;
-      const bclx_csr_t Bt = B.tile(kk, x.tj);
+      const bclx_csr_t Bt = B.tile(k, x.tj);
       brp = Bt.row_ptr;
       bci = Bt.col_ind;
     }
@@ -315,19 +377,24 @@ __device__ __forceinline__ void walk_columns_ranged(const SpGridView& A, const S
                                                     const RowInfo& x, int fb_lo, int fb_hi,
                                                     const int32_t* __restrict__ tab, FS&& fs) {
   const int lane = lane_id();
-  for (int g0 = 0; g0 < g.gk; g0 += 32) {
-    const int kk = g0 + lane;
+  const int ns = stage_count(g, x.ti, x.tj);
+  for (int g0 = 0; g0 < ns; g0 += 32) {
+    const int si = g0 + lane;
     int32_t as = 0, alen = 0;
     const int32_t* acol = nullptr;
     const int32_t* trows = nullptr;
+    const int32_t* brp = nullptr;
     const int32_t* bci = nullptr;
-    if (kk < g.gk) {
-      const bclx_csr_t At = A.tile(x.ti, kk);
+    if (si < ns) {
+      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.ti + x.tj) % g.gk;
+      const bclx_csr_t At = A.tile(x.ti, k);
       as = __ldg(At.row_ptr + x.r);
       alen = __ldg(At.row_ptr + x.r + 1) - as;
       acol = At.col_ind;
-      trows = tab + ((int64_t)kk * g.gn + x.tj) * g.tk * (g.nfb + 1);
-      bci = B.tile(kk, x.tj).col_ind;
+      if (tab) trows = tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1);
+      const bclx_csr_t Bt = B.tile(k, x.tj);
+      brp = Bt.row_ptr;
+      bci = Bt.col_ind;
     }
     const int32_t aincl = warp_inclusive_scan(alen);
     const int32_t atot = __shfl_sync(kFull, aincl, 31);
@@ -339,13 +406,12 @@ __device__ __forceinline__ void walk_columns_ranged(const SpGridView& A, const S
       const int32_t sax = __shfl_sync(kFull, aexcl, sl);
       const int32_t* sacol = shfl_ptr(acol, sl);
       const int32_t* strows = shfl_ptr(trows, sl);
+      const int32_t* sbrp = shfl_ptr(brp, sl);
       const int32_t* sbci = shfl_ptr(bci, sl);
       int32_t bs = 0, be = 0;
       if (e < atot) {
         const int32_t kc = __ldg(sacol + sas + (e - sax));
-        const int32_t* trow = strows + (int64_t)kc * (g.nfb + 1);
-        bs = __ldg(trow + fb_lo);
-        be = __ldg(trow + fb_hi);
+        b_block_range(strows, sbrp, sbci, kc, fb_lo, fb_hi, g.nfb, bs, be);
       }
       const bool lng = be - bs >= 32;
       if (!lng)
@@ -385,17 +451,19 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
     int64_t tot = 0, annz = 0;
     int32_t bmax = 0;
     if (x.r < A.rows_of(x.ti)) {
-      for (int g0 = 0; g0 < g.gk; g0 += 32) {
-        const int kk = g0 + lane;
+      const int ns = stage_count(g, x.ti, x.tj);
+      for (int g0 = 0; g0 < ns; g0 += 32) {
+        const int si = g0 + lane;
         int32_t as = 0, alen = 0;
         const int32_t* acol = nullptr;
         const int32_t* brp = nullptr;
-        if (kk < g.gk) {
-          const bclx_csr_t At = A.tile(x.ti, kk);
+        if (si < ns) {
+          const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.ti + x.tj) % g.gk;
+          const bclx_csr_t At = A.tile(x.ti, k);
           as = __ldg(At.row_ptr + x.r);
           alen = __ldg(At.row_ptr + x.r + 1) - as;
           acol = At.col_ind;
-          brp = B.tile(kk, x.tj).row_ptr;
+          brp = B.tile(k, x.tj).row_ptr;
         }
         const int32_t aincl = warp_inclusive_scan(alen);
         const int32_t atot = __shfl_sync(kFull, aincl, 31);
@@ -843,7 +911,8 @@ constexpr float kLearnMargin = 1.15f;  // head room on the predicted count
 // Products of every heavy row per fine column block: bub[h*nfb + b].  One
 // warp per heavy row; lanes take A entries (all stages) and add each entry's
 // per-block segment lengths (from the B-row table) into shared counters.
-__global__ void __launch_bounds__(256) k_heavy_block_ub(SpGridView A, Geom g, const int32_t* __restrict__ heavy_list,
+__global__ void __launch_bounds__(256) k_heavy_block_ub(SpGridView A, SpGridView B, Geom g,
+                                                        const int32_t* __restrict__ heavy_list,
                                                         int n_heavy, const int32_t* __restrict__ tab,
                                                         int32_t* __restrict__ bub) {
   __shared__ int32_t cnt_all[8][64];
@@ -857,17 +926,29 @@ __global__ void __launch_bounds__(256) k_heavy_block_ub(SpGridView A, Geom g, co
     cnt[lane] = 0;
     cnt[lane + 32] = 0;
     __syncwarp();
-    for (int64_t k = 0; k < g.gk; k++) {
+    const int ns = stage_count(g, x.ti, x.tj);
+    for (int si = 0; si < ns; si++) {
+      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.ti + x.tj) % g.gk;
       const bclx_csr_t At = A.tile(x.ti, k);
       const int32_t a0 = __ldg(At.row_ptr + x.r), a1 = __ldg(At.row_ptr + x.r + 1);
-      const int32_t* trows = tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1);
-      for (int32_t p = a0 + lane; p < a1; p += 32) {
-        const int32_t* trow = trows + (int64_t)__ldg(At.col_ind + p) * (g.nfb + 1);
-        int32_t prev = __ldg(trow);
-        for (int b = 0; b < nfb; b++) {
-          const int32_t nx = __ldg(trow + b + 1);
-          if (nx != prev) atomicAdd(&cnt[b], nx - prev);
-          prev = nx;
+      if (tab) {
+        const int32_t* trows = tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1);
+        for (int32_t p = a0 + lane; p < a1; p += 32) {
+          const int32_t* trow = trows + (int64_t)__ldg(At.col_ind + p) * (g.nfb + 1);
+          int32_t prev = __ldg(trow);
+          for (int b = 0; b < nfb; b++) {
+            const int32_t nx = __ldg(trow + b + 1);
+            if (nx != prev) atomicAdd(&cnt[b], nx - prev);
+            prev = nx;
+          }
+        }
+      } else {
+        // no table: count the B row's columns per block
+        const bclx_csr_t Bt = B.tile(k, x.tj);
+        for (int32_t p = a0 + lane; p < a1; p += 32) {
+          const int32_t kc = __ldg(At.col_ind + p);
+          const int32_t b1 = __ldg(Bt.row_ptr + kc + 1);
+          for (int32_t q = __ldg(Bt.row_ptr + kc); q < b1; q++) atomicAdd(&cnt[__ldg(Bt.col_ind + q) / kFineCols], 1);
         }
       }
     }
@@ -1053,6 +1134,8 @@ struct bclx_spgemm_plan_s {
   int64_t* heavy_first = nullptr;
   HeavyItem* heavy_items = nullptr;
   int32_t* tab = nullptr;
+  int32_t* smap_own = nullptr;    // stage map (Geom::smap / scount) owned by this plan
+  int32_t* scount_own = nullptr;
   unsigned long long* queue = nullptr;  // work-queue heads, one per stage launch
   // numeric tuning (bclx_spgemm_plan_tune)
   int grab = 2, blocks_per_sm = 4, long_seg = kLongSegDefault;
@@ -1118,9 +1201,11 @@ struct bclx_spgemm_plan_s {
     light_slot = item_pos = redo_off = nullptr;
     temp_val = redo_val = nullptr;
     void* ps[] = {queue, light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
-                  heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset};
+                  heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset,
+                  smap_own, scount_own};
     for (void* p : ps) scratch_free(ctx, p);
     queue = nullptr;
+    smap_own = scount_own = nullptr;
     light_list = heavy_list = vheavy_list = heavy_tmp = counters = row_count = heavy_nitems = tab = id_rp = id_ci = nullptr;
     products_dev = nullptr;
     row_offset = heavy_first = acc_tile_offset = nullptr;
@@ -1218,9 +1303,65 @@ static int launch_numeric(Context* ctx, const SpGridView& A, const SpGridView& B
   return launch_numeric_w<VT, kMaxWords>(ctx, A, B, P, out_col, out_val, s0, s1);
 }
 
+// Stage map for fine grids: per C tile, the rotated stage positions whose A
+// and B tiles both have entries (a banded matrix on a fine grid has a few of
+// gk).  Coarse grids (gk <= 16) walk every stage.
+__global__ void k_stage_map(SpGridView A, SpGridView B, Geom g, int32_t* __restrict__ smap,
+                            int32_t* __restrict__ scount) {
+  const int64_t nt = g.gm * g.gn;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ti = t / g.gn, tj = t - ti * g.gn;
+    int32_t c = 0;
+    for (int64_t kk = 0; kk < g.gk; kk++) {
+      const int64_t k = (kk + ti + tj) % g.gk;
+      if (A.tile(ti, k).nnz > 0 && B.tile(k, tj).nnz > 0) smap[t * g.gk + c++] = (int32_t)kk;
+    }
+    scount[t] = c;
+  }
+}
+
+constexpr int64_t kStageMapMinGrid = 17;
+constexpr int64_t kBTableMaxBytes = 2ll << 30;  // larger tables give way to binary searches of B rows
+
+static int build_stage_map(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P, Geom& g) {
+  g.smap = g.scount = nullptr;
+  if (g.gk < kStageMapMinGrid) return BCLX_OK;
+  const int64_t nt = g.gm * g.gn;
+  BCLX_TRY(scratch_alloc_n(ctx, &P->smap_own, (size_t)(nt * g.gk)));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->scount_own, (size_t)nt));
+  k_stage_map<<<grid_for(ctx, nt / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(A, B, g, P->smap_own, P->scount_own);
+  note_launch();
+  BCLX_CK_LAUNCH();
+  g.smap = P->smap_own;
+  g.scount = P->scount_own;
+  return BCLX_OK;
+}
+
+// B-row table (k_btable) when it fits kBTableMaxBytes; otherwise none and the
+// walks find column-block ranges by binary search.
+// BCLX_BTABLE_MAX_BYTES overrides the cap (0: never build the table).
+static int64_t btable_cap() {
+  const char* e = std::getenv("BCLX_BTABLE_MAX_BYTES");
+  return e && *e ? std::strtoll(e, nullptr, 10) : kBTableMaxBytes;
+}
+
+static int build_btable(Context* ctx, const SpGridView& B, const Geom& g, bclx_spgemm_plan_s* P) {
+  const int64_t nbrows = g.gk * g.gn * g.tk;
+  if ((int64_t)sizeof(int32_t) * nbrows * (g.nfb + 1) > btable_cap()) {
+    P->tab = nullptr;
+    return BCLX_OK;
+  }
+  BCLX_TRY(scratch_alloc_n(ctx, &P->tab, (size_t)nbrows * (g.nfb + 1)));
+  k_btable<<<grid_for(ctx, nbrows / 32 + 1, 8, 16), 256, 0, ctx->stream>>>(B, g, P->tab);
+  note_launch();
+  BCLX_CK_LAUNCH();
+  return BCLX_OK;
+}
+
 // Classification, symbolic, row offsets and the heavy-row cut.
-static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B, const Geom& g, int dtype,
+static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B, Geom g, int dtype,
                          int32_t* tile_row_ptr, int64_t* tile_offset, bclx_spgemm_plan_s* P) {
+  BCLX_TRY(build_stage_map(ctx, A, B, P, g));
   P->g = g;
   P->dtype = dtype;
   const int64_t nri = g.n_row_items;
@@ -1302,11 +1443,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     note_launch();
     BCLX_CK_LAUNCH();
     // B-row table for the heavy items' column ranges
-    const int64_t nbrows = g.gk * g.gn * g.tk;
-    BCLX_TRY(scratch_alloc_n(ctx, &P->tab, (size_t)nbrows * (g.nfb + 1)));
-    k_btable<<<grid_for(ctx, nbrows / 32 + 1, 8, 16), 256, 0, ctx->stream>>>(B, g, P->tab);
-    note_launch();
-    BCLX_CK_LAUNCH();
+    BCLX_TRY(build_btable(ctx, B, g, P));
   }
   return BCLX_OK;
 }
@@ -1775,9 +1912,10 @@ static int exact_numeric_into(Context* ctx, const SpGridView& A, const SpGridVie
 
 // Everything up to the final offsets: predict, cut, one numeric pass into
 // temp slots, redo the failed rows exactly, row offsets.  nnz in P->nnz.
-static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, const Geom& g, int dtype,
+static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, Geom g, int dtype,
                         const float* params, int32_t* tile_row_ptr, int64_t* tile_offset, bclx_spgemm_plan_s* P) {
   P->learned = true;
+  BCLX_TRY(build_stage_map(ctx, A, B, P, g));
   P->g = g;
   P->dtype = dtype;
   P->hbm_words = (g.tn + 31) / 32;
@@ -1843,13 +1981,9 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   BCLX_TRY(scratch_alloc_n(ctx, &P->light_slot, P->n_light + 1));
   const unsigned hb = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
   if (P->n_heavy > 0) {
-    const int64_t nbrows = g.gk * g.gn * g.tk;
-    BCLX_TRY(scratch_alloc_n(ctx, &P->tab, (size_t)nbrows * (g.nfb + 1)));
-    k_btable<<<grid_for(ctx, nbrows / 32 + 1, 8, 16), 256, 0, ctx->stream>>>(B, g, P->tab);
-    note_launch();
-    BCLX_CK_LAUNCH();
+    BCLX_TRY(build_btable(ctx, B, g, P));
     BCLX_TRY(scratch_alloc_n(ctx, &P->block_ub, (size_t)P->n_heavy * g.nfb));
-    k_heavy_block_ub<<<grid_for(ctx, P->n_heavy, 8, 16), 256, 0, ctx->stream>>>(A, g, P->heavy_list,
+    k_heavy_block_ub<<<grid_for(ctx, P->n_heavy, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P->heavy_list,
                                                                                (int)P->n_heavy, P->tab, P->block_ub);
     note_launch();
     BCLX_CK_LAUNCH();

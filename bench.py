@@ -43,6 +43,11 @@ WORKLOADS = {
                               desc="R-MAT scale 16, C = A*A, 8x8 tile grid, int32 values in [-8, 8]"),
     "spgemm_rmat18": dict(kind="spgemm", scale=18, grid=16, value_type="f32",
                           desc="R-MAT scale 18 (262144^2), C = A*A, 16x16 tile grid, FP32"),
+    "spgemm_rmat20": dict(kind="spgemm", scale=20, grid=64, value_type="f32",
+                          desc="R-MAT scale 20 (1048576^2), C = A*A, 64x64 tile grid (16384-wide tiles), FP32"),
+    "spgemm_stencil128": dict(kind="spgemm", matrix="stencil", g=128, grid=128, value_type="f32",
+                              desc="27-point stencil Laplacian on a 128^3 grid (2097152^2), C = L*L, "
+                                   "128x128 tile grid, FP32"),
     "spmm_er16k": dict(kind="spmm", matrix="er", n=16384, N=128, grid=4, dtype="f32", bdist="uniform",
                        desc="Erdos-Renyi 16384^2 (16 nnz/row) x dense 16384x128 U(-1,1), 4x4 tile grid, FP32"),
     "spmm_rmat21": dict(kind="spmm", matrix="rmat", scale=21, N=256, grid=8, dtype="f32", bdist="normal",
@@ -64,6 +69,8 @@ def parse_args():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU timing")
     p.add_argument("--no-precision", action="store_true", help="skip the R-MAT scale-21 BF16/FP32 SpMM extra")
+    p.add_argument("--path", default="fused", choices=["fused", "per_stage", "batched_graph", "learned"],
+                   help="SpGEMM form timed as the step (default: all stages fused)")
     p.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
     return p.parse_args()
 
@@ -205,12 +212,38 @@ def peaks():
 # ---- our arm: SpGEMM ------------------------------------------------------------------
 
 
+def spgemm_matrix(wl, seed):
+    from bcl_b200 import gen
+    if wl.get("matrix") == "stencil":
+        return gen.stencil27(wl["g"], value_type=wl["value_type"])
+    return gen.rmat(wl["scale"], seed=seed, value_type=wl["value_type"])
+
+
+def plain_sampled_time(A, n_tiles, seed):
+    """The per-tile-product loop (spgemm_plain) on a seeded sample of C tiles:
+    each sampled tile runs its G two-phase partial products and their
+    accumulation; returns the time scaled to all grid_m*grid_n tiles."""
+    import torch
+    from bcl_b200.containers import _tile_view, spgemm, tile_accumulate
+    G = A.gn
+    rng = np.random.default_rng(seed)
+    picks = rng.choice(A.gm * A.gn, size=min(n_tiles, A.gm * A.gn), replace=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for t in picks:
+        i, j = divmod(int(t), A.gn)
+        parts = [spgemm(_tile_view(A, (i, (k_ + i + j) % G)), _tile_view(A, ((k_ + i + j) % G, j))) for k_ in range(G)]
+        tile_accumulate(parts)
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) * (A.gm * A.gn) / len(picks)
+
+
 def bench_spgemm(args, wl, dist, device):
     import torch
     from bcl_b200 import _lib, gen
     from bcl_b200.containers import BlockCustom, SPMatrix, spgemm, spgemm_numeric, spgemm_symbolic
 
-    a = gen.rmat(wl["scale"], seed=args.seed + dist.rank, value_type=wl["value_type"])
+    a = spgemm_matrix(wl, args.seed + dist.rank)
     n = a.m
     G = wl["grid"]
     ts = -(-n // G)
@@ -224,7 +257,24 @@ def bench_spgemm(args, wl, dist, device):
     host_t = {"symbolic": 0.0, "alloc": 0.0, "numeric": 0.0, "close": 0.0}
     outbuf = {}
 
+    pred = None
+    if args.path == "learned":
+        from bcl_b200 import learned as _learned
+        pred = _learned.get_default(train_if_missing=False)
+    learned_st = {}
+
     def step(record=None):
+        if args.path == "learned":
+            # the learned product: prediction in place of the symbolic pass
+            from bcl_b200.containers import learned_stats, spgemm_learned
+            if record:
+                record[0].record(stream)
+            C, pl = spgemm_learned(A, A, predictor=pred, keep_plan=True)
+            if record:
+                record[1].record(stream)
+            learned_st.update(learned_stats(pl))
+            pl.close()
+            return C.nnz(), None
         t0 = time.perf_counter()
         plan, out, trp, toff, nnz = spgemm_symbolic(A, A)
         t1 = time.perf_counter()
@@ -239,7 +289,7 @@ def bench_spgemm(args, wl, dist, device):
         t2 = time.perf_counter()
         if record:
             record[0].record(stream)
-        spgemm_numeric(plan, A, A, out)
+        spgemm_numeric(plan, A, A, out, "fused" if args.path == "fused" else args.path)
         if record:
             record[1].record(stream)
         t3 = time.perf_counter()
@@ -284,11 +334,22 @@ def bench_spgemm(args, wl, dist, device):
     traffic = read_profile_traffic("spgemm_numeric_rmat16")
     roofline = {"bound": "hbm", "achieved": alg / num_avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
                 "frac": alg / num_avg_s / 1e9 / hbm_peak, "traffic": traffic,
-                "kernel": "k_spgemm_numeric (all SUMMA stages, one launch)", "peak_source": peak_kind,
+                "kernel": ("k_numeric (all SUMMA stages, one launch)" if args.path == "fused" else
+                           "whole learned product" if args.path == "learned" else f"numeric pass ({args.path})"),
+                "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": alg, "kernel_ms": num_avg_s * 1e3}
 
+    # the timed loop's output buffers and the pool's cached scratch go back
+    # before the end-to-end and secondary runs allocate their own
+    outbuf.clear()
+    from bcl_b200.containers import context
+    context(device).release_cached()
+    torch.cuda.empty_cache()
     # end to end: host CSR tiles in pinned memory -> device -> product -> host
-    e2e = bench_spgemm_e2e(args, A, stream, flops, dist)
+    try:
+        e2e = bench_spgemm_e2e(args, A, stream, flops, dist)
+    except Exception as e:  # e.g. pinned host memory for a very large C
+        e2e = {"value": None, "unit": "GFLOP/s", "error": repr(e)[:300]}
 
     extras = {}
     if not args.no_extras and dist.world == 1:
@@ -306,6 +367,8 @@ def bench_spgemm(args, wl, dist, device):
             "step_ms": step_ms}
     if extras:
         line["extras"] = extras
+    if learned_st:
+        line["learned"] = dict(learned_st, misprediction_rate=learned_st["rows_redone"] / max(learned_st["heavy_rows"], 1))
     return line
 
 
@@ -372,18 +435,25 @@ def spgemm_extras(args, A, a, ts, products, stream):
     ex = {}
     t = time_region(lambda: spgemm(A, A, stages="per_stage"), 3, stream)
     ex["spgemm_per_stage_gflops"] = flops / t / 1e9
-    t = time_region(lambda: spgemm_plain(A, A), 1, stream)
-    ex["spgemm_plain_gflops"] = flops / t / 1e9
-    ex["spgemm_plain_ms"] = t * 1e3
+    if A.gn <= 16:
+        t = time_region(lambda: spgemm_plain(A, A), 1, stream)
+        ex["spgemm_plain_gflops"] = flops / t / 1e9
+        ex["spgemm_plain_ms"] = t * 1e3
+    else:  # G^3 tile products: time a seeded sample of C tiles and scale
+        t = plain_sampled_time(A, 16, args.seed)
+        ex["spgemm_plain_gflops"] = flops / t / 1e9
+        ex["spgemm_plain_ms"] = t * 1e3
+        ex["spgemm_plain_note"] = "16 seeded C tiles (each: G partial products + accumulation), scaled to all tiles"
     try:
         ex["learned"] = learned_summary(A, products, stream)
     except Exception as e:  # keep the headline line even if an extra fails
         ex["learned"] = {"error": repr(e)}
-    try:
-        ex["spmm_er16k"] = spmm_summary(args, stream)
-    except Exception as e:
-        ex["spmm_er16k"] = {"error": repr(e)}
-    if not args.no_precision:
+    if A.gn <= 16:
+        try:
+            ex["spmm_er16k"] = spmm_summary(args, stream)
+        except Exception as e:
+            ex["spmm_er16k"] = {"error": repr(e)}
+    if not args.no_precision and A.gn <= 16:
         try:
             ex["spmm_precision_rmat21"] = spmm_precision_summary(args, stream)
         except Exception as e:
@@ -732,9 +802,9 @@ def run_reference(args, dist):
                                  "sample": sample + f", {args.steps} reps"},
                 "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "gpu_launches": 0}
-    a = gen.rmat(wl["scale"], seed=args.seed, value_type=wl["value_type"])
+    a = spgemm_matrix(wl, args.seed)
     G = wl["grid"]
-    stride = 128 if wl["scale"] <= 16 else 2048
+    stride = 128 if a.m <= 65536 else 2048
     products, times, rows = reference_spgemm_sample(a, G, stride, args.warmup, args.steps)
     t = statistics.mean(times)
     value = 2.0 * products / t / 1e9
@@ -769,10 +839,9 @@ def main():
     if wl["kind"] == "spgemm":
         line = bench_spgemm(args, wl, dist, device)
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-            from bcl_b200 import gen
-            a = gen.rmat(wl["scale"], seed=args.seed, value_type=wl["value_type"])
+            a = spgemm_matrix(wl, args.seed)
             try:
-                line["cpu_baseline"] = cpu_baseline_spgemm(a, wl["grid"], stride=64 if wl["scale"] <= 16 else 1024)
+                line["cpu_baseline"] = cpu_baseline_spgemm(a, wl["grid"], stride=64 if a.m <= 65536 else 1024)
             except Exception as e:
                 line["cpu_baseline"] = {"value": None, "error": repr(e)}
     else:

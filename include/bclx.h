@@ -134,6 +134,10 @@ BCLX_API int bclx_context_destroy(bclx_context_t ctx);
 /* Use `stream` (a cudaStream_t; NULL = legacy default) for every later call. */
 BCLX_API int bclx_context_set_stream(bclx_context_t ctx, void* stream);
 BCLX_API int bclx_context_synchronize(bclx_context_t ctx);
+/* Wait for the context's stream, then return the scratch pool's cached
+ * device memory to the driver (the pool keeps freed scratch for reuse).
+ * Counterpart of freeing a BCL segment (BCL::finalize, backends/mpi/backend.hpp:120-130). */
+BCLX_API int bclx_context_release_cached(bclx_context_t ctx);
 /* Text of the last CUDA error seen on this thread (empty if none). */
 BCLX_API const char* bclx_last_error(void);
 /* Library version, e.g. 100 for 0.1.0. */

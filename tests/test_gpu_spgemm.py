@@ -96,6 +96,38 @@ def test_rmat11_vs_oracle(value_type, tiles):
     assert_csr_identical(got, rp, ci, cv)
 
 
+@pytest.mark.parametrize("mode", ["fused", "per_stage"])
+def test_fine_grid_stage_map(mode):
+    """Grids with more than 16 tile columns walk only the stages whose A and
+    B tiles both have entries: a banded stencil (most tile products empty)
+    and R-MAT, against the oracle on the same grid."""
+    s = gen.stencil27(24)
+    rp, ci, cv = O.gemm_tiled(s, s, 512, 512, 512)
+    assert_csr_identical(product(s, s, (512, 512, 512), mode).get(), rp, ci, cv)
+    a = gen.rmat(12, seed=103)
+    rp, ci, cv = O.gemm_tiled(a, a, 128, 128, 128)
+    assert_csr_identical(product(a, a, (128, 128, 128), mode).get(), rp, ci, cv)
+
+
+@pytest.mark.parametrize("learned", [False, True])
+def test_without_btable_binary_search(monkeypatch, learned):
+    """With the B-row table disabled (as for grids where it would not fit),
+    heavy items find their column-block ranges by binary search: same
+    result."""
+    from bcl_b200.containers import BlockCustom, SPMatrix, spgemm_learned
+    monkeypatch.setenv("BCLX_BTABLE_MAX_BYTES", "0")
+    a = gen.rmat(12, seed=104)
+    tiles = (1024, 4096, 4096)
+    rp, ci, cv = O.gemm_tiled(a, a, *tiles)
+    if learned:
+        A = SPMatrix.from_csr(a, BlockCustom(tiles[:2]))
+        B = SPMatrix.from_csr(a, BlockCustom(tiles[1:]))
+        got = spgemm_learned(A, B).get()
+    else:
+        got = product(a, a, tiles).get()
+    assert_csr_identical(got, rp, ci, cv)
+
+
 def test_wide_tiles_heavy_rows():
     """Tiles 16384 columns wide send every row through the block-wide
     symbolic pass and the cut into <= 512-output items (heavy path)."""
