@@ -688,7 +688,8 @@ struct WarpSmem {
 // own products, and an item with more than kVcap outputs marks its row in
 // row_failed and stops (that row is redone by the exact path).  Outputs go
 // to temp slots (light row l at light_slot[l], heavy item idx at
-// heavy_slot_base + idx*kVcap, after all light slots),
+// heavy_slot_base + item_off[idx], after all light slots; an item's slot
+// count, at most kVcap, comes from the prediction),
 // counts to item_count / row_count_w.
 template <typename VT, int WORDS, bool LEARNED>
 __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
@@ -700,7 +701,8 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
               int32_t* __restrict__ out_col, VT* __restrict__ out_val, int s0, int s1,
               unsigned long long* __restrict__ queue, int grab, int long_seg,
               const int64_t* __restrict__ light_slot, int32_t* __restrict__ item_count,
-              int32_t* __restrict__ row_count_w, int32_t* __restrict__ row_failed, int64_t heavy_slot_base) {
+              int32_t* __restrict__ row_count_w, int32_t* __restrict__ row_failed, int64_t heavy_slot_base,
+              const int64_t* __restrict__ item_off) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem<VT, WORDS>& S = reinterpret_cast<WarpSmem<VT, WORDS>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = lane_id();
@@ -720,7 +722,7 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     // heavy items first (they are the larger ones)
     const bool heavy = idx < n_heavy_items;
     int64_t ri;
-    int cnt = 0, fb_lo = 0, fb_hi = 0, lo = 0, hi, hslot = 0;
+    int cnt = 0, fb_lo = 0, fb_hi = 0, lo = 0, hi, hslot = 0, icap = kVcap;
     int64_t off;
     const uint32_t* hb = nullptr;
     if (heavy) {
@@ -730,7 +732,8 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
       fb_lo = it.fb_lo;
       fb_hi = it.fb_hi;
       if (LEARNED) {
-        off = heavy_slot_base + idx * kVcap;
+        off = heavy_slot_base + item_off[idx];
+        icap = it.count;  // temp slots sized from the prediction
       } else {
         cnt = it.count;
         off = row_offset[ri] + it.rel;
@@ -795,7 +798,7 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     }
     __syncwarp();
     if (LEARNED) {
-      if (heavy && cnt > kVcap) {  // the prediction cut this item too wide
+      if (heavy && cnt > icap) {  // the prediction cut this item too wide, or sized it too small
         if (lane == 0) row_failed[hslot] = 1;
         continue;
       }
@@ -907,6 +910,8 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
 
 constexpr float kLearnTarget = 320.f;  // outputs aimed at per heavy item (the accumulator holds 512)
 constexpr float kLearnMargin = 1.15f;  // head room on the predicted count
+constexpr float kCapMargin = 1.25f;    // head room of an item's temp slots over its estimate
+constexpr float kCapSlack = 32.f;
 
 // Products of every heavy row per fine column block: bub[h*nfb + b].  One
 // warp per heavy row; lanes take A entries (all stages) and add each entry's
@@ -967,11 +972,21 @@ __global__ void __launch_bounds__(256) k_heavy_block_ub(SpGridView A, SpGridView
 // Without a network a block's product count (capped at its width) is used:
 // an upper bound, so no item can overflow.  FILL = false counts the items,
 // FILL = true writes them.
+// Temp slots of a heavy item from its expected outputs: a predicted estimate
+// gets head room (an item that outgrows it is redone exactly); without a
+// network the estimate is already an upper bound.
+__device__ __forceinline__ int item_capacity(float est, bool predicted) {
+  const float want = predicted ? est * kCapMargin + kCapSlack : est;
+  const int c = ((int)ceilf(want) + 15) & ~15;
+  return c < 16 ? 16 : (c > kVcap ? kVcap : c);
+}
+
 template <bool FILL>
 __global__ void k_learned_cut(Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
                               const float* __restrict__ pred, const int32_t* __restrict__ ub,
                               const int32_t* __restrict__ bub, int32_t* __restrict__ n_items,
-                              const int64_t* __restrict__ first, HeavyItem* __restrict__ items) {
+                              const int64_t* __restrict__ first, HeavyItem* __restrict__ items,
+                              int32_t* __restrict__ item_cap) {
   const int nfb_g = (int)g.nfb;
   for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n_heavy; h += (int64_t)gridDim.x * blockDim.x) {
     const int64_t ri = heavy_list[h];
@@ -996,14 +1011,22 @@ __global__ void k_learned_cut(Geom g, const int32_t* __restrict__ heavy_list, in
       const float p = (float)bu[b];
       const float e = pred ? fminf(w, kappa * w * (1.f - __expf(-p / w))) : fminf(w, p);
       if (b > start && cur + e > kLearnTarget) {
-        if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)b, 0, 0};
+        if (FILL) {
+          const int cap = item_capacity(cur, pred != nullptr);
+          item_cap[out] = cap;
+          items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)b, 0, cap};
+        }
         n++;
         start = b;
         cur = 0.f;
       }
       cur += e;
     }
-    if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)nfb, 0, 0};
+    if (FILL) {
+      const int cap = item_capacity(cur, pred != nullptr);
+      item_cap[out] = cap;
+      items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)nfb, 0, cap};
+    }
     n++;
     if (!FILL) n_items[h] = n;
   }
@@ -1052,7 +1075,8 @@ __global__ void k_compact(Geom g, const int32_t* __restrict__ light_list, int n_
                           const HeavyItem* __restrict__ items, int64_t n_items, const int64_t* __restrict__ first,
                           const int32_t* __restrict__ item_count, const int64_t* __restrict__ item_pos,
                           const int32_t* __restrict__ row_failed, const int32_t* __restrict__ failed_list,
-                          int n_failed, int64_t heavy_slot_base, const int64_t* __restrict__ redo_off,
+                          int n_failed, int64_t heavy_slot_base, const int64_t* __restrict__ item_off,
+                          const int64_t* __restrict__ redo_off,
                           const int32_t* __restrict__ row_count,
                           const int64_t* __restrict__ row_offset, const int32_t* __restrict__ tcol,
                           const VT* __restrict__ tval, const int32_t* __restrict__ rcol, const VT* __restrict__ rval,
@@ -1076,7 +1100,7 @@ __global__ void k_compact(Geom g, const int32_t* __restrict__ light_list, int n_
       const HeavyItem it = items[idx];
       if (row_failed[it.h]) continue;
       const int ri = heavy_list[it.h];
-      src = heavy_slot_base + idx * kVcap;
+      src = heavy_slot_base + item_off[idx];
       dst = row_offset[ri] + (item_pos[idx] - item_pos[first[it.h]]);
       cnt = item_count[idx];
     } else {
@@ -1152,6 +1176,8 @@ struct bclx_spgemm_plan_s {
   int64_t* light_slot = nullptr;    // [n_light+1]
   int32_t* light_ub = nullptr;      // [n_light]
   int32_t* item_count = nullptr;    // [n_heavy_items]
+  int32_t* item_cap = nullptr;      // [n_heavy_items] temp slots per heavy item
+  int64_t* item_off = nullptr;      // [n_heavy_items+1] their offsets
   int64_t* item_pos = nullptr;      // [n_heavy_items+1]
   int32_t* row_failed = nullptr;    // [n_heavy]
   int32_t* block_ub = nullptr;      // [n_heavy*nfb] products per fine block
@@ -1192,13 +1218,14 @@ struct bclx_spgemm_plan_s {
       delete redo;
       redo = nullptr;
     }
-    void* lp[] = {feat, ub, pred, light_slot, light_ub, item_count, item_pos, row_failed, block_ub, failed_list,
+    void* lp[] = {feat, ub, pred, light_slot, light_ub, item_count, item_cap, item_off, item_pos, row_failed, block_ub,
+                  failed_list,
                   temp_col,
                   temp_val, redo_off, redo_col, redo_val};
     for (void* p : lp) scratch_free(ctx, p);
     feat = pred = nullptr;
-    ub = light_ub = item_count = row_failed = block_ub = failed_list = temp_col = redo_col = nullptr;
-    light_slot = item_pos = redo_off = nullptr;
+    ub = light_ub = item_count = item_cap = row_failed = block_ub = failed_list = temp_col = redo_col = nullptr;
+    light_slot = item_pos = item_off = redo_off = nullptr;
     temp_val = redo_val = nullptr;
     void* ps[] = {queue, light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
                   heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset,
@@ -1290,7 +1317,7 @@ static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView&
       P->hbm_words, P->tab, P->row_count, P->row_offset, out_col, reinterpret_cast<VT*>(out_val), s0, s1, q,
       P->grab < 1 ? 1 : P->grab, P->long_seg < 1 ? 1 : P->long_seg, LEARNED ? P->light_slot : nullptr,
       LEARNED ? P->item_count : nullptr, LEARNED ? P->row_count : nullptr, LEARNED ? P->row_failed : nullptr,
-      P->heavy_slot_base);
+      P->heavy_slot_base, LEARNED ? P->item_off : nullptr);
   note_launch();
   BCLX_CK_LAUNCH();
   return BCLX_OK;
@@ -1988,7 +2015,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
     note_launch();
     BCLX_CK_LAUNCH();
     k_learned_cut<false><<<hb, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, params ? P->pred : nullptr,
-                                                      P->ub, P->block_ub, P->heavy_nitems, nullptr, nullptr);
+                                                      P->ub, P->block_ub, P->heavy_nitems, nullptr, nullptr, nullptr);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -2009,16 +2036,25 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   P->n_heavy_items = tails[0];
   const int64_t light_total = tails[1];
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_items, P->n_heavy_items));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->item_cap, P->n_heavy_items));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->item_off, P->n_heavy_items + 1));
   if (P->n_heavy > 0) {
     k_learned_cut<true><<<hb, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, params ? P->pred : nullptr,
-                                                     P->ub, P->block_ub, nullptr, P->heavy_first, P->heavy_items);
+                                                     P->ub, P->block_ub, nullptr, P->heavy_first, P->heavy_items,
+                                                     P->item_cap);
     note_launch();
     BCLX_CK_LAUNCH();
   }
+  // heavy items' temp slots: their sizes, in item order
+  BCLX_TRY(exclusive_scan_i32(ctx, P->item_cap, P->item_off, P->n_heavy_items));
+  int64_t heavy_total = 0;
+  BCLX_CK(cudaMemcpyAsync(&heavy_total, P->item_off + P->n_heavy_items, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));
 
   // one numeric pass into temp slots
   P->heavy_slot_base = light_total;  // heavy item slots follow the light rows' slots
-  P->temp_entries = light_total + P->n_heavy_items * (int64_t)kVcap;
+  P->temp_entries = light_total + heavy_total;
   BCLX_TRY(scratch_alloc_n(ctx, &P->temp_col, P->temp_entries));
   BCLX_TRY(scratch_alloc(ctx, &P->temp_val, 4 * (size_t)(P->temp_entries > 0 ? P->temp_entries : 1)));
   BCLX_TRY(scratch_alloc_n(ctx, &P->item_count, P->n_heavy_items));
@@ -2127,7 +2163,7 @@ static int learned_finish_impl(Context* ctx, bclx_spgemm_plan_s* P, int32_t* out
   k_compact<VT><<<grid_for(ctx, units, 8, 8), 256, 0, ctx->stream>>>(
       P->g, P->light_list, (int)P->n_light, P->light_slot, P->heavy_list, P->heavy_items, P->n_heavy_items,
       P->heavy_first, P->item_count, P->item_pos, P->row_failed, P->failed_list, (int)P->n_failed,
-      P->heavy_slot_base, P->redo_off,
+      P->heavy_slot_base, P->item_off, P->redo_off,
       P->row_count, P->row_offset, P->temp_col, reinterpret_cast<const VT*>(P->temp_val), P->redo_col,
       reinterpret_cast<const VT*>(P->redo_val), out_col, reinterpret_cast<VT*>(out_val));
   note_launch();

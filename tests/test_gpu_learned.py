@@ -112,20 +112,25 @@ def test_learned_product_bit_identical(predictor, which, value_type):
         assert st["rows_redone"] > 0
 
 
-def test_learned_gain_over_predictor_free_cut(predictor):
-    """What the network buys: sized from predicted counts, the single pass
-    reserves far less temporary space than when sized from product counts
-    (the predictor-free bound), while mispredicting few rows."""
+def test_learned_gain_over_predictor_free_cut():
+    """What the network buys: heavy rows cut and their temporary slots sized
+    from predicted counts give fewer items and less temporary space than
+    when both come from product counts (the predictor-free upper bound),
+    while mispredicting few rows."""
     from bcl_b200.containers import BlockCustom, SPMatrix, learned_stats, spgemm_learned
-    a = gen.rmat(13, seed=78)
-    A = SPMatrix.from_csr(a, BlockCustom((2048, 2048)))
-    _, p1 = spgemm_learned(A, A, predictor=predictor, keep_plan=True)
+    # a 27-point stencil squared: 729 products per row for 125 outputs, so
+    # the product-count bound is loose and a good prediction pays
+    a = gen.stencil27(32)
+    A = SPMatrix.from_csr(a, BlockCustom((4096, 4096)))
+    from bcl_b200 import learned
+    trained = learned.get_default(train_if_missing=False)  # the packaged network
+    _, p1 = spgemm_learned(A, A, predictor=trained, keep_plan=True)
     with_net = learned_stats(p1)
     p1.close()
     _, p0 = spgemm_learned(A, A, predictor=None, keep_plan=True)
     without = learned_stats(p0)
     p0.close()
     print(f"\nwith network: {with_net}\nwithout:      {without}")
-    assert with_net["heavy_items"] < without["heavy_items"]
-    assert with_net["temp_entries"] < 0.8 * without["temp_entries"]
+    assert with_net["heavy_items"] < 0.8 * without["heavy_items"]
+    assert with_net["temp_entries"] < 0.7 * without["temp_entries"]
     assert with_net["rows_redone"] <= 0.05 * with_net["heavy_rows"]
