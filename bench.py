@@ -79,27 +79,39 @@ def parse_args():
 
 
 class Dist:
-    def __init__(self):
+    """One process per GPU (torchrun env).  Each rank multiplies its own
+    independent matrix of the workload (seed + rank): no data-path
+    collective; the process group carries only the barrier around the timed
+    region and the max of the ranks' times.  NCCL on GPUs; gloo where there
+    is no GPU (the host-side logic is tested that way)."""
+
+    def __init__(self, backend=None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.backend = None
         if self.world > 1:
             import datetime
+            import torch
             import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=300))
             self.pg = dist
 
     def barrier(self):
         if self.pg:
             import torch
-            self.pg.barrier(device_ids=[torch.cuda.current_device()])
+            if self.backend == "nccl":
+                self.pg.barrier(device_ids=[torch.cuda.current_device()])
+            else:
+                self.pg.barrier()
 
     def max(self, x: float) -> float:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -163,6 +175,12 @@ class ClockSampler:
 
 
 # ---- helpers ------------------------------------------------------------------------
+
+
+def job_rate(world, work_per_rank_step, steps, max_seconds):
+    """Whole-job throughput: every rank did the same work per step (weak
+    scaling); the job took the slowest rank's time."""
+    return world * work_per_rank_step * steps / max_seconds
 
 
 def tile_nnz_grid(csr, tm, tn):
@@ -325,7 +343,7 @@ def bench_spgemm(args, wl, dist, device):
     num_ms = [e[2].elapsed_time(e[3]) for e in ev]
     total_s = dist.max(sum(step_ms) / 1e3)
     ms_per_step = total_s * 1e3 / args.steps
-    value = dist.world * flops * args.steps / total_s / 1e9
+    value = job_rate(dist.world, flops, args.steps, total_s) / 1e9
 
     c_tiles = G * G
     alg = spgemm_alg_bytes(a_nnz, a_nnz, n, n, ts, ts, nnz_c, c_tiles)
@@ -409,7 +427,7 @@ def bench_spgemm_e2e(args, A, stream, flops, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     t = dist.max(e0.elapsed_time(e1) / 1e3)
-    return {"value": dist.world * flops * args.steps / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+    return {"value": job_rate(dist.world, flops, args.steps, t) / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3 / args.steps}
 
 
@@ -632,7 +650,7 @@ def bench_spmm(args, wl, dist, device):
     step_ms = [e[0].elapsed_time(e[1]) for e in ev]
     total_s = dist.max(sum(step_ms) / 1e3)
     ms_per_step = total_s * 1e3 / args.steps
-    value = dist.world * flops * args.steps / total_s / 1e9
+    value = job_rate(dist.world, flops, args.steps, total_s) / 1e9
     hbm_peak, peak_kind = peaks()
     kern_s = statistics.mean(step_ms) / 1e3  # the step is the one k_spmm launch
     model = spmm_model_bytes(a, ts, G, N, es)
@@ -698,7 +716,7 @@ def bench_spmm_e2e(args, A, B, C, stream, flops, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     t = dist.max(e0.elapsed_time(e1) / 1e3)
-    return {"value": dist.world * flops * args.steps / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+    return {"value": job_rate(dist.world, flops, args.steps, t) / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3 / args.steps}
 
 
