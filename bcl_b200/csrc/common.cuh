@@ -47,7 +47,14 @@ struct Context {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   int64_t* pinned = nullptr;  // host readback slots
+  // A second stream for planning work that overlaps the main stream (created
+  // on first use), with events to fork from and join back to the main stream.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, fork2_ev = nullptr, join_ev = nullptr;
 };
+
+// Create ctx->side and its events if they do not exist yet.
+int ensure_side_stream(Context* ctx);
 
 // Stream-ordered scratch from the device's default memory pool (kept cached:
 // the release threshold is raised at context creation).

@@ -152,6 +152,15 @@ int exclusive_scan_i64(Context* ctx, const int64_t* in, int64_t* out, int64_t n)
   return exclusive_scan_impl(ctx, in, out, n);
 }
 
+int ensure_side_stream(Context* ctx) {
+  if (ctx->side) return BCLX_OK;
+  BCLX_CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+  BCLX_CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+  BCLX_CK(cudaEventCreateWithFlags(&ctx->fork2_ev, cudaEventDisableTiming));
+  BCLX_CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
+  return BCLX_OK;
+}
+
 }  // namespace bclx
 
 using namespace bclx;
@@ -202,6 +211,12 @@ int bclx_context_destroy(bclx_context_t c) {
   if (!ctx) return BCLX_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  for (cudaEvent_t e : {ctx->fork_ev, ctx->fork2_ev, ctx->join_ev})
+    if (e) cudaEventDestroy(e);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   delete ctx;
   return BCLX_OK;

@@ -1197,6 +1197,8 @@ struct bclx_spgemm_plan_s {
   int64_t* acc_tile_offset = nullptr;
 
   void release() {
+    // planning work on the side stream must be done before its scratch goes
+    if (ctx && ctx->side) cudaStreamSynchronize(ctx->side);
     if (graph) {
       cudaGraphExecDestroy(graph);
       graph = nullptr;
@@ -1279,9 +1281,19 @@ static unsigned grid_for(Context* ctx, int64_t work_warps, int warps_per_block, 
   return (unsigned)want;
 }
 
-static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P) {
+// With `side`, the very heavy rows (a block per row, few blocks) run on the
+// context's side stream beside the warp-per-row kernel; the caller joins the
+// side stream back before reading the counts.
+static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P,
+                           bool side = false) {
   if (P->n_vheavy > 0) {
-    k_symbolic_block<<<grid_for(ctx, P->n_vheavy, 1, 8), kWarpsSym * 32, 0, ctx->stream>>>(
+    cudaStream_t st = ctx->stream;
+    if (side) {
+      BCLX_CK(cudaEventRecord(ctx->fork2_ev, ctx->stream));
+      BCLX_CK(cudaStreamWaitEvent(ctx->side, ctx->fork2_ev, 0));
+      st = ctx->side;
+    }
+    k_symbolic_block<<<grid_for(ctx, P->n_vheavy, 1, 8), kWarpsSym * 32, 0, st>>>(
         A, B, P->g, P->heavy_list, (int)P->n_vheavy, P->row_count, P->heavy_bitmaps, P->hbm_words);
     note_launch();
     BCLX_CK_LAUNCH();
@@ -1372,14 +1384,23 @@ static int64_t btable_cap() {
   return e && *e ? std::strtoll(e, nullptr, 10) : kBTableMaxBytes;
 }
 
-static int build_btable(Context* ctx, const SpGridView& B, const Geom& g, bclx_spgemm_plan_s* P) {
+// With `side`, the table is allocated in stream order on the main stream and
+// built on `side` after a fork event.
+static int build_btable(Context* ctx, const SpGridView& B, const Geom& g, bclx_spgemm_plan_s* P,
+                        cudaStream_t side = nullptr) {
   const int64_t nbrows = g.gk * g.gn * g.tk;
   if ((int64_t)sizeof(int32_t) * nbrows * (g.nfb + 1) > btable_cap()) {
     P->tab = nullptr;
     return BCLX_OK;
   }
   BCLX_TRY(scratch_alloc_n(ctx, &P->tab, (size_t)nbrows * (g.nfb + 1)));
-  k_btable<<<grid_for(ctx, nbrows / 32 + 1, 8, 16), 256, 0, ctx->stream>>>(B, g, P->tab);
+  cudaStream_t st = ctx->stream;
+  if (side) {
+    BCLX_CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
+    BCLX_CK(cudaStreamWaitEvent(side, ctx->fork_ev, 0));
+    st = side;
+  }
+  k_btable<<<grid_for(ctx, nbrows / 32 + 1, 8, 16), 256, 0, st>>>(B, g, P->tab);
   note_launch();
   BCLX_CK_LAUNCH();
   return BCLX_OK;
@@ -1390,6 +1411,10 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
                          int32_t* tile_row_ptr, int64_t* tile_offset, bclx_spgemm_plan_s* P) {
   BCLX_TRY(build_stage_map(ctx, A, B, P, g));
   P->g = g;
+  // The B-row table depends on B alone: it is built on the side stream from
+  // the start, beside classification and the symbolic pass.
+  BCLX_TRY(ensure_side_stream(ctx));
+  BCLX_TRY(build_btable(ctx, B, g, P, ctx->side));
   P->dtype = dtype;
   const int64_t nri = g.n_row_items;
   P->hbm_words = (g.tn + 31) / 32;
@@ -1434,7 +1459,10 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_bitmaps, (size_t)P->n_heavy * P->hbm_words));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_nitems, P->n_heavy));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_first, P->n_heavy + 1));
-  BCLX_TRY(launch_symbolic(ctx, A, B, P));
+  BCLX_TRY(launch_symbolic(ctx, A, B, P, true));
+  // the side stream (B-row table, very heavy rows) joins before the scan
+  BCLX_CK(cudaEventRecord(ctx->join_ev, ctx->side));
+  BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
   BCLX_TRY(exclusive_scan_i32(ctx, P->row_count, P->row_offset, nri));
   const int64_t ntiles = g.gm * g.gn;
   k_tile_ptrs<<<grid_for(ctx, ntiles * (g.tm + 1) / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
@@ -1469,8 +1497,10 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
                                                        P->hbm_words, nullptr, P->heavy_first, P->heavy_items);
     note_launch();
     BCLX_CK_LAUNCH();
-    // B-row table for the heavy items' column ranges
-    BCLX_TRY(build_btable(ctx, B, g, P));
+  }
+  if (P->n_heavy == 0 && P->tab) {  // no heavy item reads the table
+    scratch_free(ctx, P->tab);
+    P->tab = nullptr;
   }
   return BCLX_OK;
 }
