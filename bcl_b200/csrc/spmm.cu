@@ -18,6 +18,9 @@
 // in FP32 registers and rounds each C element once when it is stored.
 #include "common.cuh"
 
+#include <algorithm>
+#include <cstdlib>
+
 namespace bclx {
 
 constexpr int kSpmmWarps = 8;
@@ -133,7 +136,7 @@ __device__ __forceinline__ bool tiles_aligned(const DGridView& B, const DGridVie
 // 16-byte vectors) are in flight before their multiply-adds are applied in
 // entry order.  `vec`: every B and C row slice of this tile pair is 16-byte
 // aligned; otherwise element-wise access.
-template <typename ST>
+template <typename ST, int UNROLL = kSpmmUnroll>
 __device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
                                          int64_t tj, int64_t r, int c0, int W, bool vec) {
   using V = Vec<ST>;
@@ -207,18 +210,18 @@ __device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B
       const int ne = min(32, atot - e0);
       const uint4* t = tb + buf * 32;
       if (vec) {
-        for (int u0 = 0; u0 < ne; u0 += kSpmmUnroll) {
-          uint4 ent[kSpmmUnroll];
-          uint4 raw[kSpmmUnroll];
+        for (int u0 = 0; u0 < ne; u0 += UNROLL) {
+          uint4 ent[UNROLL];
+          uint4 raw[UNROLL];
 #pragma unroll
-          for (int u = 0; u < kSpmmUnroll; u++) ent[u] = t[(u0 + u) & 31];
+          for (int u = 0; u < UNROLL; u++) ent[u] = t[(u0 + u) & 31];
 #pragma unroll
-          for (int u = 0; u < kSpmmUnroll; u++) {
+          for (int u = 0; u < UNROLL; u++) {
             const ST* rp = reinterpret_cast<const ST*>((uint64_t)ent[u].x | ((uint64_t)ent[u].y << 32));
             if (u0 + u < ne && own) raw[u] = __ldg(reinterpret_cast<const uint4*>(rp + col));
           }
 #pragma unroll
-          for (int u = 0; u < kSpmmUnroll; u++) {
+          for (int u = 0; u < UNROLL; u++) {
             if (u0 + u < ne && own) {
               float b[VN];
               V::unpack_raw(raw[u], b);
@@ -260,7 +263,8 @@ __device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B
 
 template <typename ST>
 __global__ void __launch_bounds__(kSpmmWarps * 32)
-    k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int row_align_ok) {
+    k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int row_align_ok,
+           const uint8_t* __restrict__ long_flag) {
   constexpr int PW = 32 * Vec<ST>::N;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -275,8 +279,73 @@ __global__ void __launch_bounds__(kSpmmWarps * 32)
     const int c0 = panel * PW;
     if (c0 >= W) continue;
     const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
+    if (long_flag && vec && long_flag[ti * C.tm + r]) continue;  // k_spmm_long takes it
     spmm_row<ST>(A, B, C, ti, tj, r, c0, W, vec);
   }
+}
+
+// ---- long rows ----------------------------------------------------------------
+//
+// A row with thousands of entries is one chain of multiply-adds per output
+// element (the reference's order), so a warp with 8 B-row loads in flight
+// spends milliseconds on it.  Such rows are found first (k_spmm_find_long),
+// skipped by k_spmm and run by k_spmm_long on the context's side stream at
+// the same time: one warp per (row, C tile column, panel), the same walk
+// with kLongUnroll B-row loads in flight per lane (warps with the registers
+// for it: few of them, each on one long chain).
+
+constexpr int kLongUnroll = 32;  // B-row loads in flight per lane on long rows (half for BF16: registers)
+constexpr int kLongWarps = 4;
+constexpr int kSpmmLongRow = 1024;         // entries over all stages
+constexpr int64_t kSpmmLongMinRows = 65536;  // smaller products do not use the long-row path
+
+// Thread per A row (ti, r): entries over all stages; rows with at least
+// long_row are flagged and listed.
+__global__ void k_spmm_find_long(SpGridView A, int long_row, uint8_t* __restrict__ flag, int64_t* __restrict__ list,
+                                 int32_t* __restrict__ count) {
+  const int64_t rows = A.gm * A.tm;
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < rows; x += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ti = x / A.tm, r = x - ti * A.tm;
+    int64_t tot = 0;
+    if (r < A.rows_of(ti))
+      for (int64_t k = 0; k < A.gn; k++) {
+        const int32_t* rp = A.tile(ti, k).row_ptr;
+        tot += __ldg(rp + r + 1) - __ldg(rp + r);
+      }
+    const bool lng = tot >= long_row;
+    flag[x] = lng ? 1 : 0;
+    if (lng) list[atomicAdd(count, 1)] = x;
+  }
+}
+
+template <typename ST>
+__global__ void __launch_bounds__(kLongWarps * 32)
+    k_spmm_long(SpGridView A, DGridView B, DGridView C, const int64_t* __restrict__ list,
+                const int32_t* __restrict__ count, int npanels, int row_align_ok) {
+  constexpr int PW = 32 * Vec<ST>::N;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t nl = *count;
+  const int64_t n = nl * C.gn * npanels;
+  for (int64_t w = warp; w < n; w += nwarps) {
+    // consecutive warps take different rows; a row's panels are spread out
+    const int64_t li = w % nl;
+    const int64_t pt = w / nl;
+    const int panel = (int)(pt % npanels);
+    const int64_t tj = pt / npanels;
+    const int64_t x = list[li];
+    const int64_t ti = x / A.tm, r = x - ti * A.tm;
+    const int W = (int)C.cols_of(tj);
+    if (panel * PW >= W) continue;
+    const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
+    if (!vec) continue;  // k_spmm did this one element-wise
+    spmm_row<ST, sizeof(ST) == 4 ? kLongUnroll : kLongUnroll / 2>(A, B, C, ti, tj, r, panel * PW, W, true);
+  }
+}
+
+static int64_t spmm_long_min_rows() {
+  const char* e = std::getenv("BCLX_SPMM_LONG_MIN_ROWS");
+  return e && *e ? std::strtoll(e, nullptr, 10) : kSpmmLongMinRows;
 }
 
 template <typename ST>
@@ -287,10 +356,40 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   if (n_items == 0) return BCLX_OK;
   const int64_t want = ceil_div(n_items, kSpmmWarps);
   const int64_t cap = (int64_t)ctx->num_sms * 8;
+  const int64_t arows = A.gm * A.tm;
+  const bool long_path = align_ok && A.gn <= 32 && arows >= spmm_long_min_rows();
+  uint8_t* flag = nullptr;
+  int64_t* list = nullptr;
+  int32_t* cnt = nullptr;
+  if (long_path) {
+    // find the long rows, then run them on the side stream beside k_spmm
+    BCLX_TRY(ensure_side_stream(ctx));
+    BCLX_TRY(scratch_alloc_n(ctx, &flag, (size_t)arows));
+    BCLX_TRY(scratch_alloc_n(ctx, &list, (size_t)arows));
+    BCLX_TRY(scratch_alloc_n(ctx, &cnt, 1));
+    BCLX_CK(cudaMemsetAsync(cnt, 0, sizeof(int32_t), ctx->stream));
+    k_spmm_find_long<<<(unsigned)std::min<int64_t>(ceil_div(arows, 256), (int64_t)ctx->num_sms * 16), 256, 0,
+                       ctx->stream>>>(A, kSpmmLongRow, flag, list, cnt);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    BCLX_CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
+    BCLX_CK(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+    k_spmm_long<ST><<<(unsigned)ctx->num_sms, kLongWarps * 32, 0, ctx->side>>>(A, B, C, list, cnt, npanels,
+                                                                                align_ok);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    BCLX_CK(cudaEventRecord(ctx->join_ev, ctx->side));
+  }
   k_spmm<ST><<<(unsigned)(want < cap ? want : cap), kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels,
-                                                                                        align_ok);
+                                                                                        align_ok, flag);
   note_launch();
   BCLX_CK_LAUNCH();
+  if (long_path) {
+    BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
+    scratch_free(ctx, flag);
+    scratch_free(ctx, list);
+    scratch_free(ctx, cnt);
+  }
   return BCLX_OK;
 }
 

@@ -78,6 +78,59 @@ def test_spmm_bf16(n, tiles):
     assert err < 1e-2
 
 
+def heavy_rows_matrix(n=16384, light=8, heavy=(12000, 9000, 6000, 4500, 1024, 1023), seed=11):
+    """Mostly `light` entries per row, a few empty rows, and a few rows long
+    enough for the long-row kernel (1024 or more entries over all stages)
+    with one just below."""
+    rng = np.random.default_rng(seed)
+    lens = np.full(n, light, np.int64)
+    lens[rng.choice(n, size=300, replace=False)] = 0
+    rows = rng.choice(n, size=len(heavy), replace=False)
+    lens[rows] = heavy
+    cols = [np.sort(rng.choice(n, size=int(k), replace=False)) for k in lens]
+    row_ptr = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=row_ptr[1:])
+    col_ind = np.concatenate(cols).astype(np.int32)
+    vals = rng.uniform(-1, 1, size=col_ind.size).astype(np.float32)
+    return gen.CSR(n, n, row_ptr.astype(np.int32), col_ind, vals)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+@pytest.mark.parametrize("tiles", [(4096, 4096, 256), (16384, 16384, 256), (3000, 5000, 200), (1000, 1024, 128)])
+def test_spmm_long_rows(monkeypatch, dtype, tiles):
+    """Rows of thousands of entries run by the long-row kernel on the side
+    stream (its panels and tile columns spread over warps) while the rest
+    run as usual; enabled here below its size threshold."""
+    monkeypatch.setenv("BCLX_SPMM_LONG_MIN_ROWS", "0")
+    a = heavy_rows_matrix()
+    n = tiles[2] if tiles[2] in (128, 256) else 400
+    b = gen.dense(a.n, n, seed=12, dist="normal")
+    c0 = gen.dense(a.m, n, seed=13)
+    if dtype == "f32":
+        got = run(a, b, tiles, c0=c0)
+        want = O.spmm_tiled(a, b, c0, *tiles)
+        assert np.array_equal(bits(got), bits(want))
+    else:
+        b16, c16 = O.to_bf16(b), O.to_bf16(c0)
+        got = run(a, b16, tiles, dtype="bf16", c0=c16)
+        want = O.spmm_tiled_bf16(a, b16, c16, *tiles)
+        assert np.array_equal(got, want)
+
+
+def test_spmm_ragged_last_tile_unaligned_width(monkeypatch):
+    """Aligned leading dimension but a last tile column whose width is not a
+    whole number of 16-byte vectors: element-wise access for that tile (and
+    the long-row kernel leaves its long rows to the element-wise form)."""
+    monkeypatch.setenv("BCLX_SPMM_LONG_MIN_ROWS", "0")
+    a = heavy_rows_matrix(n=4096, heavy=(3000, 2000))
+    b = gen.dense(a.n, 38, seed=15)
+    c0 = gen.dense(a.m, 38, seed=16)
+    tiles = (1000, 1500, 24)
+    got = run(a, b, tiles, c0=c0)
+    want = O.spmm_tiled(a, b, c0, *tiles)
+    assert np.array_equal(bits(got), bits(want))
+
+
 def test_spmm_tile_single_call_ld():
     """bclx_spmm_tile with leading dimensions larger than n (sub-blocks)."""
     import ctypes
