@@ -154,7 +154,11 @@ int exclusive_scan_i64(Context* ctx, const int64_t* in, int64_t* out, int64_t n)
 
 int ensure_side_stream(Context* ctx) {
   if (ctx->side) return BCLX_OK;
-  BCLX_CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+  // highest priority: work forked to the side stream (long SpMM rows, the
+  // SpGEMM B-row table) gets SMs ahead of the main stream's blocks
+  int lo = 0, hi = 0;
+  BCLX_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  BCLX_CK(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, hi));
   BCLX_CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
   BCLX_CK(cudaEventCreateWithFlags(&ctx->fork2_ev, cudaEventDisableTiming));
   BCLX_CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
