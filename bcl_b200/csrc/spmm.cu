@@ -82,7 +82,7 @@ struct Vec<__nv_bfloat16> {
   __device__ __forceinline__ static void unpack_raw(uint4 v, float* out) { unpack(v, out); }
 };
 
-constexpr int kSpmmUnroll = 8;  // B-row loads in flight per lane
+constexpr int kSpmmUnroll = 4;  // B-row loads in flight per lane (with 32 warps per SM)
 
 // Ask L2 for the 128-byte lines of [p, p + bytes) (no-op for null).
 __device__ __forceinline__ void l2_prefetch_slice(const void* p, int bytes) {
@@ -262,7 +262,7 @@ __device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B
 }
 
 template <typename ST>
-__global__ void __launch_bounds__(kSpmmWarps * 32)
+__global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int row_align_ok,
            const uint8_t* __restrict__ long_flag) {
   constexpr int PW = 32 * Vec<ST>::N;
