@@ -55,7 +55,9 @@ class Context:
 
     def use_current_stream(self):
         s = torch.cuda.current_stream(self.device).cuda_stream
-        call("bclx_context_set_stream", self.h, ctypes.c_void_p(s))
+        if s != getattr(self, "_stream", None):  # the C call only when the stream changes
+            call("bclx_context_set_stream", self.h, ctypes.c_void_p(s))
+            self._stream = s
         return self.h
 
     def release_cached(self):
@@ -236,8 +238,12 @@ class SPMatrix:
         return int(self._offsets()[-1])
 
     def spgrid(self) -> SpGrid:
-        return SpGrid(self.m, self.n, self.tm, self.tn, self.gm, self.gn, self.desc.data_ptr(),
-                      _NP_TO_DT[self.dtype], 0)
+        key = self.desc.data_ptr()
+        g = getattr(self, "_spgrid", None)
+        if g is None or g[0] != key:  # built once per descriptor array
+            g = (key, SpGrid(self.m, self.n, self.tm, self.tn, self.gm, self.gn, key, _NP_TO_DT[self.dtype], 0))
+            self._spgrid = g
+        return g[1]
 
     def tile_desc_ptr(self, index) -> int:
         """Device address of one tile's bclx_csr_t (a 1x1 grid view of it)."""
@@ -397,7 +403,12 @@ class DMatrix:
         raise TypeError("DMatrix tiles must be float32 or bfloat16")
 
     def dgrid(self) -> DGrid:
-        return DGrid(self.m, self.n, self.tm, self.tn, self.gm, self.gn, self.ptrs.data_ptr(), self.bclx_dtype, 0)
+        key = self.ptrs.data_ptr()
+        g = getattr(self, "_dgrid", None)
+        if g is None or g[0] != key:  # built once per tile-pointer array
+            g = (key, DGrid(self.m, self.n, self.tm, self.tn, self.gm, self.gn, key, self.bclx_dtype, 0))
+            self._dgrid = g
+        return g[1]
 
 
 # ---- products -----------------------------------------------------------------------
