@@ -165,15 +165,47 @@ class SPMatrix:
     # -- construction
     @classmethod
     def from_csr(cls, a: CSR, blocking: BlockCustom, device: Optional[int] = None) -> "SPMatrix":
-        """Tile a host matrix and upload it (the SPMatrix(fname, blocking)
-        constructor's slicing, SPMatrix.hpp:211-271, from an in-memory CSR)."""
+        """Upload a host matrix and tile it on the device (the SPMatrix(fname,
+        blocking) constructor's slicing, SPMatrix.hpp:211-271, from an
+        in-memory CSR whose columns are ascending within each row)."""
         dev = torch.cuda.current_device() if device is None else device
         tm, tn = blocking.seed(a.m, a.n)
-        trp, toff, ci, v = split_tiles(a, tm, tn)
         td = torch.device("cuda", dev)
-        return cls(a.m, a.n, tm, tn, a.vals.dtype, dev,
-                   torch.from_numpy(trp).to(td), torch.from_numpy(toff).to(td),
-                   torch.from_numpy(ci).to(td), torch.from_numpy(np.ascontiguousarray(v)).to(td))
+        rp = torch.from_numpy(a.row_ptr.astype(np.int32)).to(td)
+        ci = torch.from_numpy(a.col_ind.astype(np.int32)).to(td)
+        v = torch.from_numpy(np.ascontiguousarray(a.vals)).to(td)
+        return cls.from_device_csr(a.m, a.n, rp, ci, v, (tm, tn), device=dev)
+
+    @classmethod
+    def from_device_csr(cls, m: int, n: int, row_ptr: torch.Tensor, col_ind: torch.Tensor, vals: torch.Tensor,
+                        tile_shape: Tuple[int, int], device: Optional[int] = None) -> "SPMatrix":
+        """Tile a CSR matrix already in device memory (int32 row_ptr [m+1] and
+        col_ind, FP32 or int32 vals; columns ascending within each row)
+        into a tile_m x tile_n grid, on the device (bclx_csr_to_tiles)."""
+        dev = torch.cuda.current_device() if device is None else device
+        tm, tn = int(tile_shape[0]), int(tile_shape[1])
+        gm, gn = _ceil_div(m, tm), _ceil_div(n, tn)
+        td = torch.device("cuda", dev)
+        nnz = int(col_ind.numel())
+        np_dtype = np.dtype(np.float32) if vals.dtype == torch.float32 else np.dtype(np.int32)
+        dt = _NP_TO_DT[np_dtype]
+        trp = torch.empty((gm * gn, tm + 1), dtype=torch.int32, device=td)
+        toff = torch.zeros(gm * gn + 1, dtype=torch.int64, device=td)
+        oci = torch.empty(max(nnz, 1), dtype=torch.int32, device=td)
+        ov = torch.empty(max(nnz, 1), dtype=vals.dtype, device=td)
+        desc = CSRDesc(m, n, nnz, row_ptr.data_ptr(), col_ind.data_ptr() if nnz else 0,
+                       vals.data_ptr() if nnz else 0, dt, 0)
+        out = SpGridOut(m, n, tm, tn, gm, gn, trp.data_ptr(), toff.data_ptr(), oci.data_ptr(), ov.data_ptr(), dt, 0)
+        call("bclx_csr_to_tiles", context(dev).use_current_stream(), ctypes.byref(desc), ctypes.byref(out))
+        return cls(m, n, tm, tn, np_dtype, dev, trp, toff, oci[:nnz], ov[:nnz])
+
+    @classmethod
+    def from_file(cls, path: str, blocking: BlockCustom, value_dtype=np.float32,
+                  device: Optional[int] = None) -> "SPMatrix":
+        """SPMatrix(fname, blocking) (SPMatrix.hpp:108-113, 194-271): a
+        MatrixMarket (.mtx) or binary (.binary) file, tiled on the device."""
+        from . import gen
+        return cls.from_csr(gen.read_matrix(path, value_dtype), blocking, device)
 
     @classmethod
     def zeros(cls, shape: Tuple[int, int], blocking: BlockCustom, dtype=np.float32,
@@ -260,8 +292,25 @@ class SPMatrix:
         return CSR(m, n, rp, ci, v)
 
     def get(self) -> CSR:
-        """Gather the whole matrix to the host in global coordinates
-        (SPMatrix::get, SPMatrix.hpp:516-546)."""
+        """Gather the whole matrix in global coordinates on the device
+        (bclx_tiles_to_csr) and return it on the host (SPMatrix::get,
+        SPMatrix.hpp:516-546)."""
+        rp, ci, v = self.get_device()
+        return CSR(self.m, self.n, rp.cpu().numpy(), ci.cpu().numpy(), v.cpu().numpy())
+
+    def get_device(self):
+        """The whole matrix as device CSR arrays (row_ptr, col_ind, vals)."""
+        nnz = int(self._offsets()[-1])
+        td = self.tile_row_ptr.device
+        rp = torch.empty(self.m + 1, dtype=torch.int32, device=td)
+        ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=td)
+        v = torch.empty(max(nnz, 1), dtype=self.vals.dtype, device=td)
+        call("bclx_tiles_to_csr", context(self.device).use_current_stream(), ctypes.byref(self.spgrid()),
+             ctypes.c_void_p(rp.data_ptr()), ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(v.data_ptr()))
+        return rp, ci[:nnz], v[:nnz]
+
+    def get_host_gather(self) -> CSR:
+        """The same gather done with numpy on the host (kept for checks)."""
         o = self._offsets()
         nnz = int(o[-1])
         trp = self.tile_row_ptr.cpu().numpy().astype(np.int64)

@@ -208,6 +208,90 @@ def read_binary(path: str, value_dtype=np.float32) -> CSR:
     return CSR(m, n, row_ptr, col_ind, vals)
 
 
+# ---- MatrixMarket (matrix_io.hpp:218-356, CSRMatrix.hpp:370-410, 533-547) ----
+
+def read_matrix_market(path: str, value_dtype=np.float32, one_indexed: bool = True) -> CSR:
+    """Read a coordinate MatrixMarket file as the reference's mmread does:
+    `general` or `symmetric` (an off-diagonal entry is also stored
+    transposed), `pattern` values read as 1; an index repeated later in the
+    file is ignored (the first one stays); entries sorted by (row, column).
+    Other formats, indices out of range and more entries than announced are
+    errors."""
+    with open(path, "r") as f:
+        header = f.readline().split()
+        if len(header) < 5 or header[0] != "%%MatrixMarket" or header[1] != "matrix" or header[2] != "coordinate":
+            raise RuntimeError(f"{path} could not be parsed as a Matrix Market file.")
+        pattern = header[3] == "pattern"
+        if header[4] == "general":
+            symmetric = False
+        elif header[4] == "symmetric":
+            symmetric = True
+        else:
+            raise RuntimeError(f"{path} has an unsupported matrix type")
+        line = f.readline()
+        while line.startswith("%"):
+            line = f.readline()
+        m, n, nnz = (int(x) for x in line.split()[:3])
+        body = f.read()
+    ncol = 2 if pattern else 3
+    tok = np.array(body.split(), dtype=object)
+    if tok.size % ncol:
+        raise RuntimeError(f"read_MatrixMarket: malformed entry lines in {path}")
+    tok = tok.reshape(-1, ncol)
+    if tok.shape[0] > nnz:
+        raise RuntimeError("read_MatrixMarket: error reading Matrix Market file, file has more nonzeros than reported.")
+    i = tok[:, 0].astype(np.int64)
+    j = tok[:, 1].astype(np.int64)
+    if one_indexed:
+        i -= 1
+        j -= 1
+    if ((i < 0) | (i >= m) | (j < 0) | (j >= n)).any():
+        raise RuntimeError("read_MatrixMarket: file has nonzero out of bounds.")
+    if pattern:
+        v = np.ones(i.size, dtype=value_dtype)
+    elif np.dtype(value_dtype).kind == "f":
+        v = tok[:, 2].astype(np.float64).astype(value_dtype)
+    else:
+        v = tok[:, 2].astype(np.float64).astype(np.int64).astype(value_dtype)
+    if symmetric:  # each line inserts (i, j), then (j, i) off the diagonal
+        off = i != j
+        k = np.arange(i.size, dtype=np.int64)
+        i = np.concatenate([i, j[off]])
+        j2 = np.concatenate([j, i[: k.size][off]])
+        order_key = np.concatenate([2 * k, 2 * k[off] + 1])  # insertion order
+        v = np.concatenate([v, v[off]])
+        j = j2
+    else:
+        order_key = np.arange(i.size, dtype=np.int64)
+    key = i * n + j
+    # first insertion of every index wins
+    o = np.lexsort((order_key, key))
+    keep = np.ones(o.size, dtype=bool)
+    keep[1:] = key[o][1:] != key[o][:-1]
+    o = o[keep]
+    return _csr_from_sorted_keys(key[o], m, n, v[o])
+
+
+def write_matrix_market(path: str, mat: CSR) -> None:
+    """CSRMatrix::write_MatrixMarket: an `integer general` header, then one
+    `row col value` line per entry (1-based, value printed with %f)."""
+    rows = np.repeat(np.arange(mat.m, dtype=np.int64), np.diff(mat.row_ptr.astype(np.int64)))
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate integer general\n")
+        f.write(f"{mat.m} {mat.n} {mat.nnz}\n")
+        for r, c, x in zip(rows + 1, mat.col_ind.astype(np.int64) + 1, mat.vals):
+            f.write(f"{r} {c} {float(x):f}\n")
+
+
+def read_matrix(path: str, value_dtype=np.float32) -> CSR:
+    """By suffix, as matrix_io::detect_file_type: .mtx or .binary."""
+    if path.endswith(".mtx"):
+        return read_matrix_market(path, value_dtype)
+    if path.endswith(".binary"):
+        return read_binary(path, value_dtype)
+    raise RuntimeError(f"matrix_info: Could not detect file format for \"{path}\"")
+
+
 def write_dense(path: str, arr: np.ndarray) -> None:
     """``int64 m, n``; ``T data[m*n]`` row-major."""
     with open(path, "wb") as f:

@@ -466,6 +466,10 @@ def spgemm_extras(args, A, a, ts, products, stream):
         ex["learned"] = learned_summary(A, products, stream)
     except Exception as e:  # keep the headline line even if an extra fails
         ex["learned"] = {"error": repr(e)}
+    try:
+        ex["tiling"] = tiling_summary(a, ts, stream)
+    except Exception as e:
+        ex["tiling"] = {"error": repr(e)}
     if A.gn <= 16:
         try:
             ex["spmm_er16k"] = spmm_summary(args, stream)
@@ -556,6 +560,33 @@ def spmm_precision_summary(args, stream):
     out["bf16_speedup"] = times["fp32"] / times["bf16"]
     out["alg_bytes_model"] = "A once (8 B/entry + row pointers per tile), B once, C read and written once"
     return out
+
+
+def tiling_summary(a, ts, stream):
+    """The input path on the device: slicing A (already a device CSR) into
+    its tile grid (bclx_csr_to_tiles) and gathering it back
+    (bclx_tiles_to_csr), against the host slicing of the same matrix."""
+    import torch
+    from bcl_b200.containers import SPMatrix, split_tiles
+    rp = torch.from_numpy(a.row_ptr.astype(np.int32)).cuda()
+    ci = torch.from_numpy(a.col_ind).cuda()
+    v = torch.from_numpy(a.vals).cuda()
+    holder = {}
+
+    def tile():
+        holder["S"] = SPMatrix.from_device_csr(a.m, a.n, rp, ci, v, (ts, ts))
+    t_tile = time_region(tile, 5, stream)
+    S = holder["S"]
+    t_gather = time_region(lambda: S.get_device(), 5, stream)
+    t0 = time.perf_counter()
+    split_tiles(a, ts, ts)
+    t_host = time.perf_counter() - t0
+    ntiles = S.gm * S.gn
+    # bytes read and written once: CSR in (row_ptr, col, val), tiles out (row ptrs, offsets, col, val)
+    moved = 4 * (a.m + 1) + 8 * a.nnz + 4 * ntiles * (ts + 1) + 8 * (ntiles + 1) + 8 * a.nnz
+    return {"nnz": a.nnz, "tile_ms": t_tile * 1e3, "tile_gbs": moved / t_tile / 1e9,
+            "gather_ms": t_gather * 1e3, "gather_gbs": moved / t_gather / 1e9,
+            "host_slicing_ms": t_host * 1e3, "note": "device slicing includes one host read (validation)"}
 
 
 def spmm_summary(args, stream):

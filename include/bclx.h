@@ -18,6 +18,9 @@
  *                                     colind, ldb, ldc), spgemm.hpp:140-149 (80-96)
  *   bclx_spmm_grid                    BCL::gemm(SPMatrix, DMatrix, DMatrix&)
  *                                     spgemm.hpp:153-179
+ *   bclx_csr_to_tiles                 SPMatrix(fname, blocking) slicing,
+ *                                     SPMatrix.hpp:194-271
+ *   bclx_tiles_to_csr                 SPMatrix::get, SPMatrix.hpp:516-546
  *
  * Semantics kept from the reference:
  *   - output structure is the symbolic pattern (entries that sum to zero are
@@ -267,6 +270,23 @@ BCLX_API int bclx_tile_accumulate_numeric(bclx_context_t ctx, bclx_spgemm_plan_t
 BCLX_API int bclx_spgemm_tile_noalloc(const bclx_csr_t* a, const bclx_csr_t* b, int32_t* c_row_ptr,
                                       int32_t* c_col_ind, void* c_vals, int64_t c_capacity, int64_t* c_nnz,
                                       void* stream);
+
+/* ---- whole matrix <-> tile grid ---------------------------------------------
+ * Slice a CSR matrix (device arrays, columns ascending within each row, as
+ * CSRMatrix holds them) into the packed tile layout of `out` (m, n,
+ * tile_m, tile_n, grid_m, grid_n and all four arrays set by the caller;
+ * col_ind and vals hold a->nnz entries; dtype F32 or I32).  Replaces the
+ * SPMatrix(fname, blocking) constructor's slicing (SPMatrix.hpp:194-271,
+ * CSRMatrix::get_slice_impl_ CSRMatrix.hpp:238-276), done on the device.
+ * Rows whose columns are not ascending or out of range: BCLX_ERR_INVALID,
+ * nothing written to col_ind/vals.  Synchronizes the context's stream. */
+BCLX_API int bclx_csr_to_tiles(bclx_context_t ctx, const bclx_csr_t* a, bclx_spgrid_out_t* out);
+/* Gather every tile of `g` into one CSR matrix: row_ptr [m+1], col_ind and
+ * vals [nnz] (nnz = sum of tile nnz), global columns, each row's tiles in
+ * column order.  Replaces SPMatrix::get (SPMatrix.hpp:516-546), on the
+ * device.  Reads nnz back once (synchronizes). */
+BCLX_API int bclx_tiles_to_csr(bclx_context_t ctx, const bclx_spgrid_t* g, int32_t* row_ptr, int32_t* col_ind,
+                               void* vals);
 
 /* ---- sparse x dense ------------------------------------------------------
  * C += A * B for one tile (spmm_wrapper, spgemm.hpp:140-149): A is m x k CSR

@@ -17,6 +17,9 @@
 //   bcl_ref spmm   <A.binary> <B.dense>  <tm> <tk> <tn> <out.dense|-> <warmup> <reps>
 //   bcl_ref dot    <A.binary> <B.binary> <f32|i32> <out.binary>
 //   bcl_ref accumulate <f32|i32> <out.binary> <P1.binary> [P2.binary ...]
+//   bcl_ref mmread <in.mtx> <f32|i32> <out.binary>      (CSRMatrix(fname): MatrixMarket reader)
+//   bcl_ref tiles  <A.binary> <tm> <tn> <f32|i32> <out> (SPMatrix(fname, BlockCustom) slicing:
+//                  every tile's CSR, row-major over the grid, one binary record after another)
 // Prints one JSON line with the per-rep wall times of BCL::gemm.
 
 #include <bcl/bcl.hpp>
@@ -28,6 +31,26 @@
 #include <cstring>
 #include <string>
 #include <vector>
+
+// Every tile of SPMatrix(fname, BlockCustom({tm, tn})), appended to `out` as
+// binary CSR records in row-major grid order.
+template <typename T>
+static int run_tiles(const std::string& fa, size_t tm, size_t tn, const std::string& out) {
+  BCL::SPMatrix<T, int> a(fa, BCL::BlockCustom({tm, tn}, {1, 1}));
+  FILE* f = fopen(out.c_str(), "wb");
+  if (!f) return 1;
+  for (size_t i = 0; i < a.grid_shape()[0]; i++)
+    for (size_t j = 0; j < a.grid_shape()[1]; j++) {
+      auto t = a.get_tile({i, j});
+      const size_t hdr[3] = {t.shape()[0], t.shape()[1], t.nnz_};
+      fwrite(hdr, sizeof(size_t), 3, f);
+      fwrite(t.vals_.data(), sizeof(T), t.nnz_, f);
+      fwrite(t.col_ind_.data(), sizeof(int), t.nnz_, f);
+      fwrite(t.row_ptr_.data(), sizeof(int), t.shape()[0] + 1, f);
+    }
+  fclose(f);
+  return 0;
+}
 
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -148,6 +171,17 @@ static int run_accumulate(int nparts, char** files, const std::string& out) {
 int main(int argc, char** argv) {
   if (argc < 2) { fprintf(stderr, "usage: see source header\n"); return 2; }
   std::string mode = argv[1];
+  if (mode == "mmread" && argc == 5) {  // no segment needed
+    std::string dt = argv[3];
+    if (dt == "f32") {
+      BCL::CSRMatrix<float, int> a(argv[2]);
+      a.write_Binary(argv[4]);
+    } else {
+      BCL::CSRMatrix<int, int> a(argv[2]);
+      a.write_Binary(argv[4]);
+    }
+    return 0;
+  }
   // Segment for tiles and the intermediate partial products (bcl_allocator);
   // the stub maps it lazily, so only touched pages are committed.
   const char* seg = getenv("BCLX_REF_SEGMENT_MB");
@@ -164,6 +198,10 @@ int main(int argc, char** argv) {
   } else if (mode == "dot" && argc == 6) {
     std::string dt = argv[4];
     rc = dt == "f32" ? run_dot<float>(argv[2], argv[3], argv[5]) : run_dot<int>(argv[2], argv[3], argv[5]);
+  } else if (mode == "tiles" && argc == 7) {
+    std::string dt = argv[5];
+    size_t tm = strtoull(argv[3], nullptr, 10), tn = strtoull(argv[4], nullptr, 10);
+    rc = dt == "f32" ? run_tiles<float>(argv[2], tm, tn, argv[6]) : run_tiles<int>(argv[2], tm, tn, argv[6]);
   } else if (mode == "accumulate" && argc >= 5) {
     std::string dt = argv[2];
     rc = dt == "f32" ? run_accumulate<float>(argc - 4, argv + 4, argv[3])

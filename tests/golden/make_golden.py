@@ -12,6 +12,11 @@ Each fixture is an .npz holding the inputs and the reference's outputs:
   order (SparseHashAccumulator.hpp:101-182).
 * ``spmm_*``: BCL::gemm(SPMatrix, DMatrix, DMatrix&) with C = 0 first
   (spgemm.hpp:153-179).
+* ``mm_*.mtx`` / ``mm_*.npz``: MatrixMarket files written here (duplicates,
+  comments, empty rows, symmetric, pattern, integer) and the CSR matrix the
+  reference's reader makes of each (CSRMatrix(fname), matrix_io.hpp:218-356).
+* ``tiles_*``: every tile of SPMatrix(fname, BlockCustom) (the reference's
+  slicing, SPMatrix.hpp:194-271), row-major over the grid.
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -122,5 +127,79 @@ def main():
         print(f"spmm_{name}: C {c.shape}")
 
 
+def _mtx_lines(rng, m, n, count, field, symmetric):
+    i = rng.integers(0, m, count)
+    j = rng.integers(0, n, count)
+    if symmetric:
+        i, j = np.maximum(i, j), np.minimum(i, j)
+    # about 10 % repeat an earlier index with another value
+    rep_ = rng.random(count) < 0.1
+    src = rng.integers(0, count, count)
+    i = np.where(rep_, i[src], i)
+    j = np.where(rep_, j[src], j)
+    lines = []
+    for a, b in zip(i, j):
+        if field == "pattern":
+            lines.append(f"{a + 1} {b + 1}")
+        elif field == "integer":
+            lines.append(f"{a + 1} {b + 1} {int(rng.integers(-9, 10))}")
+        else:
+            lines.append(f"{a + 1} {b + 1} {rng.uniform(-2, 2):.6g}")
+    return lines
+
+
+def io_fixtures():
+    import subprocess
+    import tempfile
+    rng = np.random.default_rng(60)
+    cases = [("general_real_dups", 60, 45, 300, "real", "general", "f32"),
+             ("symmetric_real", 50, 50, 200, "real", "symmetric", "f32"),
+             ("pattern_general", 40, 70, 150, "pattern", "general", "f32"),
+             ("integer_general", 30, 30, 90, "integer", "general", "i32")]
+    for name, m, n, cnt, field, sym, dt in cases:
+        lines = _mtx_lines(rng, m, n, cnt, field, sym == "symmetric")
+        path = os.path.join(OUT, f"mm_{name}.mtx")
+        with open(path, "w") as f:
+            f.write(f"%%MatrixMarket matrix coordinate {field} {sym}\n% written by make_golden.py\n%\n")
+            f.write(f"{m} {n} {len(lines)}\n")
+            f.write("\n".join(lines) + "\n")
+        with tempfile.TemporaryDirectory() as d:
+            out = os.path.join(d, "a.binary")
+            subprocess.run([O.REF_BIN, "mmread", path, dt, out], check=True)
+            c = gen.read_binary(out, np.float32 if dt == "f32" else np.int32)
+        np.savez_compressed(os.path.join(OUT, f"mm_{name}.npz"), dtype=np.array(dt), **csr_dict("c", c))
+        print(f"mm_{name}: nnz={c.nnz}")
+    for name, a, tiles in [("rmat9_ragged", gen.rmat(9, seed=61), (100, 70)),
+                           ("empty_rect", sparse_with_empty(300, 200, seed=62), (64, 50)),
+                           ("stencil6", gen.stencil27(6), (50, 128))]:
+        dt = "f32" if a.vals.dtype == np.float32 else "i32"
+        vt = np.float32 if dt == "f32" else np.int32
+        with tempfile.TemporaryDirectory() as d:
+            fa, ft = os.path.join(d, "a.binary"), os.path.join(d, "t.bin")
+            gen.write_binary(fa, a)
+            subprocess.run([O.REF_BIN, "tiles", fa, str(tiles[0]), str(tiles[1]), dt, ft], check=True)
+            raw = open(ft, "rb").read()
+        rps, cis, vs, nnzs = [], [], [], []
+        pos = 0
+        while pos < len(raw):
+            tm_, tn_, nz = np.frombuffer(raw, np.uint64, 3, pos).astype(np.int64)
+            pos += 24
+            vs.append(np.frombuffer(raw, vt, nz, pos)); pos += 4 * nz
+            cis.append(np.frombuffer(raw, np.int32, nz, pos)); pos += 4 * nz
+            rps.append(np.frombuffer(raw, np.int32, tm_ + 1, pos)); pos += 4 * (tm_ + 1)
+            nnzs.append(nz)
+        d = csr_dict("a", a)
+        d.update({"tiles": np.array(tiles, np.int64), "tile_nnz": np.array(nnzs, np.int64),
+                  "tile_rows": np.array([r.size - 1 for r in rps], np.int64),
+                  "row_ptr": np.concatenate(rps), "col_ind": np.concatenate(cis),
+                  "vals": np.concatenate(vs)})
+        np.savez_compressed(os.path.join(OUT, f"tiles_{name}.npz"), **d)
+        print(f"tiles_{name}: {len(nnzs)} tiles")
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["io"]:
+        io_fixtures()
+    else:
+        main()
+        io_fixtures()
