@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
 // ---- long rows ----------------------------------------------------------------
 //
 // A row with thousands of entries is one chain of multiply-adds per output
-// element (the reference's order), so a warp with 8 B-row loads in flight
+// element (the reference's order), so a warp with a few B-row loads in flight
 // spends milliseconds on it.  Such rows are found first (k_spmm_find_long),
 // skipped by k_spmm and run by k_spmm_long on the context's side stream at
 // the same time: one warp per (row, C tile column, panel), the same walk
