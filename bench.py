@@ -321,7 +321,7 @@ def bench_spgemm(args, wl, dist, device):
         return nnz, (trp, toff, ci, v)
 
     for _ in range(args.warmup):
-        nnz_c, _ = step()
+        nnz_c = step()[0]
     torch.cuda.synchronize()
     clocks = ClockSampler(device)
     clocks.start()
@@ -333,7 +333,7 @@ def bench_spgemm(args, wl, dist, device):
     for s in range(args.steps):
         flush.zero_()
         ev[s][0].record(stream)
-        nnz_c, _ = step(record=(ev[s][2], ev[s][3]))
+        nnz_c = step(record=(ev[s][2], ev[s][3]))[0]
         ev[s][1].record(stream)
     torch.cuda.synchronize()
     dist.barrier()
