@@ -23,7 +23,7 @@ CANDIDATES = {
     "blocks_per_sm": (3, 4),
     "long_seg": (32, 48, 64, 1 << 30),
 }
-DEFAULT = (2, 4, 48)
+DEFAULT = (1, 4, 32)
 
 
 def cache_path() -> str:

@@ -56,8 +56,8 @@ constexpr int kMaxCols = kMaxWords * 32;
 constexpr int kWarpsSym = 8;
 constexpr int kWarpsNum = 8;
 constexpr int kNoStage = 0xff;
-constexpr int kLongSegDefault = 48;
-constexpr int kQueueSlots = 256;          // work-queue heads in a plan (one per stage launch)       // B segments at least this long are walked in direct mode
+constexpr int kLongSegDefault = 32;       // B segments at least this long are walked in direct mode
+constexpr int kQueueSlots = 256;          // work-queue heads in a plan (one per stage launch)
 constexpr int64_t kVeryHeavyUb = 32768;  // rows above this many products get a whole block in the symbolic pass
 
 struct Geom {
@@ -1162,7 +1162,7 @@ struct bclx_spgemm_plan_s {
   int32_t* scount_own = nullptr;
   unsigned long long* queue = nullptr;  // work-queue heads, one per stage launch
   // numeric tuning (bclx_spgemm_plan_tune)
-  int grab = 2, blocks_per_sm = 4, long_seg = kLongSegDefault;
+  int grab = 1, blocks_per_sm = 4, long_seg = kLongSegDefault;
   // CUDA graph of the staged numeric pass (bclx_spgemm_numeric_staged)
   cudaGraphExec_t graph = nullptr;
   const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
