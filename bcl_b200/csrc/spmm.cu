@@ -3,13 +3,14 @@
 // tile loop of BCL::gemm(SPMatrix, DMatrix, DMatrix&) (spgemm.hpp:153-179) in
 // one launch.
 //
-// Layout: one warp per (C tile row, column panel).  Lane l owns VEC
-// consecutive columns per chunk (a 16-byte vector: 4 floats or 8 bfloat16),
-// so a warp covers 128 FP32 / 256 BF16 columns per chunk, CH chunks per
-// panel.  The warp reads 32 (column, value) pairs of the A row at once and
-// broadcasts them with shuffles; for each entry every lane issues its 16-byte
-// loads of the B row (coalesced: the warp reads whole 512-byte row segments),
-// UNROLL entries' loads in flight before their multiply-adds are applied.
+// Layout: one warp per (group of 1, 2 or 4 rows of one C tile, column panel
+// of 32 16-byte vectors: 128 FP32 / 256 BF16 columns); lane l owns one
+// vector.  The group's A entries are flattened over rows and stages and put
+// 32 at a time into a per-warp shared-memory table (B-row address, value,
+// row); every lane then issues its 16-byte loads of the B rows (the warp
+// reads whole 512-byte row segments), UNROLL entries' loads in flight before
+// their multiply-adds are applied.  Rows with thousands of entries run in
+// k_spmm_long beside it.
 //
 // Order: per output element the multiply-adds run in stored A-row order, and
 // over the C tile's stages k = (k_ + i + j) mod G in that order, starting
@@ -91,12 +92,44 @@ __device__ __forceinline__ void l2_prefetch_slice(const void* p, int bytes) {
   for (int o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(q + o));
 }
 
-// Per-warp entry tables (two 32-entry buffers of 16 bytes per warp).
-__shared__ uint4 spmm_tables[kSpmmWarps * 64];
+constexpr int kSpmmMaxRows = 4;  // rows of one C tile a warp walks together
+constexpr int kARing = 4;        // A-entry staging slots (chunks of 32 entries) per warp
+constexpr int kTabBufs = 3;      // entry-table buffers per warp: applied, next, being built
 
-// The stages of C-tile row (ti, tj, r), one lane per stage of the group
-// [g0, g0+32), in the reference's rotated order k = (k_ + ti + tj) mod gk:
-// the A-row segment of that stage and its B tile.
+// Per-warp shared memory of the walk:
+//  * entry tables: per chunk of 32 entries, (B-row address, A value, row) of
+//    each entry, read back with broadcast 16-byte loads;
+//  * A staging ring: the (column, value) pair of each entry, copied by
+//    cp.async kARing - 1 chunks ahead, with the entry's stage lane;
+//  * C staging: the C row slices the item updates (one 16-byte vector per
+//    lane and row), copied by cp.async while the A and B loads are in flight.
+__shared__ uint4 spmm_tables[kSpmmWarps * kTabBufs * 32];
+__shared__ uint2 spmm_aring[kSpmmWarps * kARing * 32];
+__shared__ uint8_t spmm_asrc[kSpmmWarps * kARing * 32];
+__shared__ uint4 spmm_cstage[kSpmmWarps * kSpmmMaxRows * 32];
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// One stage of one row of C tile (ti, tj): for stage slot kk of the
+// reference's rotated order k = (k_ + ti + tj) mod gk, the A-row segment of
+// row r in tile (ti, k) and the B tile (k, tj).  Empty when !valid.
 template <typename ST>
 struct StageLane {
   int32_t alen;
@@ -107,11 +140,10 @@ struct StageLane {
 
 template <typename ST>
 __device__ __forceinline__ StageLane<ST> stage_lane(const SpGridView& A, const DGridView& B, int64_t ti, int64_t tj,
-                                                    int64_t r, int64_t g0) {
+                                                    int64_t r, int64_t kk, bool valid) {
   StageLane<ST> s{0, nullptr, nullptr, nullptr};
-  const int64_t kk = g0 + lane_id();
   const int64_t gk = A.gn;
-  if (kk < gk) {
+  if (valid && kk < gk) {
     const int64_t k = (kk + ti + tj) % gk;
     const bclx_csr_t At = A.tile(ti, k);
     const int32_t as = __ldg(At.row_ptr + r);
@@ -130,85 +162,162 @@ __device__ __forceinline__ bool tiles_aligned(const DGridView& B, const DGridVie
   return __all_sync(kFull, ok);
 }
 
-// One warp per (C row, panel of 32 16-byte vectors).  The A entries of all
-// stages are taken 32 at a time (one lane each finds its B row), then
-// broadcast kSpmmUnroll at a time so that that many B-row loads (raw
-// 16-byte vectors) are in flight before their multiply-adds are applied in
-// entry order.  `vec`: every B and C row slice of this tile pair is 16-byte
-// aligned; otherwise element-wise access.
-template <typename ST, int UNROLL = kSpmmUnroll>
-__device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
-                                         int64_t tj, int64_t r, int c0, int W, bool vec) {
+// One warp per (R consecutive rows of C tile (ti, tj) from r0, panel of 32
+// 16-byte vectors from column c0).  The A entries of the rows' stages are
+// flattened (row by row, each row's stages in rotated order) and taken in
+// chunks of 32, one entry per lane, through a software pipeline:
+//   * chunk c + kARing + 1: each lane finds its entry's stage and copies the
+//     entry's (column, value) into the warp's staging ring by cp.async;
+//   * chunk c + 2: each lane turns its staged entry into a table entry
+//     (B-row address, value, row) and asks L2 for that B-row slice;
+//   * chunk c: the warp reads the table UNROLL entries at a time, so that
+//     many B-row loads (raw 16-byte vectors) are in flight before their
+//     multiply-adds are applied in entry order.
+// No load result is waited for before it is used, so the A loads of later
+// chunks never stall the current one.  A row's chain starts from its C
+// value, staged in shared memory by cp.async once the row is known to have
+// entries; rows without entries are not touched.  R > 1 needs R * gk <= 32
+// (one lane per (row, stage)); R == 1 takes the stages 32 at a time.
+// GROUP = false compiles the one-row walk alone (R == 1, no row changes to
+// test for inside the unrolled loop).  `skip` (or null): rows flagged there
+// are left to another kernel.  `vec`: every B and C row slice of this tile
+// pair is 16-byte aligned; otherwise element-wise access.
+template <typename ST, bool GROUP, int UNROLL = kSpmmUnroll>
+__device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
+                                          int64_t tj, int64_t r0, int R, int c0, int W, bool vec,
+                                          const uint8_t* __restrict__ skip) {
+  if (!GROUP) R = 1;
   using V = Vec<ST>;
   constexpr int VN = V::N;
   const int lane = lane_id();
-  ST* __restrict__ crow = reinterpret_cast<ST*>(C.tile(ti, tj)) + r * C.ld;
+  const int64_t nrows = min((int64_t)R, C.rows_of(ti) - r0);
+  ST* __restrict__ crow0 = reinterpret_cast<ST*>(C.tile(ti, tj)) + r0 * C.ld;
   const int col = c0 + lane * VN;
   const bool own = col < W;
-  float acc[VN];
-  if (vec) {
-    if (own) V::load_c(crow + col, acc);
-  } else {
-#pragma unroll
-    for (int x = 0; x < VN; x++) acc[x] = (col + x < W) ? V::to_f(crow[col + x]) : 0.f;
-  }
-  // Entry table of one 32-entry chunk per buffer: B row address (column 0
-  // of the tile) and A value, written lane-parallel one chunk ahead and read
-  // back with broadcast 16-byte shared loads.
-  uint4* tb = spmm_tables + (threadIdx.x >> 5) * 64;
+  const int bcol = own ? col : 0;  // lanes past the tile edge load column 0 (in bounds) and store nothing
+  const int wib = threadIdx.x >> 5;
+  uint4* tb = spmm_tables + wib * (kTabBufs * 32);
+  uint2* ar = spmm_aring + wib * (kARing * 32);
+  uint8_t* asrc = spmm_asrc + wib * (kARing * 32);
+  uint4* cs = spmm_cstage + wib * (kSpmmMaxRows * 32);
   // bytes of this warp's panel in one B row
   const int pbytes = min(32 * VN, W - c0) * (int)sizeof(ST);
-  for (int64_t g0 = 0; g0 < A.gn; g0 += 32) {
-    const StageLane<ST> sl = stage_lane<ST>(A, B, ti, tj, r, g0);
+  const int gk = (int)A.gn;
+  float acc[VN];
+  int cur = -1;  // row whose chain is in acc
+  bool staged = false;
+  auto flush = [&]() {
+    if (cur < 0 || !own) return;
+    ST* p = crow0 + cur * C.ld;
+    if (vec) {
+      V::store(p + col, acc);
+    } else {
+#pragma unroll
+      for (int x = 0; x < VN; x++)
+        if (col + x < W) p[col + x] = V::from_f(acc[x]);
+    }
+  };
+  auto enter = [&](int q) {
+    flush();
+    cur = q;
+    if (!own) return;
+    if (vec) {
+      cp_async_wait_all();
+      V::unpack_raw(cs[q * 32 + lane], acc);
+    } else {
+      const ST* p = crow0 + q * C.ld;
+#pragma unroll
+      for (int x = 0; x < VN; x++) acc[x] = (col + x < W) ? V::to_f(p[col + x]) : 0.f;
+    }
+  };
+  for (int64_t g0 = 0; g0 < gk; g0 += 32) {
+    const int ql = GROUP ? lane / gk : 0;
+    const int64_t kk = GROUP ? lane - ql * gk : g0 + lane;
+    bool valid = ql < nrows;
+    if (valid && skip) valid = skip[ti * C.tm + r0 + ql] == 0;
+    const StageLane<ST> sl = stage_lane<ST>(A, B, ti, tj, r0 + ql, kk, valid);
     const int32_t aincl = warp_inclusive_scan(sl.alen);
     const int32_t atot = __shfl_sync(kFull, aincl, 31);
+    if (atot == 0) continue;
     const int32_t aexcl = aincl - sl.alen;
-    // entry e0 + lane of the flattened stages: its A value and B row
-    auto chunk = [&](int32_t e0, float& v, const ST*& brow) {
-      const int32_t e = e0 + lane;
-      int src = 0;
+    // stage the C slices of the rows that have entries
+    if (!GROUP) {
+      if (vec && !staged) {
+        if (own) cp_async16(cs + lane, crow0 + col);
+        staged = true;
+      }
+    } else {
+      for (int q = 0; q < R; q++) {
+        const int32_t hi = __shfl_sync(kFull, aincl, q * gk + gk - 1);
+        const int32_t lo = __shfl_sync(kFull, aexcl, q * gk);
+        if (vec && own && hi > lo) cp_async16(cs + q * 32 + lane, crow0 + q * C.ld + col);
+      }
+    }
+    const int32_t nch = (atot + 31) >> 5;
+    // chunk x: each lane's entry x*32 + lane into ring slot x % kARing (one
+    // commit group per chunk, empty past the end)
+    auto issue_a = [&](int32_t x) {
+      if (x < nch) {
+        const int32_t e = x * 32 + lane;
+        int src = 0;
 #pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const int32_t t = __shfl_sync(kFull, aincl, src + step - 1);
-        if (t <= e) src += step;
+        for (int step = 16; step >= 1; step >>= 1) {
+          const int32_t t = __shfl_sync(kFull, aincl, src + step - 1);
+          if (t <= e) src += step;
+        }
+        src = min(src, 31);
+        const int32_t off = e - __shfl_sync(kFull, aexcl, src);
+        const int32_t* sacol = reinterpret_cast<const int32_t*>(
+            __shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.acol), src));
+        const float* saval = reinterpret_cast<const float*>(
+            __shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.aval), src));
+        const int slot = (x % kARing) * 32 + lane;
+        asrc[slot] = (uint8_t)src;
+        if (e < atot) {
+          cp_async4(&ar[slot].x, sacol + off);
+          cp_async4(&ar[slot].y, saval + off);
+        }
       }
-      src = min(src, 31);
-      const int32_t off = e - __shfl_sync(kFull, aexcl, src);
-      const int32_t* sacol = reinterpret_cast<const int32_t*>(
-          __shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.acol), src));
-      const float* saval = reinterpret_cast<const float*>(
-          __shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.aval), src));
+      cp_async_commit();
+    };
+    // chunk x (staged): table entries and L2 requests for the B-row slices.
+    // Entries past the end point at the last entry's B row with value 0 (an
+    // in-bounds load whose product is never applied).
+    auto build = [&](int32_t x) {
+      if (x >= nch) return;
+      const int slot = (x % kARing) * 32 + lane;
+      const int src = asrc[slot];
       const ST* sbt = reinterpret_cast<const ST*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.bt), src));
-      v = 0.f;
-      brow = sbt;
+      const int32_t e = x * 32 + lane;
+      float v = 0.f;
+      const ST* brow = sbt;
       if (e < atot) {
-        v = __ldg(saval + off);
-        brow = sbt + (int64_t)__ldg(sacol + off) * B.ld;
+        const uint2 a = ar[slot];
+        v = __uint_as_float(a.y);
+        brow = sbt + (int64_t)(int32_t)a.x * B.ld;
       }
-    };
-    auto put = [&](int buf, float v, const ST* brow) {
+      const ST* last = reinterpret_cast<const ST*>(
+          __shfl_sync(kFull, reinterpret_cast<unsigned long long>(brow), (atot - 1) & 31));
+      if (e >= atot) brow = last;
       const uint64_t pa = reinterpret_cast<uint64_t>(brow);
-      tb[buf * 32 + lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), __float_as_uint(v), 0u);
+      tb[(x % kTabBufs) * 32 + lane] =
+          make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), __float_as_uint(v), GROUP ? (uint32_t)(src / gk) : 0u);
+      l2_prefetch_slice(vec && e < atot ? brow + c0 : nullptr, pbytes);
     };
-    // Chunk c is applied from the table while the rows of chunk c+2 are
-    // asked into L2 (each lane its own entry's panel slice) and the A loads
-    // of chunk c+3 are in flight.
-    float v0, v1, v2, v3;
-    const ST *b0, *b1, *b2, *b3;
-    chunk(0, v0, b0);
-    chunk(32, v1, b1);
-    chunk(64, v2, b2);
-    put(0, v0, b0);
-    l2_prefetch_slice(vec && lane < atot ? b0 + c0 : nullptr, pbytes);
-    l2_prefetch_slice(vec && 32 + lane < atot ? b1 + c0 : nullptr, pbytes);
+    // pipeline fill: chunks 0 .. kARing-1 staged, 0 and 1 built, kARing staged
+    for (int x = 0; x < kARing; x++) issue_a(x);
+    cp_async_wait_group<kARing - 2>();
+    build(0);
+    build(1);
+    issue_a(kARing);
     __syncwarp();
-    int buf = 0;
-    for (int32_t e0 = 0; e0 < atot; e0 += 32) {
-      const bool more = e0 + 32 < atot;
-      if (e0 + 96 < atot) chunk(e0 + 96, v3, b3);  // A loads three chunks ahead
-      l2_prefetch_slice(vec && e0 + 64 + lane < atot ? b2 + c0 : nullptr, pbytes);
-      const int ne = min(32, atot - e0);
-      const uint4* t = tb + buf * 32;
+    if (!GROUP && cur < 0) enter(0);
+    for (int32_t c = 0; c < nch; c++) {
+      issue_a(c + kARing + 1);
+      cp_async_wait_group<kARing - 1>();
+      build(c + 2);
+      const int ne = min(32, atot - c * 32);
+      const uint4* t = tb + (c % kTabBufs) * 32;
       if (vec) {
         for (int u0 = 0; u0 < ne; u0 += UNROLL) {
           uint4 ent[UNROLL];
@@ -218,22 +327,29 @@ __device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B
 #pragma unroll
           for (int u = 0; u < UNROLL; u++) {
             const ST* rp = reinterpret_cast<const ST*>((uint64_t)ent[u].x | ((uint64_t)ent[u].y << 32));
-            if (u0 + u < ne && own) raw[u] = __ldg(reinterpret_cast<const uint4*>(rp + col));
+            raw[u] = __ldg(reinterpret_cast<const uint4*>(rp + bcol));
           }
+          auto apply = [&](int u) {
+            if (GROUP && (int)ent[u].w != cur) enter((int)ent[u].w);
+            float b[VN];
+            V::unpack_raw(raw[u], b);
+            const float vs = __uint_as_float(ent[u].z);
 #pragma unroll
-          for (int u = 0; u < UNROLL; u++) {
-            if (u0 + u < ne && own) {
-              float b[VN];
-              V::unpack_raw(raw[u], b);
-              const float vs = __uint_as_float(ent[u].z);
+            for (int x = 0; x < VN; x++) acc[x] = __fmaf_rn(vs, b[x], acc[x]);
+          };
+          if (u0 + UNROLL <= ne) {  // whole group: no test between the loads and their use
 #pragma unroll
-              for (int x = 0; x < VN; x++) acc[x] = __fmaf_rn(vs, b[x], acc[x]);
-            }
+            for (int u = 0; u < UNROLL; u++) apply(u);
+          } else {
+#pragma unroll
+            for (int u = 0; u < UNROLL; u++)
+              if (u0 + u < ne) apply(u);
           }
         }
       } else {
         for (int u = 0; u < ne; u++) {
           const uint4 en = t[u];
+          if (GROUP && (int)en.w != cur) enter((int)en.w);
           const ST* rp = reinterpret_cast<const ST*>((uint64_t)en.x | ((uint64_t)en.y << 32));
           const float vs = __uint_as_float(en.z);
 #pragma unroll
@@ -241,46 +357,42 @@ __device__ __forceinline__ void spmm_row(const SpGridView& A, const DGridView& B
             if (col + x < W) acc[x] = __fmaf_rn(vs, V::to_f(rp[col + x]), acc[x]);
         }
       }
-      if (more) {
-        buf ^= 1;
-        put(buf, v1, b1);
-      }
       __syncwarp();
-      v1 = v2;
-      b1 = b2;
-      v2 = v3;
-      b2 = b3;
     }
   }
-  if (vec) {
-    if (own) V::store(crow + col, acc);
-  } else {
-#pragma unroll
-    for (int x = 0; x < VN; x++)
-      if (col + x < W) crow[col + x] = V::from_f(acc[x]);
-  }
+  flush();
 }
 
-template <typename ST>
+// Warp items come from a device counter (one grab per item, the next grab in
+// flight while the current item runs), so warps that draw short rows take
+// more of them: the cost of a (row group, panel) item varies by orders of
+// magnitude on power-law matrices.
+template <typename ST, bool GROUP>
 __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
-    k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int row_align_ok,
-           const uint8_t* __restrict__ long_flag) {
+    k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int R, int64_t ngroups,
+           int row_align_ok, const uint8_t* __restrict__ long_flag, unsigned long long* __restrict__ next_item) {
   constexpr int PW = 32 * Vec<ST>::N;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t item = warp; item < n_items; item += nwarps) {
-    const int64_t ri = item / npanels;
-    const int panel = (int)(item - ri * npanels);
-    const int64_t t = ri / C.tm;
-    const int64_t r = ri - t * C.tm;
+  const int lane = lane_id();
+  unsigned long long it = 0;
+  if (lane == 0) it = atomicAdd(next_item, 1ULL);
+  it = __shfl_sync(kFull, it, 0);
+  while (it < (unsigned long long)n_items) {
+    unsigned long long nx = 0;
+    if (lane == 0) nx = atomicAdd(next_item, 1ULL);
+    const int64_t item = (int64_t)it;
+    const int64_t rg = item / npanels;
+    const int panel = (int)(item - rg * npanels);
+    const int64_t t = rg / ngroups;
+    const int64_t r0 = (rg - t * ngroups) * R;
     const int64_t ti = t / C.gn, tj = t - ti * C.gn;
-    if (r >= C.rows_of(ti)) continue;
     const int W = (int)C.cols_of(tj);
     const int c0 = panel * PW;
-    if (c0 >= W) continue;
-    const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
-    if (long_flag && vec && long_flag[ti * C.tm + r]) continue;  // k_spmm_long takes it
-    spmm_row<ST>(A, B, C, ti, tj, r, c0, W, vec);
+    if (r0 < C.rows_of(ti) && c0 < W) {
+      const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
+      // rows flagged long are k_spmm_long's (it takes the aligned ones)
+      spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr);
+    }
+    it = __shfl_sync(kFull, nx, 0);
   }
 }
 
@@ -292,17 +404,20 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
 // skipped by k_spmm and run by k_spmm_long on the context's side stream at
 // the same time: one warp per (row, C tile column, panel), the same walk
 // with kLongUnroll B-row loads in flight per lane (warps with the registers
-// for it: few of them, each on one long chain).
+// for it: few of them, each on one long chain).  Rows of kSpmmVeryLongRow
+// entries or more are listed first, so that the longest chains start first.
 
-constexpr int kLongUnroll = 32;  // B-row loads in flight per lane on long rows (half for BF16: registers)
+constexpr int kLongUnroll = 32;  // B-row loads in flight per lane on long rows
 constexpr int kLongWarps = 4;
-constexpr int kSpmmLongRow = 1024;         // entries over all stages
+constexpr int kSpmmLongRow = 1024;           // entries over all stages
+constexpr int kSpmmVeryLongRow = 8192;       // listed at the front
 constexpr int64_t kSpmmLongMinRows = 65536;  // smaller products do not use the long-row path
 
 // Thread per A row (ti, r): entries over all stages; rows with at least
-// long_row are flagged and listed.
-__global__ void k_spmm_find_long(SpGridView A, int long_row, uint8_t* __restrict__ flag, int64_t* __restrict__ list,
-                                 int32_t* __restrict__ count) {
+// long_row are flagged and listed: very long rows from list[0] up
+// (count[0]), the others from list[rows-1] down (count[1]).
+__global__ void k_spmm_find_long(SpGridView A, int long_row, int very_long_row, uint8_t* __restrict__ flag,
+                                 int64_t* __restrict__ list, int32_t* __restrict__ count) {
   const int64_t rows = A.gm * A.tm;
   for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < rows; x += (int64_t)gridDim.x * blockDim.x) {
     const int64_t ti = x / A.tm, r = x - ti * A.tm;
@@ -314,32 +429,48 @@ __global__ void k_spmm_find_long(SpGridView A, int long_row, uint8_t* __restrict
       }
     const bool lng = tot >= long_row;
     flag[x] = lng ? 1 : 0;
-    if (lng) list[atomicAdd(count, 1)] = x;
+    if (lng) {
+      if (tot >= very_long_row)
+        list[atomicAdd(count, 1)] = x;
+      else
+        list[rows - 1 - atomicAdd(count + 1, 1)] = x;
+    }
   }
 }
 
+// Items (listed row, C tile column, panel), a row's items consecutive, taken
+// from a device counter in list order.
 template <typename ST>
 __global__ void __launch_bounds__(kLongWarps * 32)
     k_spmm_long(SpGridView A, DGridView B, DGridView C, const int64_t* __restrict__ list,
-                const int32_t* __restrict__ count, int npanels, int row_align_ok) {
+                const int32_t* __restrict__ count, int npanels, int row_align_ok,
+                unsigned long long* __restrict__ next_item) {
   constexpr int PW = 32 * Vec<ST>::N;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t nl = *count;
-  const int64_t n = nl * C.gn * npanels;
-  for (int64_t w = warp; w < n; w += nwarps) {
-    // consecutive warps take different rows; a row's panels are spread out
-    const int64_t li = w % nl;
-    const int64_t pt = w / nl;
+  const int lane = lane_id();
+  const int64_t rows = A.gm * A.tm;
+  const int64_t nv = count[0];
+  const int64_t nl = nv + count[1];
+  const int64_t per_row = C.gn * npanels;
+  const unsigned long long n = (unsigned long long)(nl * per_row);
+  unsigned long long it = 0;
+  if (lane == 0) it = atomicAdd(next_item, 1ULL);
+  it = __shfl_sync(kFull, it, 0);
+  while (it < n) {
+    unsigned long long nx = 0;
+    if (lane == 0) nx = atomicAdd(next_item, 1ULL);
+    const int64_t li = (int64_t)it / per_row;
+    const int64_t pt = (int64_t)it - li * per_row;
     const int panel = (int)(pt % npanels);
     const int64_t tj = pt / npanels;
-    const int64_t x = list[li];
+    const int64_t x = li < nv ? list[li] : list[rows - 1 - (li - nv)];
     const int64_t ti = x / A.tm, r = x - ti * A.tm;
     const int W = (int)C.cols_of(tj);
-    if (panel * PW >= W) continue;
-    const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
-    if (!vec) continue;  // k_spmm did this one element-wise
-    spmm_row<ST, sizeof(ST) == 4 ? kLongUnroll : kLongUnroll / 2>(A, B, C, ti, tj, r, panel * PW, W, true);
+    if (panel * PW < W) {
+      const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
+      if (vec)  // otherwise k_spmm did this one element-wise
+        spmm_rows<ST, false, kLongUnroll>(A, B, C, ti, tj, r, 1, panel * PW, W, true, nullptr);
+    }
+    it = __shfl_sync(kFull, nx, 0);
   }
 }
 
@@ -348,48 +479,73 @@ static int64_t spmm_long_min_rows() {
   return e && *e ? std::strtoll(e, nullptr, 10) : kSpmmLongMinRows;
 }
 
+// Rows per k_spmm warp item: grouping short rows shares one prologue (tile
+// descriptors, row pointers, A loads) among them, but only while the items
+// still fill the GPU several times over.  BCLX_SPMM_ROWS overrides (1, 2, 4).
+static int spmm_rows_per_item(const Context* ctx, const DGridView& C, int64_t gk, int npanels) {
+  auto fits = [&](int r) { return r <= kSpmmMaxRows && r * gk <= 32; };
+  const char* e = std::getenv("BCLX_SPMM_ROWS");
+  if (e && *e) {
+    const int r = std::atoi(e);
+    if ((r == 1 || r == 2 || r == 4) && fits(r)) return r;
+  }
+  const int64_t resident = (int64_t)ctx->num_sms * 4 * kSpmmWarps;
+  int r = 1;
+  while (fits(2 * r) && C.gm * C.gn * ceil_div(C.tm, (int64_t)(2 * r)) * npanels >= 4 * resident) r *= 2;
+  return r;
+}
+
 template <typename ST>
 static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, const DGridView& C, int align_ok) {
   constexpr int VN = Vec<ST>::N;
   const int npanels = (int)ceil_div(C.tn, 32 * VN);
-  const int64_t n_items = C.gm * C.gn * C.tm * npanels;
+  const int R = spmm_rows_per_item(ctx, C, A.gn, npanels);
+  const int64_t ngroups = ceil_div(C.tm, (int64_t)R);
+  const int64_t n_items = C.gm * C.gn * ngroups * npanels;
   if (n_items == 0) return BCLX_OK;
   const int64_t want = ceil_div(n_items, kSpmmWarps);
-  const int64_t cap = (int64_t)ctx->num_sms * 8;
+  const int64_t cap = (int64_t)ctx->num_sms * 4;  // resident blocks: warps take items from a counter
   const int64_t arows = A.gm * A.tm;
   const bool long_path = align_ok && A.gn <= 32 && arows >= spmm_long_min_rows();
+  // counters: [0] k_spmm items, [1] k_spmm_long items, [2] listed very long / other long rows (2 x int32)
+  unsigned long long* ctr = nullptr;
+  BCLX_TRY(scratch_alloc_n(ctx, &ctr, 3));
+  BCLX_CK(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), ctx->stream));
+  int32_t* cnt = reinterpret_cast<int32_t*>(ctr + 2);
   uint8_t* flag = nullptr;
   int64_t* list = nullptr;
-  int32_t* cnt = nullptr;
   if (long_path) {
     // find the long rows, then run them on the side stream beside k_spmm
     BCLX_TRY(ensure_side_stream(ctx));
     BCLX_TRY(scratch_alloc_n(ctx, &flag, (size_t)arows));
     BCLX_TRY(scratch_alloc_n(ctx, &list, (size_t)arows));
-    BCLX_TRY(scratch_alloc_n(ctx, &cnt, 1));
-    BCLX_CK(cudaMemsetAsync(cnt, 0, sizeof(int32_t), ctx->stream));
     k_spmm_find_long<<<(unsigned)std::min<int64_t>(ceil_div(arows, 256), (int64_t)ctx->num_sms * 16), 256, 0,
-                       ctx->stream>>>(A, kSpmmLongRow, flag, list, cnt);
+                       ctx->stream>>>(A, kSpmmLongRow, kSpmmVeryLongRow, flag, list, cnt);
     note_launch();
     BCLX_CK_LAUNCH();
     BCLX_CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
     BCLX_CK(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
     k_spmm_long<ST><<<(unsigned)ctx->num_sms, kLongWarps * 32, 0, ctx->side>>>(A, B, C, list, cnt, npanels,
-                                                                                align_ok);
+                                                                                align_ok, ctr + 1);
     note_launch();
     BCLX_CK_LAUNCH();
     BCLX_CK(cudaEventRecord(ctx->join_ev, ctx->side));
   }
-  k_spmm<ST><<<(unsigned)(want < cap ? want : cap), kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels,
-                                                                                        align_ok, flag);
+  const unsigned grid = (unsigned)(want < cap ? want : cap);
+  if (R > 1)
+    k_spmm<ST, true><<<grid, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, R, ngroups, align_ok, flag,
+                                                                 ctr);
+  else
+    k_spmm<ST, false><<<grid, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, 1, ngroups, align_ok, flag,
+                                                                  ctr);
   note_launch();
   BCLX_CK_LAUNCH();
   if (long_path) {
     BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
     scratch_free(ctx, flag);
     scratch_free(ctx, list);
-    scratch_free(ctx, cnt);
   }
+  scratch_free(ctx, ctr);
   return BCLX_OK;
 }
 

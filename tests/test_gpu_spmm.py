@@ -131,6 +131,33 @@ def test_spmm_ragged_last_tile_unaligned_width(monkeypatch):
     assert np.array_equal(bits(got), bits(want))
 
 
+@pytest.mark.parametrize("rows", ["2", "4"])
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+@pytest.mark.parametrize("tiles,n,long_rows", [((4096, 4096, 256), 256, True), ((3001, 5000, 200), 400, False),
+                                               ((1000, 1024, 128), 128, True), ((999, 1500, 24), 38, False)])
+def test_spmm_grouped_rows(monkeypatch, rows, dtype, tiles, n, long_rows):
+    """Several rows of one C tile walked by one warp (their entries
+    flattened, each row's chain started from its own C value): the same bits
+    as one row per warp, with empty rows, tile row counts that are not a
+    multiple of the group, long rows left to the long-row kernel, and an
+    element-wise (unaligned width) tile column."""
+    monkeypatch.setenv("BCLX_SPMM_ROWS", rows)
+    if long_rows:
+        monkeypatch.setenv("BCLX_SPMM_LONG_MIN_ROWS", "0")
+    a = heavy_rows_matrix(n=8192, light=3, heavy=(5000, 1024, 700))
+    b = gen.dense(a.n, n, seed=17, dist="normal")
+    c0 = gen.dense(a.m, n, seed=18)
+    if dtype == "f32":
+        got = run(a, b, tiles, c0=c0)
+        want = O.spmm_tiled(a, b, c0, *tiles)
+        assert np.array_equal(bits(got), bits(want))
+    else:
+        b16, c16 = O.to_bf16(b), O.to_bf16(c0)
+        got = run(a, b16, tiles, dtype="bf16", c0=c16)
+        want = O.spmm_tiled_bf16(a, b16, c16, *tiles)
+        assert np.array_equal(got, want)
+
+
 def test_spmm_tile_single_call_ld():
     """bclx_spmm_tile with leading dimensions larger than n (sub-blocks)."""
     import ctypes
