@@ -118,6 +118,20 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
+// The same copies without a compiler memory barrier, for the pipelined loops:
+// there every earlier access to the target shared memory is ordered before the
+// copy by a __syncwarp, and every later one after it by a wait (which is a
+// barrier), so the loads around the copies may be scheduled freely.
+__device__ __forceinline__ void cp_async16_nb(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+
+__device__ __forceinline__ void cp_async4_nb(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
 template <int N>
@@ -274,8 +288,8 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
         const int slot = (x % kARing) * 32 + lane;
         asrc[slot] = (uint8_t)src;
         if (e < atot) {
-          cp_async4(&ar[slot].x, sacol + off);
-          cp_async4(&ar[slot].y, saval + off);
+          cp_async4_nb(&ar[slot].x, sacol + off);
+          cp_async4_nb(&ar[slot].y, saval + off);
         }
       }
       cp_async_commit();
@@ -399,19 +413,29 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
 // ---- long rows ----------------------------------------------------------------
 //
 // A row with thousands of entries is one chain of multiply-adds per output
-// element (the reference's order), so a warp with a few B-row loads in flight
-// spends milliseconds on it.  Such rows are found first (k_spmm_find_long),
-// skipped by k_spmm and run by k_spmm_long on the context's side stream at
-// the same time: one warp per (row, C tile column, panel), the same walk
-// with kLongUnroll B-row loads in flight per lane (warps with the registers
-// for it: few of them, each on one long chain).  Rows of kSpmmVeryLongRow
-// entries or more are listed first, so that the longest chains start first.
+// element (the reference's order): it cannot be split, only fed faster.  Such
+// rows are found first (k_spmm_find_long), skipped by k_spmm and run by
+// k_spmm_long on the context's side stream at the same time, one warp per
+// (row, C tile column, panel), with the B-row slices themselves copied into
+// shared memory by cp.async two chunks (64 entries) ahead: the loads in
+// flight cost no registers, and a chunk's multiply-adds read shared memory.
+// Rows of kSpmmVeryLongRow entries or more are listed first, so that the
+// longest chains start first.
 
-constexpr int kLongUnroll = 32;  // B-row loads in flight per lane on long rows
 constexpr int kLongWarps = 4;
+constexpr int kLongBSlots = 3;  // chunks of B slices per warp: applied, in flight, being issued
+constexpr int kLongTSlots = 3;  // chunks of table entries per warp (with the B slices)
+constexpr int kLongASlots = 6;  // chunks of staged A entries per warp
 constexpr int kSpmmLongRow = 1024;           // entries over all stages
 constexpr int kSpmmVeryLongRow = 8192;       // listed at the front
 constexpr int64_t kSpmmLongMinRows = 65536;  // smaller products do not use the long-row path
+
+struct LongSmem {
+  uint4 b[kLongBSlots][32][32];  // [chunk slot][entry][lane]: each lane's 16 bytes of the entry's B row
+  uint4 tab[kLongTSlots][32];    // [chunk slot][entry]: B-row address, A value
+  uint2 a[kLongASlots][32];      // [chunk slot][entry]: staged A (column, value)
+  uint8_t src[kLongASlots][32];  // the entry's stage lane
+};
 
 // Thread per A row (ti, r): entries over all stages; rows with at least
 // long_row are flagged and listed: very long rows from list[0] up
@@ -438,6 +462,140 @@ __global__ void k_spmm_find_long(SpGridView A, int long_row, int very_long_row, 
   }
 }
 
+// One long row r of C tile (ti, tj), panel from column c0 (16-byte aligned
+// access: the caller checked).  Pipeline at chunk c (32 entries, one per
+// lane when staged or built):
+//   * A of chunk c + 6 staged (cp.async, 8 bytes per lane);
+//   * chunk c + 2 built: each lane's entry -> table (B-row address, value),
+//     then every lane copies its 16 bytes of each of the chunk's 32 B rows
+//     into the chunk's B slot (cp.async);
+//   * chunk c applied: the multiply-adds in entry order from shared memory.
+// One commit group per chunk step holds A(c+6) and B(c+2); B(c) is in the
+// group two steps back.  The stages are at most 32 (one lane each).
+template <typename ST>
+__device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, const DGridView& B,
+                                              const DGridView& C, int64_t ti, int64_t tj, int64_t r, int c0, int W) {
+  using V = Vec<ST>;
+  constexpr int VN = V::N;
+  const int lane = lane_id();
+  ST* __restrict__ crow = reinterpret_cast<ST*>(C.tile(ti, tj)) + r * C.ld;
+  const int col = c0 + lane * VN;
+  const bool own = col < W;
+  float acc[VN];
+  if (own) V::load_c(crow + col, acc);
+  const StageLane<ST> sl = stage_lane<ST>(A, B, ti, tj, r, lane, true);
+  const int32_t aincl = warp_inclusive_scan(sl.alen);
+  const int32_t atot = __shfl_sync(kFull, aincl, 31);
+  const int32_t aexcl = aincl - sl.alen;
+  const int32_t nch = (atot + 31) >> 5;
+  auto issue_a = [&](int32_t x) {
+    if (x >= nch) return;
+    const int32_t e = x * 32 + lane;
+    int src = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      const int32_t t = __shfl_sync(kFull, aincl, src + step - 1);
+      if (t <= e) src += step;
+    }
+    src = min(src, 31);
+    const int32_t off = e - __shfl_sync(kFull, aexcl, src);
+    const int32_t* sacol = reinterpret_cast<const int32_t*>(
+        __shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.acol), src));
+    const float* saval = reinterpret_cast<const float*>(
+        __shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.aval), src));
+    const int slot = x % kLongASlots;
+    S.src[slot][lane] = (uint8_t)src;
+    if (e < atot) {
+      cp_async4_nb(&S.a[slot][lane].x, sacol + off);
+      cp_async4_nb(&S.a[slot][lane].y, saval + off);
+    }
+  };
+  auto build = [&](int32_t x) {  // A(x) has landed
+    if (x >= nch) return;
+    const int slot = x % kLongASlots;
+    const int src = S.src[slot][lane];
+    const ST* sbt = reinterpret_cast<const ST*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.bt), src));
+    const int32_t e = x * 32 + lane;
+    if (e < atot) {
+      const uint2 a = S.a[slot][lane];
+      const uint64_t pa = reinterpret_cast<uint64_t>(sbt + (int64_t)(int32_t)a.x * B.ld);
+      S.tab[x % kLongTSlots][lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), a.y, 0u);
+    }
+  };
+  auto issue_b = [&](int32_t x) {  // table of chunk x built, then a __syncwarp
+    if (x >= nch || !own) return;
+    const int ne = min(32, atot - x * 32);
+    const int bslot = x % kLongBSlots, tslot = x % kLongTSlots;
+    auto copy = [&](int u, const uint4& t) {
+      const ST* rp = reinterpret_cast<const ST*>((uint64_t)t.x | ((uint64_t)t.y << 32));
+      cp_async16_nb(&S.b[bslot][u][lane], rp + col);
+    };
+    if (ne == 32) {
+#pragma unroll
+      for (int u0 = 0; u0 < 32; u0 += 8) {
+        uint4 t[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) t[k] = S.tab[tslot][u0 + k];
+#pragma unroll
+        for (int k = 0; k < 8; k++) copy(u0 + k, t[k]);
+      }
+    } else {
+      for (int u = 0; u < ne; u++) copy(u, S.tab[tslot][u]);
+    }
+  };
+  // fill: A(0..5) staged, chunks 0 and 1 built and their B slices asked for
+  issue_a(0);
+  issue_a(1);
+  cp_async_commit();
+  issue_a(2);
+  issue_a(3);
+  cp_async_commit();
+  cp_async_wait_group<1>();
+  build(0);
+  build(1);
+  __syncwarp();
+  issue_b(0);
+  issue_a(4);
+  cp_async_commit();
+  issue_b(1);
+  issue_a(5);
+  cp_async_commit();
+  cp_async_wait_group<2>();
+  for (int32_t c = 0; c < nch; c++) {
+    issue_a(c + 6);
+    build(c + 2);
+    __syncwarp();
+    issue_b(c + 2);
+    cp_async_commit();
+    cp_async_wait_group<2>();  // B(c) and A(c + 4) have landed
+    const int ne = min(32, atot - c * 32);
+    const int bslot = c % kLongBSlots, tslot = c % kLongTSlots;
+    if (own) {
+      if (ne == 32) {
+#pragma unroll 8
+        for (int u = 0; u < 32; u++) {
+          float b[VN];
+          V::unpack_raw(S.b[bslot][u][lane], b);
+          const float vs = __uint_as_float(S.tab[tslot][u].z);
+#pragma unroll
+          for (int x = 0; x < VN; x++) acc[x] = __fmaf_rn(vs, b[x], acc[x]);
+        }
+      } else {
+        for (int u = 0; u < ne; u++) {
+          float b[VN];
+          V::unpack_raw(S.b[bslot][u][lane], b);
+          const float vs = __uint_as_float(S.tab[tslot][u].z);
+#pragma unroll
+          for (int x = 0; x < VN; x++) acc[x] = __fmaf_rn(vs, b[x], acc[x]);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  cp_async_wait_all();
+  if (own) V::store(crow + col, acc);
+}
+
 // Items (listed row, C tile column, panel), a row's items consecutive, taken
 // from a device counter in list order.
 template <typename ST>
@@ -445,6 +603,8 @@ __global__ void __launch_bounds__(kLongWarps * 32)
     k_spmm_long(SpGridView A, DGridView B, DGridView C, const int64_t* __restrict__ list,
                 const int32_t* __restrict__ count, int npanels, int row_align_ok,
                 unsigned long long* __restrict__ next_item) {
+  extern __shared__ __align__(16) unsigned char long_smem[];
+  LongSmem& S = reinterpret_cast<LongSmem*>(long_smem)[threadIdx.x >> 5];
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
   const int64_t rows = A.gm * A.tm;
@@ -467,11 +627,18 @@ __global__ void __launch_bounds__(kLongWarps * 32)
     const int W = (int)C.cols_of(tj);
     if (panel * PW < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
-      if (vec)  // otherwise k_spmm did this one element-wise
-        spmm_rows<ST, false, kLongUnroll>(A, B, C, ti, tj, r, 1, panel * PW, W, true, nullptr);
+      if (vec) spmm_long_row<ST>(S, A, B, C, ti, tj, r, panel * PW, W);  // otherwise k_spmm did it element-wise
     }
     it = __shfl_sync(kFull, nx, 0);
   }
+}
+
+// Blocks of k_spmm_long (one per SM: its shared memory fills the SM): half
+// the SMs by default, the rest run k_spmm.  BCLX_SPMM_LONG_BLOCKS overrides.
+static int spmm_long_blocks(const Context* ctx) {
+  const char* e = std::getenv("BCLX_SPMM_LONG_BLOCKS");
+  const int b = e && *e ? std::atoi(e) : ctx->num_sms / 2;
+  return std::max(1, std::min(b, ctx->num_sms));
 }
 
 static int64_t spmm_long_min_rows() {
@@ -480,8 +647,8 @@ static int64_t spmm_long_min_rows() {
 }
 
 // Rows per k_spmm warp item: grouping short rows shares one prologue (tile
-// descriptors, row pointers, A loads) among them, but only while the items
-// still fill the GPU several times over.  BCLX_SPMM_ROWS overrides (1, 2, 4).
+// descriptors, row pointers, A loads) among them, while the items still
+// cover every resident warp.  BCLX_SPMM_ROWS overrides (1, 2, 4).
 static int spmm_rows_per_item(const Context* ctx, const DGridView& C, int64_t gk, int npanels) {
   auto fits = [&](int r) { return r <= kSpmmMaxRows && r * gk <= 32; };
   const char* e = std::getenv("BCLX_SPMM_ROWS");
@@ -491,7 +658,7 @@ static int spmm_rows_per_item(const Context* ctx, const DGridView& C, int64_t gk
   }
   const int64_t resident = (int64_t)ctx->num_sms * 4 * kSpmmWarps;
   int r = 1;
-  while (fits(2 * r) && C.gm * C.gn * ceil_div(C.tm, (int64_t)(2 * r)) * npanels >= 4 * resident) r *= 2;
+  while (fits(2 * r) && C.gm * C.gn * ceil_div(C.tm, (int64_t)(2 * r)) * npanels >= resident) r *= 2;
   return r;
 }
 
@@ -515,21 +682,28 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   uint8_t* flag = nullptr;
   int64_t* list = nullptr;
   if (long_path) {
-    // find the long rows, then run them on the side stream beside k_spmm
+    // On the side stream: find the long rows, then run them; k_spmm waits
+    // only for the list (an event after k_spmm_find_long), so the long-row
+    // blocks, next in their stream, are dispatched before k_spmm's blocks
+    // fill the SMs.
     BCLX_TRY(ensure_side_stream(ctx));
     BCLX_TRY(scratch_alloc_n(ctx, &flag, (size_t)arows));
     BCLX_TRY(scratch_alloc_n(ctx, &list, (size_t)arows));
-    k_spmm_find_long<<<(unsigned)std::min<int64_t>(ceil_div(arows, 256), (int64_t)ctx->num_sms * 16), 256, 0,
-                       ctx->stream>>>(A, kSpmmLongRow, kSpmmVeryLongRow, flag, list, cnt);
-    note_launch();
-    BCLX_CK_LAUNCH();
     BCLX_CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
     BCLX_CK(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
-    k_spmm_long<ST><<<(unsigned)ctx->num_sms, kLongWarps * 32, 0, ctx->side>>>(A, B, C, list, cnt, npanels,
-                                                                                align_ok, ctr + 1);
+    k_spmm_find_long<<<(unsigned)std::min<int64_t>(ceil_div(arows, 256), (int64_t)ctx->num_sms * 16), 256, 0,
+                       ctx->side>>>(A, kSpmmLongRow, kSpmmVeryLongRow, flag, list, cnt);
+    note_launch();
+    BCLX_CK_LAUNCH();
+    BCLX_CK(cudaEventRecord(ctx->fork2_ev, ctx->side));
+    const size_t lsmem = sizeof(LongSmem) * kLongWarps;
+    BCLX_CK(cudaFuncSetAttribute(k_spmm_long<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
+    k_spmm_long<ST><<<(unsigned)spmm_long_blocks(ctx), kLongWarps * 32, lsmem, ctx->side>>>(A, B, C, list, cnt,
+                                                                                           npanels, align_ok, ctr + 1);
     note_launch();
     BCLX_CK_LAUNCH();
     BCLX_CK(cudaEventRecord(ctx->join_ev, ctx->side));
+    BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->fork2_ev, 0));
   }
   const unsigned grid = (unsigned)(want < cap ? want : cap);
   if (R > 1)

@@ -645,7 +645,8 @@ def spmm_model_bytes(a, ts, G, N, es):
 
 def bench_spmm(args, wl, dist, device):
     """C += A*B over the tile grids (BCL::gemm(SPMatrix, DMatrix, DMatrix&)),
-    one k_spmm launch per step."""
+    one product per step (k_spmm, and k_spmm_long beside it on products with
+    at least 65536 A rows)."""
     import torch
     from bcl_b200 import _lib
     from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm
@@ -683,20 +684,21 @@ def bench_spmm(args, wl, dist, device):
     ms_per_step = total_s * 1e3 / args.steps
     value = job_rate(dist.world, flops, args.steps, total_s) / 1e9
     hbm_peak, peak_kind = peaks()
-    kern_s = statistics.mean(step_ms) / 1e3  # the step is the one k_spmm launch
+    kern_s = statistics.mean(step_ms) / 1e3  # the step is the product's kernels
     model = spmm_model_bytes(a, ts, G, N, es)
     compulsory = 8 * a.nnz + 4 * (ts + 1) * G * G + es * a.n * N + 2 * es * a.m * N
     prof = "spmm_er16k" if wl["matrix"] == "er" else "spmm_rmat21"
     roofline = {"bound": "hbm", "achieved": model / kern_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
                 "frac": model / kern_s / 1e9 / hbm_peak, "traffic": read_profile_traffic(prof),
-                "kernel": "k_spmm (all SUMMA stages, one launch)", "peak_source": peak_kind,
+                "kernel": "k_spmm + k_spmm_long (one product, all SUMMA stages)", "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": model,
                 "bytes_model": "reference per-tile-product model (spmm.hpp:383-394): A_ik, B_kj, C_ij once per product",
                 "compulsory_bytes_per_launch": compulsory,
                 "compulsory_gbs": compulsory / kern_s / 1e9, "kernel_ms": kern_s * 1e3}
     e2e = bench_spmm_e2e(args, A, B, C, stream, flops, dist)
     cfg = {"workload": wl["desc"], "tile_grid": f"{G}x{G}", "tile": ts, "nnz_A": a.nnz, "N": N,
-           "path": "one k_spmm launch: every C row sums its stages in rotated order, C += A*B in place",
+           "path": "k_spmm (short rows, grouped per warp) + k_spmm_long (rows of >= 1024 entries, side "
+                   "stream): every C row sums its stages in rotated order, C += A*B in place",
            "l2": "flushed between steps (256 MiB write outside the timed events)" if wl["matrix"] == "er"
                  else "inputs larger than L2 (B %d MB)" % (a.n * N * es >> 20),
            "parallelism": f"independent products per GPU x{dist.world}"}
