@@ -633,6 +633,21 @@ __global__ void __launch_bounds__(kLongWarps * 32)
   }
 }
 
+// A short pause on the main stream (bounded by the global timer and an
+// iteration cap; it waits for nothing).
+constexpr unsigned kLongHeadStartNs = 4000;
+
+__global__ void k_spmm_head_start(unsigned ns) {
+  uint64_t t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (int i = 0; i < 4096; i++) {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 >= ns) break;
+    __nanosleep(256);
+  }
+}
+
 // Blocks of k_spmm_long (one per SM: its shared memory fills the SM): half
 // the SMs by default, the rest run k_spmm.  BCLX_SPMM_LONG_BLOCKS overrides.
 static int spmm_long_blocks(const Context* ctx) {
@@ -704,6 +719,11 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
     BCLX_CK_LAUNCH();
     BCLX_CK(cudaEventRecord(ctx->join_ev, ctx->side));
     BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->fork2_ev, 0));
+    // k_spmm starts a few microseconds after the list is ready: the long-row
+    // blocks, which need a whole SM's shared memory, are placed first
+    k_spmm_head_start<<<1, 32, 0, ctx->stream>>>(kLongHeadStartNs);
+    note_launch();
+    BCLX_CK_LAUNCH();
   }
   const unsigned grid = (unsigned)(want < cap ? want : cap);
   if (R > 1)
