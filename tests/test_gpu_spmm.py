@@ -158,6 +158,36 @@ def test_spmm_grouped_rows(monkeypatch, rows, dtype, tiles, n, long_rows):
         assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("rows", ["1", "4"])
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_spmm_rows_without_entries_untouched(monkeypatch, dtype, rows):
+    """C rows whose A rows have no entries (over all stages) keep their exact
+    bits, NaN payloads included: no load or store reaches them; the other
+    rows match the oracle bit for bit.  With and without the long-row path."""
+    monkeypatch.setenv("BCLX_SPMM_LONG_MIN_ROWS", "0")
+    monkeypatch.setenv("BCLX_SPMM_ROWS", rows)
+    a = heavy_rows_matrix(n=8192, light=2, heavy=(3000, 1100))
+    n = 256
+    tiles = (1024, 2048, 256)
+    empty = np.diff(a.row_ptr) == 0
+    assert empty.sum() >= 100
+    b = gen.dense(a.n, n, seed=21, dist="normal")
+    c0 = gen.dense(a.m, n, seed=22)
+    if dtype == "f32":
+        c0.view(np.uint32)[empty] = np.uint32(0x7FC01234)
+        got = run(a, b, tiles, c0=c0)
+        want = O.spmm_tiled(a, b, c0, *tiles)
+        assert np.all(bits(got)[empty] == np.uint32(0x7FC01234))
+        assert np.array_equal(bits(got)[~empty], bits(want)[~empty])
+    else:
+        b16, c16 = O.to_bf16(b), O.to_bf16(c0)
+        c16[empty] = np.uint16(0x7FC5)
+        got = run(a, b16, tiles, dtype="bf16", c0=c16)
+        want = O.spmm_tiled_bf16(a, b16, c16, *tiles)
+        assert np.all(got[empty] == np.uint16(0x7FC5))
+        assert np.array_equal(got[~empty], want[~empty])
+
+
 def test_spmm_tile_single_call_ld():
     """bclx_spmm_tile with leading dimensions larger than n (sub-blocks)."""
     import ctypes
