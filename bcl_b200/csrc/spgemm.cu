@@ -540,17 +540,25 @@ __global__ void k_btable(SpGridView B, Geom g, int32_t* __restrict__ tab) {
 // the row's output count, and heavy rows also store the bitmap for the
 // numeric pass (hbm_words words per row).
 //
-// One warp per row for the light and ordinary heavy rows (heavy first) ...
+// One warp per row for the light and ordinary heavy rows (heavy first),
+// rows taken from a device counter (each warp grabs its next row while it
+// walks the current one) ...
 __global__ void __launch_bounds__(kWarpsSym * 32)
     k_symbolic(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
                const int32_t* __restrict__ heavy_list, int n_light, int n_heavy, int n_vheavy,
-               int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words) {
+               int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
+               unsigned long long* __restrict__ queue) {
   __shared__ uint32_t bm_all[kWarpsSym][kMaxWords];
   uint32_t* bm = bm_all[threadIdx.x >> 5];
   const int lane = lane_id();
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t idx = n_vheavy + warp; idx < (int64_t)n_light + n_heavy; idx += nwarps) {
+  const unsigned long long n_items = (unsigned long long)((int64_t)n_light + n_heavy - n_vheavy);
+  unsigned long long it = 0;
+  if (lane == 0) it = atomicAdd(queue, 1ULL);
+  it = __shfl_sync(kFull, it, 0);
+  while (it < n_items) {
+    unsigned long long nx = 0;
+    if (lane == 0) nx = atomicAdd(queue, 1ULL);
+    const int64_t idx = n_vheavy + (int64_t)it;
     const bool heavy = idx < n_heavy;
     const int64_t ri = heavy ? heavy_list[idx] : light_list[idx - n_heavy];
     const RowInfo x = decode_row(g, ri);
@@ -569,6 +577,7 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
     cnt = warp_sum(cnt);
     if (lane == 0) row_count[ri] = cnt;
     __syncwarp();
+    it = __shfl_sync(kFull, nx, 0);
   }
 }
 
@@ -1300,9 +1309,11 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
   }
   const int64_t rows = P->n_light + P->n_heavy - P->n_vheavy;
   if (rows > 0) {
+    // queue head 0 (each numeric launch clears its head before use)
+    BCLX_CK(cudaMemsetAsync(P->queue, 0, sizeof(unsigned long long), ctx->stream));
     k_symbolic<<<grid_for(ctx, rows, kWarpsSym, 8), kWarpsSym * 32, 0, ctx->stream>>>(
         A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, (int)P->n_heavy, (int)P->n_vheavy,
-        P->row_count, P->heavy_bitmaps, P->hbm_words);
+        P->row_count, P->heavy_bitmaps, P->hbm_words, P->queue);
     note_launch();
     BCLX_CK_LAUNCH();
   }
