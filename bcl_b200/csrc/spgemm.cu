@@ -441,12 +441,18 @@ template <bool FEATURES>
 __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restrict__ light_list,
                            int32_t* __restrict__ heavy_list, int32_t* __restrict__ vheavy_list,
                            int32_t* __restrict__ counters, unsigned long long* __restrict__ products,
-                           int heavy_min_cols, float* __restrict__ X, int32_t* __restrict__ ub_out) {
+                           int heavy_min_cols, float* __restrict__ X, int32_t* __restrict__ ub_out,
+                           unsigned long long* __restrict__ queue) {
   const int lane = lane_id();
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long mine = 0;
-  for (int64_t ri = warp; ri < g.n_row_items; ri += nwarps) {
+  // rows from a device counter, the next grab in flight while a row is walked
+  unsigned long long it = 0;
+  if (lane == 0) it = atomicAdd(queue, 1ULL);
+  it = __shfl_sync(kFull, it, 0);
+  while (it < (unsigned long long)g.n_row_items) {
+    unsigned long long nx = 0;
+    if (lane == 0) nx = atomicAdd(queue, 1ULL);
+    const int64_t ri = (int64_t)it;
     const RowInfo x = decode_row(g, ri);
     int64_t tot = 0, annz = 0;
     int32_t bmax = 0;
@@ -507,6 +513,7 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
       else
         vheavy_list[atomicAdd(&counters[3], 1)] = (int32_t)ri;
     }
+    it = __shfl_sync(kFull, nx, 0);
   }
   if (lane == 0 && mine) atomicAdd(products, mine);
 }
@@ -1444,9 +1451,10 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   // rows of tiles wider than 8192 columns always take the block path
   const int heavy_min_cols = 8192 + 1;
   if (nri > 0) {
+    BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, heavy_min_cols, nullptr,
-        nullptr);
+        nullptr, P->queue + 1);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1848,8 +1856,10 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
   BCLX_CK(cudaMemsetAsync(P.counters, 0, 4 * sizeof(int32_t), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P.products_dev, 0, sizeof(unsigned long long), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P.row_count, 0, sizeof(int32_t) * nri, ctx->stream));
+  BCLX_CK(cudaMemsetAsync(P.queue + 1, 0, sizeof(unsigned long long), ctx->stream));
   k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
-      A, B, g, P.light_list, P.heavy_tmp, P.vheavy_list, P.counters, P.products_dev, 8192 + 1, nullptr, nullptr);
+      A, B, g, P.light_list, P.heavy_tmp, P.vheavy_list, P.counters, P.products_dev, 8192 + 1, nullptr, nullptr,
+      P.queue + 1);
   note_launch();
   BCLX_CK_LAUNCH();
   int32_t cnts[4];
@@ -2004,8 +2014,10 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   BCLX_CK(cudaMemsetAsync(P->products_dev, 0, sizeof(unsigned long long), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P->row_count, 0, sizeof(int32_t) * (nri > 0 ? nri : 1), ctx->stream));
   if (nri > 0) {
+    BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
-        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, 8192 + 1, P->feat, P->ub);
+        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, 8192 + 1, P->feat, P->ub,
+        P->queue + 1);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -2272,11 +2284,12 @@ int bclx_spgemm_row_features(bclx_context_t c, const bclx_spgrid_t* a, const bcl
   unsigned long long* prod = nullptr;
   BCLX_TRY(scratch_alloc_n(ctx, &lists, 3 * (size_t)nri));
   int rc = scratch_alloc_n(ctx, &cnt, 4);
-  if (rc == BCLX_OK) rc = scratch_alloc_n(ctx, &prod, 1);
+  if (rc == BCLX_OK) rc = scratch_alloc_n(ctx, &prod, 2);  // products, row counter
   if (rc == BCLX_OK) {
     cudaMemsetAsync(cnt, 0, 4 * sizeof(int32_t), ctx->stream);
+    cudaMemsetAsync(prod, 0, 2 * sizeof(unsigned long long), ctx->stream);
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
-        make_view(*a), make_view(*b), g, lists, lists + nri, lists + 2 * nri, cnt, prod, 8192 + 1, X, ub);
+        make_view(*a), make_view(*b), g, lists, lists + nri, lists + 2 * nri, cnt, prod, 8192 + 1, X, ub, prod + 1);
     note_launch();
     if (cudaGetLastError() != cudaSuccess) rc = BCLX_ERR_CUDA;
   }
