@@ -639,8 +639,10 @@ __global__ void k_tile_ptrs(Geom g, const int64_t* __restrict__ row_offset, int3
 }
 
 // Heavy rows are cut at fine-block boundaries into items of <= kVcap outputs
-// (greedy left to right; leading empty blocks are skipped).  One thread per
-// heavy row; FILL = false counts the items, FILL = true writes them.
+// (greedy left to right; leading empty blocks are skipped).  One warp per
+// heavy row (blocks of 256 threads): lanes count the fine blocks' outputs
+// from the row's bitmap, lane 0 cuts.  FILL = false counts the items,
+// FILL = true writes them.
 struct HeavyItem {
   int32_t h;       // heavy slot
   int16_t fb_lo;   // first fine block
@@ -650,35 +652,53 @@ struct HeavyItem {
 };
 
 template <bool FILL>
-__global__ void k_cut_heavy(Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
-                            const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
-                            int32_t* __restrict__ n_items, const int64_t* __restrict__ first,
-                            HeavyItem* __restrict__ items) {
-  for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n_heavy; h += (int64_t)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(256)
+    k_cut_heavy(Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
+                const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, int32_t* __restrict__ n_items,
+                const int64_t* __restrict__ first, HeavyItem* __restrict__ items) {
+  __shared__ int32_t cnt_all[8][kMaxCols / kFineCols];
+  int32_t* cnt = cnt_all[threadIdx.x >> 5];
+  const int lane = lane_id();
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  constexpr int kWordsPerBlock = kFineCols / 32;
+  for (int64_t h = warp; h < n_heavy; h += nwarps) {
     const RowInfo x = decode_row(g, heavy_list[h]);
     const int nfb = (x.w + kFineCols - 1) / kFineCols;
     const uint32_t* bm = heavy_bitmaps + h * hbm_words;
     const int words = (x.w + 31) >> 5;
-    int nit = 0, cur = 0, start = 0, rel = 0;
-    int64_t out = FILL ? first[h] : 0;
-    for (int b = 0; b < nfb; b++) {
+    for (int b = lane; b < nfb; b += 32) {
       int c = 0;
-      for (int w = b * (kFineCols / 32); w < (b + 1) * (kFineCols / 32) && w < words; w++) c += __popc(__ldg(bm + w));
-      if (cur > 0 && cur + c > kVcap) {
-        if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)b, rel, cur};
-        nit++;
-        rel += cur;
-        cur = 0;
-        start = b;
+#pragma unroll
+      for (int q = 0; q < kWordsPerBlock; q++) {
+        const int w = b * kWordsPerBlock + q;
+        if (w < words) c += __popc(__ldg(bm + w));
       }
-      if (cur == 0 && c == 0) start = b + 1;
-      cur += c;
+      cnt[b] = c;
     }
-    if (cur > 0) {
-      if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)nfb, rel, cur};
-      nit++;
+    __syncwarp();
+    if (lane == 0) {
+      int nit = 0, cur = 0, start = 0, rel = 0;
+      int64_t out = FILL ? first[h] : 0;
+      for (int b = 0; b < nfb; b++) {
+        const int c = cnt[b];
+        if (cur > 0 && cur + c > kVcap) {
+          if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)b, rel, cur};
+          nit++;
+          rel += cur;
+          cur = 0;
+          start = b;
+        }
+        if (cur == 0 && c == 0) start = b + 1;
+        cur += c;
+      }
+      if (cur > 0) {
+        if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)nfb, rel, cur};
+        nit++;
+      }
+      if (!FILL) n_items[h] = nit;
     }
-    if (!FILL) n_items[h] = nit;
+    __syncwarp();
   }
 }
 
@@ -1489,7 +1509,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   note_launch();
   BCLX_CK_LAUNCH();
   if (P->n_heavy > 0) {
-    const unsigned blocks = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
+    const unsigned blocks = grid_for(ctx, P->n_heavy, 8, 8);
     k_cut_heavy<false><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
                                                         P->hbm_words, P->heavy_nitems, nullptr, nullptr);
     note_launch();
@@ -1511,7 +1531,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   }
   if (P->n_heavy > 0) {
     BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_items, P->n_heavy_items));
-    const unsigned blocks = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
+    const unsigned blocks = grid_for(ctx, P->n_heavy, 8, 8);
     k_cut_heavy<true><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
                                                        P->hbm_words, nullptr, P->heavy_first, P->heavy_items);
     note_launch();
@@ -1886,7 +1906,7 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
   note_launch();
   BCLX_CK_LAUNCH();
   if (P.n_heavy > 0) {
-    k_cut_heavy<false><<<grid_for(ctx, P.n_heavy / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
+    k_cut_heavy<false><<<grid_for(ctx, P.n_heavy, 8, 8), 256, 0, ctx->stream>>>(
         g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, P.heavy_nitems, nullptr, nullptr);
     note_launch();
     BCLX_CK_LAUNCH();
@@ -1916,7 +1936,7 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
     P.heavy_items = ar.take<HeavyItem>(P.n_heavy_items);
     P.tab = ar.take<int32_t>((size_t)g.tk * (g.nfb + 1));
     if (!ar.ok) return noalloc_exhausted();
-    k_cut_heavy<true><<<grid_for(ctx, P.n_heavy / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(
+    k_cut_heavy<true><<<grid_for(ctx, P.n_heavy, 8, 8), 256, 0, ctx->stream>>>(
         g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, nullptr, P.heavy_first, P.heavy_items);
     note_launch();
     BCLX_CK_LAUNCH();
@@ -2158,7 +2178,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
     BCLX_TRY(launch_symbolic(ctx, A, B, R));
     BCLX_TRY(exclusive_scan_i32(ctx, R->row_count, P->redo_off, nri));
     R->row_offset = P->redo_off;  // borrowed
-    const unsigned rb = grid_for(ctx, nf / 32 + 1, 8, 8);
+    const unsigned rb = grid_for(ctx, nf, 8, 8);
     k_cut_heavy<false><<<rb, 256, 0, ctx->stream>>>(g, R->heavy_list, nf, R->heavy_bitmaps, R->hbm_words,
                                                     R->heavy_nitems, nullptr, nullptr);
     note_launch();
