@@ -113,12 +113,7 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-
-// The same copies without a compiler memory barrier, for the pipelined loops:
+// Copies without a compiler memory barrier, for the pipelined loops:
 // there every earlier access to the target shared memory is ordered before the
 // copy by a __syncwarp, and every later one after it by a wait (which is a
 // barrier), so the loads around the copies may be scheduled freely.
