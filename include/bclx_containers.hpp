@@ -8,6 +8,11 @@
 //   bclx::CSR<T>        BCL::CSRMatrix<T, int> host matrix and its binary file
 //                       format (bcl/containers/sequential/CSRMatrix.hpp:489-530)
 //
+// Members kept from the reference: SPMatrix(fname | CSR, blocking), shape,
+// grid_shape, tile_shape, tile_nnz, nnz, tile_rank, get_tile, arget_tile,
+// assign_tile, dot, get; DMatrix shape, grid_shape, tile_shape, tile_size,
+// tile_rank, tile_ptr, get_tile, operator=(value), get_matrix.
+//
 // Every tile lives on one GPU (the one-rank case of the reference): an
 // SPMatrix packs all its CSR tiles into four device arrays plus a device
 // array of bclx_csr_t descriptors, a DMatrix keeps padded row-major tiles in
@@ -22,7 +27,10 @@
 #include <array>
 #include <cstdint>
 #include <cstdio>
+#include <fstream>
+#include <future>
 #include <memory>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -131,6 +139,81 @@ struct CSR {
       throw std::runtime_error("short read: " + path);
     return a;
   }
+  // Coordinate MatrixMarket (matrix_io.hpp:218-356, CSRMatrix.hpp:370-410):
+  // `general` or `symmetric` (an off-diagonal entry is also stored
+  // transposed), `pattern` values 1; an index repeated later in the file is
+  // ignored (the first one stays); entries sorted by (row, column).  Other
+  // formats, indices out of range and more entries than announced throw.
+  static CSR read_matrix_market(const std::string& path) {
+    std::ifstream f(path);
+    if (!f.is_open()) throw std::runtime_error("mmread: cannot open " + path);
+    std::string buf, word[5];
+    std::getline(f, buf);
+    {
+      std::istringstream ss(buf);
+      for (auto& w : word) ss >> w;
+    }
+    if (word[0] != "%%MatrixMarket" || word[1] != "matrix" || word[2] != "coordinate")
+      throw std::runtime_error(path + " could not be parsed as a Matrix Market file.");
+    const bool pattern = word[3] == "pattern";
+    bool symmetric = false;
+    if (word[4] == "symmetric")
+      symmetric = true;
+    else if (word[4] != "general")
+      throw std::runtime_error(path + " has an unsupported matrix type");
+    while (std::getline(f, buf) && !buf.empty() && buf[0] == '%') {
+    }
+    size_t m = 0, n = 0, announced = 0;
+    {
+      std::istringstream ss(buf);
+      ss >> m >> n >> announced;
+    }
+    struct Entry {
+      size_t i, j, order;
+      T v;
+    };
+    std::vector<Entry> e;
+    size_t lines = 0;
+    while (std::getline(f, buf)) {
+      std::istringstream ss(buf);
+      long long i = 0, j = 0;
+      T v = T(1);
+      if (!(ss >> i >> j)) continue;  // blank line
+      if (!pattern && !(ss >> v)) throw std::runtime_error("read_MatrixMarket: malformed entry line in " + path);
+      i--, j--;
+      if (i < 0 || j < 0 || (size_t)i >= m || (size_t)j >= n)
+        throw std::runtime_error("read_MatrixMarket: file has nonzero out of bounds.");
+      e.push_back({(size_t)i, (size_t)j, e.size(), v});
+      if (symmetric && i != j) e.push_back({(size_t)j, (size_t)i, e.size(), v});
+      if (++lines > announced)
+        throw std::runtime_error(
+            "read_MatrixMarket: error reading Matrix Market file, file has more nonzeros than reported.");
+    }
+    std::stable_sort(e.begin(), e.end(), [](const Entry& x, const Entry& y) {
+      return x.i != y.i ? x.i < y.i : x.j < y.j;
+    });
+    CSR a;
+    a.m = m, a.n = n;
+    a.row_ptr.assign(m + 1, 0);
+    for (size_t q = 0; q < e.size(); q++) {
+      if (q > 0 && e[q].i == e[q - 1].i && e[q].j == e[q - 1].j) continue;  // the first insertion stays
+      a.col_ind.push_back((int32_t)e[q].j);
+      a.vals.push_back(e[q].v);
+      a.row_ptr[e[q].i + 1]++;
+    }
+    for (size_t r = 0; r < m; r++) a.row_ptr[r + 1] += a.row_ptr[r];
+    return a;
+  }
+  // By suffix, as matrix_io's detect_file_type: .mtx or .binary.
+  static CSR read(const std::string& path) {
+    auto ends = [&](const char* s) {
+      const std::string x(s);
+      return path.size() >= x.size() && path.compare(path.size() - x.size(), x.size(), x) == 0;
+    };
+    if (ends(".mtx")) return read_matrix_market(path);
+    if (ends(".binary")) return read_binary(path);
+    throw std::runtime_error("matrix_info: Could not detect file format for \"" + path + "\"");
+  }
   void write_binary(const std::string& path) const {
     std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(path.c_str(), "wb"), std::fclose);
     if (!f) throw std::runtime_error("cannot open " + path);
@@ -157,36 +240,38 @@ class SPMatrix {
     set_packed(trp, off, {}, {});
   }
 
-  // Tile a host CSR matrix (SPMatrix(filename, blocking) reads and
-  // assign_tile's every tile, SPMatrix.hpp:277-357).
+  // Tile a host CSR matrix (columns ascending within rows): uploaded once
+  // and cut into tiles on the device by bclx_csr_to_tiles (the slicing of
+  // SPMatrix(fname, blocking), SPMatrix.hpp:194-271).
   SPMatrix(const CSR<T>& a, BlockCustom blk, int device = 0)
       : m_(a.m), n_(a.n), tm_(blk.tile_m), tn_(blk.tile_n), gm_(ceil_div(a.m, blk.tile_m)),
         gn_(ceil_div(a.n, blk.tile_n)), device_(device) {
-    std::vector<std::vector<int32_t>> tcol(ntiles());
-    std::vector<std::vector<T>> tval(ntiles());
-    std::vector<int32_t> trp(ntiles() * (tm_ + 1), 0);
-    for (size_t r = 0; r < m_; r++) {
-      const size_t ti = r / tm_, lr = r - ti * tm_;
-      for (int32_t p = a.row_ptr[r]; p < a.row_ptr[r + 1]; p++) {
-        const size_t c = (size_t)a.col_ind[p], tj = c / tn_;
-        const size_t t = ti * gn_ + tj;
-        tcol[t].push_back((int32_t)(c - tj * tn_));
-        tval[t].push_back(a.vals[p]);
-        trp[t * (tm_ + 1) + lr + 1]++;
-      }
-    }
-    std::vector<int64_t> off(ntiles() + 1, 0);
-    std::vector<int32_t> col;
-    std::vector<T> val;
-    for (size_t t = 0; t < ntiles(); t++) {
-      int32_t* rp = trp.data() + t * (tm_ + 1);
-      for (size_t r = 0; r < tm_; r++) rp[r + 1] += rp[r];
-      off[t + 1] = off[t] + (int64_t)tcol[t].size();
-      col.insert(col.end(), tcol[t].begin(), tcol[t].end());
-      val.insert(val.end(), tval[t].begin(), tval[t].end());
-    }
-    set_packed(trp, off, col, val);
+    check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+    DeviceArray<int32_t> rp, ci;
+    DeviceArray<T> v;
+    rp.resize(a.row_ptr.size());
+    rp.upload(a.row_ptr.data(), a.row_ptr.size());
+    ci.resize(a.nnz());
+    ci.upload(a.col_ind.data(), a.nnz());
+    v.resize(a.nnz());
+    v.upload(a.vals.data(), a.nnz());
+    tile_row_ptr_.resize(ntiles() * (tm_ + 1));
+    tile_offset_.resize(ntiles() + 1);
+    col_.resize(a.nnz());
+    vals_.resize(a.nnz());
+    bclx_csr_t src{};
+    src.m = (int64_t)a.m, src.n = (int64_t)a.n, src.nnz = (int64_t)a.nnz();
+    src.row_ptr = rp.data(), src.col_ind = ci.data(), src.vals = v.data();
+    src.dtype = dtype_of<T>::value;
+    bclx_spgrid_out_t out = out_grid();
+    check(bclx_csr_to_tiles(context(device_), &src, &out), "bclx_csr_to_tiles");
+    off_.assign(ntiles() + 1, 0);
+    tile_offset_.download(off_.data(), off_.size());
+    make_descriptors();
   }
+
+  // SPMatrix(fname, blocking) (SPMatrix.hpp:108-113): a .mtx or .binary file.
+  SPMatrix(const std::string& fname, BlockCustom blk, int device = 0) : SPMatrix(CSR<T>::read(fname), blk, device) {}
 
   std::array<size_t, 2> shape() const { return {m_, n_}; }
   std::array<size_t, 2> grid_shape() const { return {gm_, gn_}; }
@@ -200,6 +285,69 @@ class SPMatrix {
     return (size_t)(off_[t + 1] - off_[t]);
   }
   size_t nnz() const { return (size_t)off_.back(); }
+  // Every tile is on this GPU: rank 0 of one (SPMatrix::tile_rank).
+  size_t tile_rank(std::array<size_t, 2>) const { return 0; }
+
+  // SPMatrix::get_tile (SPMatrix.hpp:476-494): one tile copied to the host,
+  // tile-local columns.
+  CSR<T> get_tile(std::array<size_t, 2> idx) const {
+    const size_t t = idx[0] * gn_ + idx[1];
+    const auto ts = tile_shape(idx);
+    CSR<T> c;
+    c.m = ts[0], c.n = ts[1];
+    c.row_ptr.resize(ts[0] + 1);
+    c.col_ind.resize(tile_nnz(idx));
+    c.vals.resize(tile_nnz(idx));
+    check_cuda(cudaMemcpy(c.row_ptr.data(), tile_row_ptr_.data() + t * (tm_ + 1), sizeof(int32_t) * (ts[0] + 1),
+                          cudaMemcpyDeviceToHost),
+               "cudaMemcpy");
+    if (c.nnz()) {
+      check_cuda(cudaMemcpy(c.col_ind.data(), col_.data() + off_[t], sizeof(int32_t) * c.nnz(), cudaMemcpyDeviceToHost),
+                 "cudaMemcpy");
+      check_cuda(cudaMemcpy(c.vals.data(), vals_.data() + off_[t], sizeof(T) * c.nnz(), cudaMemcpyDeviceToHost),
+                 "cudaMemcpy");
+    }
+    return c;
+  }
+  // SPMatrix::arget_tile (SPMatrix.hpp:496-514): the same copy as a future.
+  std::future<CSR<T>> arget_tile(std::array<size_t, 2> idx) const {
+    return std::async(std::launch::deferred, [this, idx] { return get_tile(idx); });
+  }
+
+  // SPMatrix::assign_tile (SPMatrix.hpp:277-308): replace one tile (its
+  // shape must be tile_shape(idx); tile-local, sorted columns).
+  void assign_tile(std::array<size_t, 2> idx, const CSR<T>& tile) {
+    const auto ts = tile_shape(idx);
+    if (tile.m != ts[0] || tile.n != ts[1] || tile.row_ptr.size() != ts[0] + 1)
+      throw std::runtime_error("BCL::SPMatrix::assign_tile: tile shape mismatch");
+    const size_t t = idx[0] * gn_ + idx[1];
+    std::vector<int32_t> trp(ntiles() * (tm_ + 1));
+    std::vector<int32_t> col(nnz());
+    std::vector<T> val(nnz());
+    tile_row_ptr_.download(trp.data(), trp.size());
+    col_.download(col.data(), col.size());
+    vals_.download(val.data(), val.size());
+    std::vector<int32_t> ncol(col.begin(), col.begin() + off_[t]);
+    std::vector<T> nval(val.begin(), val.begin() + off_[t]);
+    ncol.insert(ncol.end(), tile.col_ind.begin(), tile.col_ind.end());
+    nval.insert(nval.end(), tile.vals.begin(), tile.vals.end());
+    ncol.insert(ncol.end(), col.begin() + off_[t + 1], col.end());
+    nval.insert(nval.end(), val.begin() + off_[t + 1], val.end());
+    int32_t* rp = trp.data() + t * (tm_ + 1);
+    for (size_t r = 0; r <= tm_; r++) rp[r] = r <= ts[0] ? tile.row_ptr[r] : (int32_t)tile.nnz();
+    std::vector<int64_t> off(off_);
+    const int64_t delta = (int64_t)tile.nnz() - (off_[t + 1] - off_[t]);
+    for (size_t u = t + 1; u < off.size(); u++) off[u] += delta;
+    set_packed(trp, off, ncol, nval);
+  }
+
+  // SPMatrix::dot (SPMatrix.hpp:550-553): this * other as a new matrix with
+  // this matrix's tile height and other's tile width.
+  SPMatrix dot(const SPMatrix& other) const {
+    SPMatrix c(m_, other.n_, {tm_, other.tn_}, device_);
+    gemm(*this, other, c);
+    return c;
+  }
 
   // The whole matrix on the host (SPMatrix::get_matrix-like gather).
   CSR<T> get() const {
@@ -242,6 +390,18 @@ class SPMatrix {
   friend void gemm(const SPMatrix<U>&, const SPMatrix<U>&, SPMatrix<U>&);
 
   size_t ntiles() const { return gm_ * gn_; }
+
+  bclx_spgrid_out_t out_grid() {
+    bclx_spgrid_out_t out{};
+    out.m = (int64_t)m_, out.n = (int64_t)n_, out.tile_m = (int64_t)tm_, out.tile_n = (int64_t)tn_;
+    out.grid_m = (int64_t)gm_, out.grid_n = (int64_t)gn_;
+    out.dtype = dtype_of<T>::value;
+    out.tile_row_ptr = tile_row_ptr_.data();
+    out.tile_offset = tile_offset_.data();
+    out.col_ind = col_.data();
+    out.vals = vals_.data();
+    return out;
+  }
 
   // Device arrays from packed host arrays, and the tile descriptors.
   void set_packed(const std::vector<int32_t>& trp, const std::vector<int64_t>& off, const std::vector<int32_t>& col,
@@ -330,6 +490,32 @@ class DMatrix {
   std::array<size_t, 2> shape() const { return {m_, n_}; }
   std::array<size_t, 2> grid_shape() const { return {gm_, gn_}; }
   std::array<size_t, 2> tile_shape() const { return {tm_, tn_}; }
+  // DMatrix::tile_shape(index): edge tiles hold fewer rows / columns (their
+  // storage is still padded to tile_shape()).
+  std::array<size_t, 2> tile_shape(std::array<size_t, 2> idx) const {
+    return {std::min(tm_, m_ - idx[0] * tm_), std::min(tn_, n_ - idx[1] * tn_)};
+  }
+  size_t tile_size() const { return tm_ * tn_; }
+  size_t tile_rank(std::array<size_t, 2>) const { return 0; }
+  // DMatrix::tile_ptr (DMatrix.hpp:151-157): the tile's device storage.
+  T* tile_ptr(std::array<size_t, 2> idx) const { return tiles_.data() + (idx[0] * gn_ + idx[1]) * tile_size(); }
+  // DMatrix::get_tile (DMatrix.hpp:169-173): the padded tile, row-major.
+  std::vector<T> get_tile(std::array<size_t, 2> idx) const {
+    std::vector<T> h(tile_size());
+    check_cuda(cudaMemcpy(h.data(), tile_ptr(idx), sizeof(T) * h.size(), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return h;
+  }
+  // DMatrix::operator=(value) (DMatrix.hpp:226-242): every element of every
+  // tile, padding included.
+  DMatrix& operator=(T value) {
+    if (value == T(0)) {
+      check_cuda(cudaMemset(tiles_.data(), 0, sizeof(T) * tiles_.size()), "cudaMemset");
+    } else {
+      std::vector<T> h(tiles_.size(), value);
+      tiles_.upload(h.data(), h.size());
+    }
+    return *this;
+  }
   bclx_dgrid_t grid(int32_t dtype) const {
     bclx_dgrid_t g{};
     g.m = (int64_t)m_, g.n = (int64_t)n_, g.tile_m = (int64_t)tm_, g.tile_n = (int64_t)tn_;

@@ -1,7 +1,9 @@
 """The header-only C++ containers (include/bclx_containers.hpp): BCL's
 SPMatrix / DMatrix / gemm names over the C ABI, used from a C++ program that
-reads the reference's binary CSR format.  The CPU test compiles it; the GPU
-test runs it and compares both products with the oracle bit for bit."""
+reads the reference's binary CSR format.  The CPU tests compile it and check
+its MatrixMarket reader against the reference's reader (golden fixtures); the
+GPU test runs it (device slicing, gemm, dot, the tile members) and compares
+both products with the oracle bit for bit."""
 import os
 import shutil
 import subprocess
@@ -39,6 +41,24 @@ def test_cpp_containers_compile(program):
     assert os.path.exists(program)
 
 
+@pytest.mark.parametrize("name", ["general_real_dups", "symmetric_real", "pattern_general", "integer_general"])
+def test_cpp_matrix_market_reader_golden(program, tmp_path, name):
+    """The header's MatrixMarket reader (CSR<T>::read, host only) against
+    what the reference's own reader made of the same files."""
+    from gpu_util import GOLD
+    d = np.load(os.path.join(GOLD, f"mm_{name}.npz"))
+    dt = str(d["dtype"])
+    out = str(tmp_path / "c.binary")
+    r = subprocess.run([program, "mmread", os.path.join(GOLD, f"mm_{name}.mtx"), dt, out], capture_output=True,
+                       text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    vt = np.float32 if dt == "f32" else np.int32
+    c = gen.read_binary(out, vt)
+    assert (c.m, c.n) == tuple(int(x) for x in d["c_shape"])
+    assert np.array_equal(c.row_ptr, d["c_row_ptr"]) and np.array_equal(c.col_ind, d["c_col_ind"])
+    assert np.array_equal(c.vals.view(np.uint32), d["c_vals"].astype(vt).view(np.uint32))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("tiles", [(256, 256, 256), (300, 700, 260)])
 def test_cpp_containers_match_oracle(program, tmp_path, tiles):
@@ -57,6 +77,9 @@ def test_cpp_containers_match_oracle(program, tmp_path, tiles):
     rp, ci, cv = O.gemm_tiled(a, a, *tiles)
     assert np.array_equal(c.row_ptr, rp) and np.array_equal(c.col_ind, ci)
     assert np.array_equal(c.vals.view(np.uint32), cv.view(np.uint32))
+    e = gen.read_binary(str(tmp_path / "e.binary"))  # A rebuilt tile by tile with assign_tile
+    assert np.array_equal(e.row_ptr, a.row_ptr) and np.array_equal(e.col_ind, a.col_ind)
+    assert np.array_equal(e.vals.view(np.uint32), a.vals.view(np.uint32))
     d = gen.read_dense(str(tmp_path / "c.dense"))
     want = O.spmm_tiled(a, b, np.zeros((a.m, 40), np.float32), tiles[0], tiles[1], 40)
     assert np.array_equal(d.view(np.uint32), want.view(np.uint32))
