@@ -59,6 +59,54 @@ def test_cpp_matrix_market_reader_golden(program, tmp_path, name):
     assert np.array_equal(c.vals.view(np.uint32), d["c_vals"].astype(vt).view(np.uint32))
 
 
+def _random_mtx(path, rng, m, n, count, field, symmetric):
+    i = rng.integers(1, m + 1, count)
+    j = rng.integers(1, n + 1, count)
+    if symmetric:
+        i, j = np.maximum(i, j), np.minimum(i, j)
+    rep = rng.random(count) < 0.15  # repeated indices with other values
+    src = rng.integers(0, count, count)
+    i, j = np.where(rep, i[src], i), np.where(rep, j[src], j)
+    with open(path, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate {field} {'symmetric' if symmetric else 'general'}\n% seeded\n")
+        f.write(f"{m} {n} {count}\n")
+        for a, b in zip(i, j):
+            if field == "pattern":
+                f.write(f"{a} {b}\n")
+            elif field == "integer":
+                f.write(f"{a} {b} {int(rng.integers(-50, 51))}\n")
+            else:
+                f.write(f"{a} {b} {rng.normal():.7g}\n")
+
+
+@pytest.mark.parametrize("seed,field,symmetric", [(1, "real", False), (2, "real", True), (3, "pattern", False),
+                                                  (4, "pattern", True), (5, "integer", False), (6, "integer", True)])
+def test_matrix_market_readers_match_live_reference(program, tmp_path, seed, field, symmetric):
+    """Fresh seeded MatrixMarket files (repeated indices, symmetric,
+    pattern, integer): the reference's own reader (the compiled reference
+    binary), the Python reader and the C++ header's reader agree bit for
+    bit."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("reference binary not built")
+    rng = np.random.default_rng(seed)
+    path = str(tmp_path / "x.mtx")
+    m = int(rng.integers(20, 90))
+    n = m if symmetric else int(rng.integers(20, 90))  # symmetric files are square
+    _random_mtx(path, rng, m, n, 400, field, symmetric)
+    dt = "i32" if field == "integer" else "f32"
+    vt = np.float32 if dt == "f32" else np.int32
+    subprocess.run([O.REF_BIN, "mmread", path, dt, str(tmp_path / "ref.binary")], check=True, timeout=60)
+    r = subprocess.run([program, "mmread", path, dt, str(tmp_path / "cpp.binary")], capture_output=True, text=True,
+                       timeout=60)
+    assert r.returncode == 0, r.stderr
+    ref = gen.read_binary(str(tmp_path / "ref.binary"), vt)
+    for got in (gen.read_binary(str(tmp_path / "cpp.binary"), vt), gen.read_matrix_market(path, vt)):
+        assert (got.m, got.n) == (ref.m, ref.n)
+        assert np.array_equal(got.row_ptr, ref.row_ptr) and np.array_equal(got.col_ind, ref.col_ind)
+        assert np.array_equal(np.asarray(got.vals, vt).view(np.uint32), ref.vals.view(np.uint32))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("tiles", [(256, 256, 256), (300, 700, 260)])
 def test_cpp_containers_match_oracle(program, tmp_path, tiles):
