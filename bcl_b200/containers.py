@@ -440,8 +440,17 @@ class DMatrix:
     def tile_rank(self, index) -> int:
         return 0
 
+    def tile_size(self) -> int:
+        """Elements of one (padded) tile storage (DMatrix::tile_size)."""
+        return self.tm * self.tn
+
     def tile_ptr(self, index) -> int:
         return int(self.tiles[index[0] * self.gn + index[1]].data_ptr())
+
+    def get_tile(self, index) -> torch.Tensor:
+        """The padded tile, row-major, copied to the host (DMatrix::get_tile,
+        DMatrix.hpp:169-173)."""
+        return self.tiles[index[0] * self.gn + index[1]].reshape(-1).cpu()
 
     @property
     def bclx_dtype(self) -> int:

@@ -70,3 +70,27 @@ def test_binary_roundtrip(tmp_path):
     assert (b.m, b.n, b.nnz) == (a.m, a.n, a.nnz)
     assert np.array_equal(b.row_ptr, a.row_ptr) and np.array_equal(b.col_ind, a.col_ind)
     assert np.array_equal(b.vals, a.vals)
+
+
+@pytest.mark.parametrize("m,n,tm,tn", [(10, 7, 4, 3), (64, 128, 64, 128), (37, 5, 8, 8)])
+def test_dmatrix_layout_on_host_tensors(m, n, tm, tn):
+    """DMatrix bookkeeping with host tensors: padded row-major tiles
+    (DMatrix.hpp:55-95), set_matrix / get_matrix round trip, edge tile
+    shapes, get_tile (the padded tile), operator=(value) over the padding."""
+    import torch
+    from bcl_b200.containers import DMatrix
+    gm, gn = -(-m // tm), -(-n // tn)
+    d = DMatrix(m, n, tm, tn, torch.zeros((gm * gn, tm, tn), dtype=torch.float32))
+    full = torch.arange(m * n, dtype=torch.float32).reshape(m, n)
+    d.set_matrix(full)
+    assert torch.equal(d.get_matrix(), full)
+    assert d.grid_shape() == (gm, gn) and d.tile_size() == tm * tn and d.tile_rank((0, 0)) == 0
+    for i in range(gm):
+        for j in range(gn):
+            th, tw = d.tile_shape((i, j))
+            assert (th, tw) == (min(tm, m - i * tm), min(tn, n - j * tn))
+            t = d.get_tile((i, j)).reshape(tm, tn)
+            assert torch.equal(t[:th, :tw], full[i * tm:i * tm + th, j * tn:j * tn + tw])
+            assert torch.all(t[th:, :] == 0) and torch.all(t[:, tw:] == 0)  # padding
+    d.fill_(2.5)
+    assert torch.all(d.tiles == 2.5)
