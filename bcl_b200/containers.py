@@ -143,6 +143,21 @@ def _nonempty(t: torch.Tensor) -> torch.Tensor:
 # ---- SPMatrix ----------------------------------------------------------------------
 
 
+class _Future:
+    """A deferred value with BCL::future's get() (core/future.hpp:13-72)."""
+
+    def __init__(self, fn):
+        self._fn, self._done, self._value = fn, False, None
+
+    def get(self):
+        if not self._done:
+            self._value, self._done, self._fn = self._fn(), True, None
+        return self._value
+
+    def wait(self) -> None:
+        self.get()
+
+
 class SPMatrix:
     """Distributed sparse matrix with every tile on this GPU
     (BCL::SPMatrix<T, int>, bcl/containers/SPMatrix.hpp:69-659)."""
@@ -290,6 +305,11 @@ class SPMatrix:
         ci = self.col_ind[o[t]:o[t + 1]].cpu().numpy() if o[t + 1] > o[t] else np.zeros(0, np.int32)
         v = self.vals[o[t]:o[t + 1]].cpu().numpy() if o[t + 1] > o[t] else np.zeros(0, self.dtype)
         return CSR(m, n, rp, ci, v)
+
+    def arget_tile(self, index) -> "_Future":
+        """SPMatrix::arget_tile (SPMatrix.hpp:496-514): the tile copy as a
+        future; its get() makes the copy (once)."""
+        return _Future(lambda: self.get_tile(index))
 
     def get(self) -> CSR:
         """Gather the whole matrix in global coordinates on the device

@@ -94,3 +94,33 @@ def test_dmatrix_layout_on_host_tensors(m, n, tm, tn):
             assert torch.all(t[th:, :] == 0) and torch.all(t[:, tw:] == 0)  # padding
     d.fill_(2.5)
     assert torch.all(d.tiles == 2.5)
+
+
+@pytest.mark.parametrize("tm,tn", [(100, 37), (64, 512)])
+def test_spmatrix_bookkeeping_on_host_tensors(tm, tn):
+    """SPMatrix bookkeeping with host tensors (no kernels): get_tile /
+    arget_tile against direct slices, tile_nnz, and a matrix rebuilt tile by
+    tile with assign_tile (SPMatrix.hpp:277-308, 476-514) gathered back."""
+    import torch
+    from bcl_b200.containers import SPMatrix
+    a = gen.rmat(9, seed=4)
+    trp, toff, ci, v = split_tiles(a, tm, tn)
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x))  # noqa: E731
+    A = SPMatrix(a.m, a.n, tm, tn, np.float32, 0, t(trp.astype(np.int32)), t(toff.astype(np.int64)),
+                 t(ci.astype(np.int32)), t(v.astype(np.float32)))
+    gm, gn = A.grid_shape()
+    E = SPMatrix(a.m, a.n, tm, tn, np.float32, 0, torch.zeros((gm * gn, tm + 1), dtype=torch.int32),
+                 torch.zeros(gm * gn + 1, dtype=torch.int64), torch.zeros(0, dtype=torch.int32),
+                 torch.zeros(0, dtype=torch.float32))
+    for i in range(gm):
+        for j in range(gn):
+            tile = A.get_tile((i, j))
+            rp, c, vals = naive_slice(a, i * tm, (i + 1) * tm, j * tn, (j + 1) * tn)
+            assert np.array_equal(tile.row_ptr, rp) and np.array_equal(tile.col_ind, c)
+            assert np.array_equal(tile.vals, vals) and A.tile_nnz((i, j)) == len(c)
+            fut = A.arget_tile((i, j))
+            assert np.array_equal(fut.get().col_ind, tile.col_ind)
+            E.assign_tile((i, j), tile)
+    g = E.get_host_gather()
+    assert np.array_equal(g.row_ptr, a.row_ptr) and np.array_equal(g.col_ind, a.col_ind)
+    assert np.array_equal(g.vals, a.vals) and E.nnz() == a.nnz
