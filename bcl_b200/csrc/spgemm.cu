@@ -1789,6 +1789,8 @@ int bclx_tile_accumulate_numeric(bclx_context_t c, bclx_spgemm_plan_t P, const b
 // call uses the same array, and whatever the last call left in it: the parts
 // that must start at zero are cleared by each call, and calls whose work
 // overlaps on the GPU (for instance on two streams) race with each other.
+// The host reads two sizes back during a call (cudaStreamSynchronize on the
+// caller's stream each time).
 
 namespace bclx {
 
@@ -1934,13 +1936,18 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
   }
   if (P.n_heavy > 0) {
     P.heavy_items = ar.take<HeavyItem>(P.n_heavy_items);
-    P.tab = ar.take<int32_t>((size_t)g.tk * (g.nfb + 1));
     if (!ar.ok) return noalloc_exhausted();
+    // The B-row table is optional: when what is left of the scratch cannot
+    // hold it, heavy items find their column blocks by binary search.
+    ScratchArena probe = ar;
+    P.tab = probe.take<int32_t>((size_t)g.tk * (g.nfb + 1));
+    if (probe.ok) ar = probe;
+    else P.tab = nullptr;
     k_cut_heavy<true><<<grid_for(ctx, P.n_heavy, 8, 8), 256, 0, ctx->stream>>>(
         g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, nullptr, P.heavy_first, P.heavy_items);
     note_launch();
     BCLX_CK_LAUNCH();
-    if (g.tk > 0) {
+    if (P.tab && g.tk > 0) {
       k_btable<<<grid_for(ctx, g.tk / 32 + 1, 8, 16), 256, 0, ctx->stream>>>(B, g, P.tab);
       note_launch();
       BCLX_CK_LAUNCH();
@@ -1973,8 +1980,7 @@ extern "C" int bclx_spgemm_tile_noalloc(const bclx_csr_t* a, const bclx_csr_t* b
   int device = 0;
   BCLX_CK(cudaGetDevice(&device));
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  if (a->m == 0) return BCLX_OK;
-  if (b->n == 0 || a->n == 0) {
+  if (a->m == 0 || b->n == 0 || a->n == 0) {
     BCLX_CK(cudaMemsetAsync(c_row_ptr, 0, sizeof(int32_t) * (a->m + 1), st));
     return BCLX_OK;
   }

@@ -210,6 +210,18 @@ def spgemm_alg_bytes(a_nnz, b_nnz, m, k, tm, tk, nnz_c, c_tiles, vsize=4):
     return tot
 
 
+# The ncu summary (profiles/<name>.md) whose measured DRAM bytes belong to a
+# workload's timed kernel; workloads without one report traffic as null.
+PROFILE_FOR = {("spgemm_rmat16", "fused"): "spgemm_numeric_rmat16",
+               ("spmm_rmat21", None): "spmm_rmat21",
+               ("spmm_er16k", None): "spmm_er16k"}
+
+
+def workload_traffic(workload, path=None):
+    name = PROFILE_FOR.get((workload, path))
+    return read_profile_traffic(name) if name else None
+
+
 def read_profile_traffic(name):
     """dram bytes per launch recorded in profiles/<name>.md ("traffic_bytes_per_launch: N")."""
     path = os.path.join(ROOT, "profiles", name + ".md")
@@ -349,7 +361,7 @@ def bench_spgemm(args, wl, dist, device):
     alg = spgemm_alg_bytes(a_nnz, a_nnz, n, n, ts, ts, nnz_c, c_tiles)
     hbm_peak, peak_kind = peaks()
     num_avg_s = statistics.mean(num_ms) / 1e3
-    traffic = read_profile_traffic("spgemm_numeric_rmat16")
+    traffic = workload_traffic(args.workload, args.path)
     roofline = {"bound": "hbm", "achieved": alg / num_avg_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
                 "frac": alg / num_avg_s / 1e9 / hbm_peak, "traffic": traffic,
                 "kernel": ("k_numeric (all SUMMA stages, one launch)" if args.path == "fused" else
@@ -687,9 +699,8 @@ def bench_spmm(args, wl, dist, device):
     kern_s = statistics.mean(step_ms) / 1e3  # the step is the product's kernels
     model = spmm_model_bytes(a, ts, G, N, es)
     compulsory = 8 * a.nnz + 4 * (ts + 1) * G * G + es * a.n * N + 2 * es * a.m * N
-    prof = "spmm_er16k" if wl["matrix"] == "er" else "spmm_rmat21"
     roofline = {"bound": "hbm", "achieved": model / kern_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                "frac": model / kern_s / 1e9 / hbm_peak, "traffic": read_profile_traffic(prof),
+                "frac": model / kern_s / 1e9 / hbm_peak, "traffic": workload_traffic(args.workload),
                 "kernel": "k_spmm + k_spmm_long (one product, all SUMMA stages)", "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": model,
                 "bytes_model": "reference per-tile-product model (spmm.hpp:383-394): A_ik, B_kj, C_ij once per product",

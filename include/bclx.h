@@ -261,12 +261,15 @@ BCLX_API int bclx_tile_accumulate_numeric(bclx_context_t ctx, bclx_spgemm_plan_t
  * touching c_col_ind/c_vals when *c_nnz > c_capacity (retry with more room).
  * No cudaMalloc/cudaFree: all work arrays come from a 32 MiB device array
  * that the library holds on every GPU it runs on; a tile product that needs
- * more (or B wider than 16384 columns) is rejected with BCLX_ERR_INVALID.
- * The first call on a device looks that array up and should come before any
- * stream capture.  Calls share the array: calls whose work overlaps on the
- * GPU (different streams) race.  Runs on `stream` on the current device; the
- * two phases synchronize that stream in between, and the values are ready
- * when the stream reaches the end of the call. */
+ * more (or B wider than 16384 columns) is rejected with BCLX_ERR_INVALID and
+ * nothing written to c_col_ind/c_vals.  The first call on a device looks that
+ * array up (cudaGetSymbolAddress) and should come before any stream capture.
+ * Calls share the array and each clears the parts that must start at zero:
+ * calls whose work overlaps on the GPU (different streams) race.  Runs on
+ * `stream` on the current device.  The host reads sizes back twice (after
+ * the row classification and after the row counts), synchronizing `stream`
+ * each time; the values are ready when the stream reaches the end of the
+ * call.  m == 0, k == 0 or n == 0 writes an all-zero c_row_ptr. */
 BCLX_API int bclx_spgemm_tile_noalloc(const bclx_csr_t* a, const bclx_csr_t* b, int32_t* c_row_ptr,
                                       int32_t* c_col_ind, void* c_vals, int64_t c_capacity, int64_t* c_nnz,
                                       void* stream);
