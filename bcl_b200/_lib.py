@@ -89,6 +89,9 @@ SIGNATURES = {
     "bclx_mlp_train": [vp, vp, vp, i64, vp, i32, ctypes.c_float, vp],
     "bclx_spmm_tile": [vp, i64, i64, i64, i64, vp, vp, vp, vp, vp, i64, i64, i32],
     "bclx_spmm_grid": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid)],
+    "bclx_spmm_grid_rowwise": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid)],
+    "bclx_dmatrix_sum": [vp, ctypes.POINTER(DGrid), vp],
+    "bclx_spmatrix_binary_op": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), i32],
     "bclx_csr_to_tiles": [vp, ctypes.POINTER(CSRDesc), ctypes.POINTER(SpGridOut)],
     "bclx_tiles_to_csr": [vp, ctypes.POINTER(SpGrid), vp, vp, vp],
 }

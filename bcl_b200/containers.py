@@ -136,6 +136,22 @@ def split_tiles(a: CSR, tm: int, tn: int):
     return tile_rp.astype(np.int32), tile_offset, col_local, a.vals[order]
 
 
+_BINARY_OPS = {"plus": 0, "minus": 1, "multiplies": 2, "divides": 3, "min": 4, "max": 5, "second": 6}
+
+
+def _binary_op_code(fn) -> int:
+    import operator
+    if isinstance(fn, str):
+        if fn not in _BINARY_OPS:
+            raise ValueError(f"unknown binary op {fn!r}")
+        return _BINARY_OPS[fn]
+    table = {operator.add: 0, operator.sub: 1, operator.mul: 2, operator.truediv: 3, operator.floordiv: 3,
+             min: 4, max: 5}
+    if fn in table:
+        return table[fn]
+    raise ValueError("binary_op_inplace runs on the device: pass one of " + ", ".join(_BINARY_OPS))
+
+
 def _nonempty(t: torch.Tensor) -> torch.Tensor:
     return t if t.numel() > 0 else torch.zeros(1, dtype=t.dtype, device=t.device)
 
@@ -351,7 +367,23 @@ class SPMatrix:
         counts = np.bincount(grow, minlength=self.m)
         rp = np.zeros(self.m + 1, dtype=np.int64)
         np.cumsum(counts, out=rp[1:])
-        return CSR(self.m, self.n, rp.astype(np.int32), gcol[order].astype(np.int32), v[order])
+        vals = v[order]
+        if vals.dtype == np.float32:  # as SPMatrix::get adds each value to 0: -0.0 -> +0.0
+            vals = np.float32(0) + vals
+        return CSR(self.m, self.n, rp.astype(np.int32), gcol[order].astype(np.int32), vals)
+
+    def binary_op_inplace(self, other: "DMatrix", fn) -> "SPMatrix":
+        """Every stored entry a(i, j) becomes fn(a(i, j), other(i, j))
+        (SPMatrix::binary_op_inplace, SPMatrix.hpp:571-616), on the device.
+        fn: one of "plus", "minus", "multiplies", "divides", "min", "max",
+        "second", or operator.add / sub / mul / truediv / floordiv, or the
+        builtins min / max."""
+        code = _binary_op_code(fn)
+        if other.m != self.m or other.n != self.n:
+            raise RuntimeError("BCL::SPMatrix::binary_op_inplace: shape mismatch")
+        call("bclx_spmatrix_binary_op", context(self.device).use_current_stream(), ctypes.byref(self.spgrid()),
+             ctypes.byref(other.dgrid()), code)
+        return self
 
     def assign_tile(self, index, tile: CSR) -> None:
         """Replace one tile (SPMatrix::assign_tile, SPMatrix.hpp:277-308)."""
@@ -478,7 +510,19 @@ class DMatrix:
             return _lib.F32
         if self.torch_dtype == torch.bfloat16:
             return _lib.BF16
-        raise TypeError("DMatrix tiles must be float32 or bfloat16")
+        if self.torch_dtype == torch.int32:
+            return _lib.I32
+        raise TypeError("DMatrix tiles must be float32, bfloat16 or int32")
+
+    def sum(self):
+        """Sum of every element (DMatrix::sum, DMatrix.hpp:537-554), on the
+        device: int32 exact (modulo 2^32); FP32/BF16 accumulated in FP64 and
+        rounded once to FP32 (the reference's sequential FP32 sum agrees
+        within its own rounding error)."""
+        out = (ctypes.c_int32 if self.torch_dtype == torch.int32 else ctypes.c_float)()
+        call("bclx_dmatrix_sum", context(self.device).use_current_stream(), ctypes.byref(self.dgrid()),
+             ctypes.byref(out))
+        return out.value
 
     def dgrid(self) -> DGrid:
         key = self.ptrs.data_ptr()
@@ -710,6 +754,31 @@ def spmm(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:
     h = context(a.device).use_current_stream()
     ag, bg, cg = a.spgrid(), b.dgrid(), c.dgrid()
     call("bclx_spmm_grid", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(cg))
+
+
+def rowwise_gemm(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:
+    """C += A * B with C in one tile column, every C tile row taking the k
+    tiles in ascending order (rowwise_gemm, experimental_gemm.hpp:83-123)."""
+    if a.n != b.m or a.m != c.m or b.n != c.n:
+        raise RuntimeError("BCL::rowwise_gemm: shape mismatch")
+    if c.gn != 1:
+        raise RuntimeError("BCL::rowwise_gemm: C must have one tile column")
+    h = context(a.device).use_current_stream()
+    call("bclx_spmm_grid_rowwise", h, ctypes.byref(a.spgrid()), ctypes.byref(b.dgrid()), ctypes.byref(c.dgrid()))
+
+
+def cached_rowwise_gemm(a: SPMatrix, b: DMatrix, c: DMatrix, cache_size: int = 0) -> None:
+    """cached_rowwise_gemm (experimental_gemm.hpp:125-165): the reference
+    caches fetched B rows in `cache_size` bytes; here B is resident in HBM,
+    so the cache size does not matter and the sums are rowwise_gemm's."""
+    rowwise_gemm(a, b, c)
+
+
+def batched_rowwise_gemm(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:
+    """batched_rowwise_gemm (experimental_gemm.hpp:167-212): the reference
+    sorts a tile's entries by B row to fetch each once; entries of one C row
+    keep their order, so the sums are rowwise_gemm's."""
+    rowwise_gemm(a, b, c)
 
 
 def spmm_plain(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:

@@ -107,6 +107,10 @@ struct DGridView {
   void* single;
   int64_t m, n, tm, tn, gm, gn;
   int64_t ld;  // leading dimension in elements
+  // SpMM stage order: 0 = the SUMMA loop's rotated order k = (k_ + i + j) mod
+  // G (spgemm.hpp:162-175), 1 = ascending k (the row-wise variants,
+  // experimental_gemm.hpp:83-214).  Read from the B view.
+  int32_t natural_order;
 
   __device__ __forceinline__ void* tile(int64_t i, int64_t j) const {
     return tiles ? tiles[i * gn + j] : single;

@@ -137,8 +137,9 @@ __device__ __forceinline__ void cp_async_wait_group() {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // One stage of one row of C tile (ti, tj): for stage slot kk of the
-// reference's rotated order k = (k_ + ti + tj) mod gk, the A-row segment of
-// row r in tile (ti, k) and the B tile (k, tj).  Empty when !valid.
+// reference's rotated order k = (k_ + ti + tj) mod gk (or k = kk when the B
+// view asks for ascending order), the A-row segment of row r in tile (ti, k)
+// and the B tile (k, tj).  Empty when !valid.
 template <typename ST>
 struct StageLane {
   int32_t alen;
@@ -153,7 +154,7 @@ __device__ __forceinline__ StageLane<ST> stage_lane(const SpGridView& A, const D
   StageLane<ST> s{0, nullptr, nullptr, nullptr};
   const int64_t gk = A.gn;
   if (valid && kk < gk) {
-    const int64_t k = (kk + ti + tj) % gk;
+    const int64_t k = B.natural_order ? kk : (kk + ti + tj) % gk;
     const bclx_csr_t At = A.tile(ti, k);
     const int32_t as = __ldg(At.row_ptr + r);
     s.alen = __ldg(At.row_ptr + r + 1) - as;
@@ -779,7 +780,8 @@ int bclx_spmm_tile(bclx_context_t c, int64_t m, int64_t n, int64_t k, int64_t nn
   return run_spmm(ctx, A, B, C, bc_dtype);
 }
 
-int bclx_spmm_grid(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg) {
+static int spmm_grid_impl(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg,
+                          int natural_order) {
   Context* ctx = reinterpret_cast<Context*>(c);
   if (!ctx || !a || !b || !cg || !a->tiles || !b->tiles || !cg->tiles) return BCLX_ERR_INVALID;
   if (a->dtype != BCLX_F32) return BCLX_ERR_DTYPE;
@@ -799,10 +801,23 @@ int bclx_spmm_grid(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t*
   DGridView B{};
   B.tiles = b->tiles; B.m = b->m; B.n = b->n; B.tm = b->tile_m; B.tn = b->tile_n; B.gm = b->grid_m;
   B.gn = b->grid_n; B.ld = b->tile_n;
+  B.natural_order = natural_order;
   DGridView C{};
   C.tiles = cg->tiles; C.m = cg->m; C.n = cg->n; C.tm = cg->tile_m; C.tn = cg->tile_n; C.gm = cg->grid_m;
   C.gn = cg->grid_n; C.ld = cg->tile_n;
   return run_spmm(ctx, A, B, C, b->dtype);
+}
+
+int bclx_spmm_grid(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg) {
+  return spmm_grid_impl(c, a, b, cg, 0);
+}
+
+int bclx_spmm_grid_rowwise(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg) {
+  if (cg && cg->grid_n != 1) {
+    set_last_error("the row-wise product needs C in one tile column (c.grid_shape()[1] == 1)");
+    return BCLX_ERR_INVALID;
+  }
+  return spmm_grid_impl(c, a, b, cg, 1);
 }
 
 }  // extern "C"

@@ -128,6 +128,19 @@ __global__ void k_rowptr32(const int64_t* __restrict__ off, int64_t m, int32_t* 
     rp[r] = (int32_t)off[r];
 }
 
+// A value as SPMatrix::get returns it: the reference gathers through
+// SparseHashAccumulator, which adds each value to a zero-initialised slot
+// (SparseHashAccumulator.hpp:50-53) on the host, so -0.0 comes back as +0.0
+// and a signalling NaN comes back quiet (its payload kept); every other
+// value is unchanged.  int32 values pass through.
+__device__ __forceinline__ int32_t gathered(int32_t v) { return v; }
+__device__ __forceinline__ float gathered(float v) {
+  uint32_t b = __float_as_uint(v);
+  if (b == 0x80000000u) b = 0u;
+  else if ((b & 0x7f800000u) == 0x7f800000u && (b & 0x007fffffu)) b |= 0x00400000u;
+  return __uint_as_float(b);
+}
+
 // Warp per global row: copy its runs in tile-column order.
 template <typename VT>
 __global__ void k_gather_rows(SpGridView g, const int64_t* __restrict__ off, int32_t* __restrict__ oci,
@@ -145,7 +158,7 @@ __global__ void k_gather_rows(SpGridView g, const int64_t* __restrict__ off, int
       const VT* tv = reinterpret_cast<const VT*>(t.vals);
       for (int32_t p = s + lane; p < e; p += 32) {
         oci[dst + (p - s)] = __ldg(t.col_ind + p) + shift;
-        ova[dst + (p - s)] = __ldg(tv + p);
+        ova[dst + (p - s)] = gathered(__ldg(tv + p));
       }
       dst += e - s;
     }

@@ -475,6 +475,11 @@ def spgemm_extras(args, A, a, ts, products, stream):
         ex["spgemm_plain_ms"] = t * 1e3
         ex["spgemm_plain_note"] = "16 seeded C tiles (each: G partial products + accumulation), scaled to all tiles"
     try:
+        t_ours = time_region(lambda: spgemm(A, A), 3, stream)
+        ex["cusparse_spgemm"] = cusparse_spgemm_summary(a, products, t_ours, stream)
+    except Exception as e:
+        ex["cusparse_spgemm"] = {"error": repr(e)[:300]}
+    try:
         ex["learned"] = learned_summary(A, products, stream)
     except Exception as e:  # keep the headline line even if an extra fails
         ex["learned"] = {"error": repr(e)}
@@ -493,6 +498,60 @@ def spgemm_extras(args, A, a, ts, products, stream):
         except Exception as e:
             ex["spmm_precision_rmat21"] = {"error": repr(e)}
     return ex
+
+
+def torch_csr(a, dtype=None):
+    """The matrix as a torch CUDA CSR tensor (int32 indices; values cast to
+    `dtype` when given): the input of the cuSPARSE comparator legs."""
+    import torch
+    v = torch.from_numpy(np.ascontiguousarray(a.vals)).cuda()
+    return torch.sparse_csr_tensor(torch.from_numpy(a.row_ptr.astype(np.int32)).cuda(),
+                                   torch.from_numpy(a.col_ind.astype(np.int32)).cuda(),
+                                   v if dtype is None else v.to(dtype), size=(a.m, a.n))
+
+
+def cusparse_spgemm_summary(a, products, ours_s, stream, reps=3):
+    """Comparator only (never on the product path): the reference's GPU
+    SpGEMM is cuSPARSE csrgemm per tile product plus csrgeam accumulation
+    (cusparse_util.cuh:269-514, 86-265); here cuSPARSE multiplies the whole
+    matrix in one call (torch's CUDA CSR x CSR product, cusparseSpGEMM), its
+    own summation order, on the same input."""
+    import torch
+    M = torch_csr(a)
+    out = {}
+    try:
+        C = M @ M
+        torch.cuda.synchronize()
+        out["nnz"] = int(C.values().numel())
+        del C
+        t = time_region(lambda: M @ M, reps, stream)
+        out.update({"ms": t * 1e3, "gflops": 2.0 * products / t / 1e9, "ours_over_cusparse": t / ours_s})
+    except Exception as e:
+        out["error"] = repr(e)[:300]
+    out["what"] = "torch CUDA CSR @ CSR (cusparseSpGEMM), whole matrix, one call"
+    return out
+
+
+def cusparse_spmm_leg(a, b_dev, ours_s, c_ours, stream, reps=5):
+    """Comparator only: cusparseSpMM (the reference's GPU SpMM,
+    cusparse_util.cuh:675-775, CSR_ALG2) via torch's CUDA CSR @ dense on the
+    same A and B; reports its time, our time ratio, and the relative
+    Frobenius difference between its C and ours."""
+    out = {}
+    try:
+        M = torch_csr(a, b_dev.dtype)
+        C = M @ b_dev
+        torch.cuda.synchronize()
+        if c_ours is not None:
+            d = (C.float() - c_ours.float()).norm() / c_ours.float().norm().clamp_min(1e-30)
+            out["rel_fro_diff_vs_ours"] = float(d)
+        del C
+        t = time_region(lambda: M @ b_dev, reps, stream)
+        out.update({"ms": t * 1e3, "gflops": 2.0 * a.nnz * b_dev.shape[1] / t / 1e9,
+                    "ours_over_cusparse": t / ours_s})
+    except Exception as e:
+        out["error"] = repr(e)[:300]
+    return out
 
 
 def learned_summary(A, products, stream):
@@ -554,6 +613,10 @@ def spmm_precision_summary(args, stream):
         spmm(A, B, C)
         got = C.tiles.view(-1, N)[torch.from_numpy(rows).cuda()].float().cpu().numpy().astype(np.float64)
         t = time_region(lambda: spmm(A, B, C), 3, stream)  # C += A*B again each time: same work
+        C0 = DMatrix.zeros((a.m, N), BlockCustom((ts, N)), dtype=dt)
+        spmm(A, B, C0)
+        cus = cusparse_spmm_leg(a, B.get_matrix(), t, C0.get_matrix(), stream)
+        del C0
         es = 4 if name == "fp32" else 2
         alg = 8 * a.nnz + 4 * (a.m + 1) * G + es * a.n * N + 2 * es * a.m * N
         err = np.abs(got - ref)
@@ -566,7 +629,7 @@ def spmm_precision_summary(args, stream):
                      "max_abs_err_over_max_abs": float(err.max() / np.abs(ref).max()),
                      "median_rel_entry_err": float(np.median(rel)) if rel.size else 0.0,
                      "p99_rel_entry_err": float(np.quantile(rel, 0.99)) if rel.size else 0.0,
-                     "entries_checked": int(nz.sum())}
+                     "entries_checked": int(nz.sum()), "cusparse": cus}
         del B, C
         torch.cuda.empty_cache()
     out["bf16_speedup"] = times["fp32"] / times["bf16"]
@@ -626,10 +689,13 @@ def spmm_summary(args, stream):
     B16 = DMatrix.from_array(torch.from_numpy(b), BlockCustom((ts, N)), dtype=torch.bfloat16)
     C16 = DMatrix.zeros((n, N), BlockCustom((ts, N)), dtype=torch.bfloat16)
     t16 = time_region(lambda: spmm(A, B16, C16), 20, stream)
+    C0 = DMatrix.zeros((n, N), BlockCustom((ts, N)))
+    spmm(A, B, C0)
+    cus = cusparse_spmm_leg(a, B.get_matrix(), t, C0.get_matrix(), stream, reps=20)
     hbm, _ = peaks()
     return {"workload": wl["desc"], "gflops": flops / t / 1e9, "alg_gbs": alg / t / 1e9, "frac_hbm": alg / t / 1e9 / hbm,
             "ms": t * 1e3, "plain_gflops": flops / tp / 1e9, "bf16_gflops": flops / t16 / 1e9,
-            "bf16_speedup": t / t16}
+            "bf16_speedup": t / t16, "cusparse": cus}
 
 
 def spmm_inputs(wl, seed):

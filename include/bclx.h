@@ -287,7 +287,9 @@ BCLX_API int bclx_csr_to_tiles(bclx_context_t ctx, const bclx_csr_t* a, bclx_spg
 /* Gather every tile of `g` into one CSR matrix: row_ptr [m+1], col_ind and
  * vals [nnz] (nnz = sum of tile nnz), global columns, each row's tiles in
  * column order.  Replaces SPMatrix::get (SPMatrix.hpp:516-546), on the
- * device.  Reads nnz back once (synchronizes). */
+ * device; FP32 values come back as that call returns them (it adds each to
+ * 0 in a SparseHashAccumulator: -0.0 becomes +0.0, a signalling NaN becomes
+ * quiet).  Reads nnz back once (synchronizes). */
 BCLX_API int bclx_tiles_to_csr(bclx_context_t ctx, const bclx_spgrid_t* g, int32_t* row_ptr, int32_t* col_ind,
                                void* vals);
 
@@ -305,6 +307,42 @@ BCLX_API int bclx_spmm_tile(bclx_context_t ctx, int64_t m, int64_t n, int64_t k,
  * b->dtype == c->dtype selects FP32 or BF16 storage. */
 BCLX_API int bclx_spmm_grid(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_dgrid_t* b,
                    const bclx_dgrid_t* c);
+/* The row-wise variants rowwise_gemm / cached_rowwise_gemm /
+ * batched_rowwise_gemm (bcl/containers/algorithms/experimental_gemm.hpp:
+ * 83-214): C += A * B with C in one tile column (c->grid_n == 1, else
+ * BCLX_ERR_INVALID) and each C tile row taking the k tiles in ascending
+ * order (all three variants give these sums: the cache only changes how
+ * B rows are fetched, the batched sort only reorders entries of different
+ * rows).  Same tile-grid rules and dtypes as bclx_spmm_grid. */
+BCLX_API int bclx_spmm_grid_rowwise(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_dgrid_t* b,
+                                    const bclx_dgrid_t* c);
+
+/* ---- dense and elementwise container operations -------------------------
+ * DMatrix::sum (DMatrix.hpp:537-554): the sum of every element of the
+ * grid's tiles (padding excluded), written to *result_host (float for
+ * BCLX_F32 and BCLX_BF16 storage, int32_t for BCLX_I32).  int32: the exact
+ * sum modulo 2^32 (what the reference's int accumulator wraps to).  Floating
+ * point: accumulated in FP64 on the device and rounded once to FP32; the
+ * reference adds in tile, row, column order in FP32, so the two agree within
+ * that sequential sum's own rounding error (|error| <= (n-1) u sum |x|,
+ * u = 2^-24).  Synchronizes the context's stream. */
+BCLX_API int bclx_dmatrix_sum(bclx_context_t ctx, const bclx_dgrid_t* a, void* result_host);
+
+/* SPMatrix::binary_op_inplace(DMatrix other, fn) (SPMatrix.hpp:571-616):
+ * every stored entry a(i, j) of the sparse grid becomes op(a(i, j), b(i, j)),
+ * b read at the same global (i, j) through its own tile grid (any blocking:
+ * the reference's same-layout and sliced branches give the same result).
+ * Values FP32 (b F32) or int32 (b I32).  The structure is unchanged. */
+typedef enum {
+  BCLX_OP_PLUS = 0,        /* a + b   (std::plus)       */
+  BCLX_OP_MINUS = 1,       /* a - b   (std::minus)      */
+  BCLX_OP_MULTIPLIES = 2,  /* a * b   (std::multiplies) */
+  BCLX_OP_DIVIDES = 3,     /* a / b   (std::divides; int32: b == 0 gives 0) */
+  BCLX_OP_MIN = 4,         /* b < a ? b : a (std::min)  */
+  BCLX_OP_MAX = 5,         /* a < b ? b : a (std::max)  */
+  BCLX_OP_SECOND = 6       /* b (assignment)            */
+} bclx_binary_op_t;
+BCLX_API int bclx_spmatrix_binary_op(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_dgrid_t* b, int32_t op);
 
 #ifdef __cplusplus
 }

@@ -268,10 +268,15 @@ ORACLE_ACCUMULATE(oracle_accumulate_i32, int32_t)
 /* per C tile the k blocks run in rotated order.  rows == NULL: all rows.     */
 /* For the rows subset form, C points at an nrows x N block (row ii).         */
 /* ------------------------------------------------------------------------ */
-void oracle_spmm_tiled_f32(int64_t m, int64_t K, int64_t N, const int32_t* arp, const int32_t* aci,
-                           const float* av, const float* b, int64_t ldb, float* c, int64_t ldc,
-                           int64_t tm, int64_t tk, int64_t tn, const int64_t* rows, int64_t nrows,
-                           int use_fma) {
+/* natural = 0: the SUMMA loop's rotated stage order; natural = 1: stages in
+ * ascending k, the order of rowwise_gemm / cached_rowwise_gemm /
+ * batched_rowwise_gemm (experimental_gemm.hpp:83-214: for k, for each A
+ * entry of the row in stored order, local_c[..] += row[j_]*value, an FMA
+ * with the same operands). */
+static void spmm_tiled_f32_impl(int64_t m, int64_t K, int64_t N, const int32_t* arp, const int32_t* aci,
+                                const float* av, const float* b, int64_t ldb, float* c, int64_t ldc,
+                                int64_t tm, int64_t tk, int64_t tn, const int64_t* rows, int64_t nrows,
+                                int use_fma, int natural) {
   if (!rows) nrows = m;
   int64_t gk = (K + tk - 1) / tk, gn = (N + tn - 1) / tn;
   if (gk < 1) gk = 1;
@@ -292,7 +297,7 @@ void oracle_spmm_tiled_f32(int64_t m, int64_t K, int64_t N, const int32_t* arp, 
       for (int64_t tj = 0; tj < gn; tj++) {
         int64_t j0 = tj * tn, j1 = j0 + tn < N ? j0 + tn : N;
         for (int64_t kk = 0; kk < gk; kk++) {
-          int64_t kb = (kk + ti + tj) % gk;
+          int64_t kb = natural ? kk : (kk + ti + tj) % gk;
           for (int64_t pa = akstart[kb]; pa < akstart[kb + 1]; pa++) {
             float v = av[pa];
             const float* brow = b + (int64_t)aci[pa] * ldb;
@@ -306,6 +311,40 @@ void oracle_spmm_tiled_f32(int64_t m, int64_t K, int64_t N, const int32_t* arp, 
     }
     free(akstart);
   }
+}
+
+void oracle_spmm_tiled_f32(int64_t m, int64_t K, int64_t N, const int32_t* arp, const int32_t* aci,
+                           const float* av, const float* b, int64_t ldb, float* c, int64_t ldc,
+                           int64_t tm, int64_t tk, int64_t tn, const int64_t* rows, int64_t nrows,
+                           int use_fma) {
+  spmm_tiled_f32_impl(m, K, N, arp, aci, av, b, ldb, c, ldc, tm, tk, tn, rows, nrows, use_fma, 0);
+}
+
+void oracle_spmm_rowwise_f32(int64_t m, int64_t K, int64_t N, const int32_t* arp, const int32_t* aci,
+                             const float* av, const float* b, int64_t ldb, float* c, int64_t ldc,
+                             int64_t tm, int64_t tk, int64_t tn, const int64_t* rows, int64_t nrows) {
+  spmm_tiled_f32_impl(m, K, N, arp, aci, av, b, ldb, c, ldc, tm, tk, tn, rows, nrows, 1, 1);
+}
+
+/* DMatrix::sum (DMatrix.hpp:537-554) on a row-major m x n matrix cut into
+ * tm x tn tiles: tiles in row-major grid order, each tile's rows, each row's
+ * columns, `local_sum += value` in FP32 from 0 (out[0]); also the FP64 sum
+ * (out[1]) and the sum of magnitudes (out[2]) for the error bound. */
+void oracle_dsum_f32(int64_t m, int64_t n, int64_t tm, int64_t tn, const float* x, double* out) {
+  float s = 0.0f;
+  double d = 0.0, a = 0.0;
+  for (int64_t i0 = 0; i0 < m; i0 += tm)
+    for (int64_t j0 = 0; j0 < n; j0 += tn)
+      for (int64_t i = i0; i < i0 + tm && i < m; i++)
+        for (int64_t j = j0; j < j0 + tn && j < n; j++) {
+          const float v = x[i * n + j];
+          s = s + v;
+          d += (double)v;
+          a += fabs((double)v);
+        }
+  out[0] = (double)s;
+  out[1] = d;
+  out[2] = a;
 }
 
 /* Same loop in double over FP32 inputs (error reference); c is double. */

@@ -132,6 +132,69 @@ def spmm_tiled(a, b, c0, tm, tk, tn, rows=None, use_fma=True):
     return c
 
 
+def spmm_rowwise(a, b, c0, tm, tk, tn, rows=None):
+    """C = C0 + A*B with the stages in ascending k (rowwise_gemm and its
+    cached / batched variants, experimental_gemm.hpp:83-214)."""
+    rows_a, nr = _rows_arg(rows)
+    c = np.array(c0, dtype=np.float32, copy=True, order="C")
+    b = np.ascontiguousarray(b, dtype=np.float32)
+    av = np.ascontiguousarray(a.vals, dtype=np.float32)
+    lib().oracle_spmm_rowwise_f32(*_i64(a.m, a.n, b.shape[1]), _p(a.row_ptr), _p(a.col_ind), _p(av),
+                                  _p(b), ctypes.c_int64(b.shape[1]), _p(c), ctypes.c_int64(c.shape[1]),
+                                  *_i64(tm, tk, tn), _p(rows_a), ctypes.c_int64(nr))
+    return c
+
+
+def dmatrix_sum(x, tm, tn):
+    """DMatrix::sum in the reference's order (FP32 sequential), plus the
+    FP64 sum and the sum of magnitudes: (f32_sum, f64_sum, abs_sum)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.zeros(3, np.float64)
+    lib().oracle_dsum_f32(*_i64(x.shape[0], x.shape[1], tm, tn), _p(x), _p(out))
+    return np.float32(out[0]), float(out[1]), float(out[2])
+
+
+def binary_op(a, b_dense, op):
+    """SPMatrix::binary_op_inplace (SPMatrix.hpp:571-616): every stored
+    entry a(i, j) becomes fn(a(i, j), b(i, j)); one IEEE rounding per
+    operation for FP32, wrapping for int32.  Returns the new values."""
+    rows = np.repeat(np.arange(a.m), np.diff(a.row_ptr.astype(np.int64)))
+    bv = np.asarray(b_dense)[rows, a.col_ind]
+    av = np.asarray(a.vals)
+    with np.errstate(all="ignore"):
+        if op == "plus":
+            return av + bv
+        if op == "minus":
+            return av - bv
+        if op == "multiplies":
+            return av * bv
+        if op == "divides":
+            if av.dtype == np.int32:  # C truncation; division by zero gives 0 here
+                q = np.zeros_like(av)
+                nz = bv != 0
+                q[nz] = np.trunc(av[nz].astype(np.float64) / bv[nz]).astype(np.int64).astype(np.int32)
+                return q
+            return av / bv
+        if op == "min":
+            return np.where(bv < av, bv, av)
+        if op == "max":
+            return np.where(av < bv, bv, av)
+        if op == "second":
+            return bv.copy()
+    raise ValueError(op)
+
+
+def gather_value(v):
+    """What SPMatrix::get (SPMatrix.hpp:516-546) makes of a stored value: it
+    goes through SparseHashAccumulator, which adds it to a zero-initialised
+    slot (SparseHashAccumulator.hpp:50-53), so -0.0 becomes +0.0 and a NaN
+    comes back quiet; everything else is unchanged."""
+    v = np.asarray(v)
+    if v.dtype != np.float32:
+        return v.copy()
+    return np.float32(0) + v
+
+
 def spmm_f64(a, b, rows=None):
     """A*B accumulated in double (all rows or the listed ones)."""
     rows_a, nr = _rows_arg(rows)

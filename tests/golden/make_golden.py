@@ -17,6 +17,12 @@ Each fixture is an .npz holding the inputs and the reference's outputs:
   reference's reader makes of each (CSRMatrix(fname), matrix_io.hpp:218-356).
 * ``tiles_*``: every tile of SPMatrix(fname, BlockCustom) (the reference's
   slicing, SPMatrix.hpp:194-271), row-major over the grid.
+* ``rowwise_*``: rowwise_gemm / cached_rowwise_gemm / batched_rowwise_gemm
+  (experimental_gemm.hpp:83-214), C = 0 first.
+* ``dsum_*``: DMatrix::sum (DMatrix.hpp:537-554), the FP32 bits it returns.
+* ``binop_*``: SPMatrix::binary_op_inplace (SPMatrix.hpp:571-616) with the
+  standard functors, on one tile (the reference's loops bound i and j by
+  grid_shape()[i] and grid_shape()[j], in range only for a 1x1 grid).
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -197,9 +203,70 @@ def io_fixtures():
         print(f"tiles_{name}: {len(nnzs)} tiles")
 
 
+def container_fixtures():
+    import subprocess
+    import tempfile
+    for name, am, bd, tiles in [
+        ("rmat10_n64_t256", gen.rmat(10, seed=70), gen.dense(1024, 64, seed=71), (256, 256, 64)),
+        ("empty_rect_n24_ragged", sparse_with_empty(300, 200, seed=72), gen.dense(200, 24, seed=73, dist="normal"),
+         (70, 60, 24)),
+    ]:
+        d = {"tiles": np.array(tiles, np.int64), "b": bd}
+        d.update(csr_dict("a", am))
+        for variant in ("plain", "cached", "batched"):
+            with tempfile.TemporaryDirectory() as td:
+                fa, fb, fc = (os.path.join(td, x) for x in ("a.binary", "b.dense", "c.dense"))
+                gen.write_binary(fa, am)
+                gen.write_dense(fb, bd)
+                subprocess.run([O.REF_BIN, "rowwise", variant, fa, fb] + [str(t) for t in tiles] + [fc],
+                               check=True, capture_output=True)
+                d[f"c_{variant}"] = gen.read_dense(fc)
+        np.savez_compressed(os.path.join(OUT, f"rowwise_{name}.npz"), **d)
+        print(f"rowwise_{name}")
+    import json
+    for name, x, tiles in [("u300x70_t64x32", gen.dense(300, 70, seed=74), (64, 32)),
+                           ("n1000x257_t128x100", gen.dense(1000, 257, seed=75, dist="normal") * 1e3, (128, 100))]:
+        with tempfile.TemporaryDirectory() as td:
+            fb = os.path.join(td, "b.dense")
+            gen.write_dense(fb, x.astype(np.float32))
+            out = subprocess.run([O.REF_BIN, "dsum", fb, str(tiles[0]), str(tiles[1])], check=True,
+                                 capture_output=True, text=True).stdout
+        res = json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
+        np.savez_compressed(os.path.join(OUT, f"dsum_{name}.npz"), x=x.astype(np.float32),
+                            tiles=np.array(tiles, np.int64), bits=np.array(res["bits"], np.uint32))
+        print(f"dsum_{name}: {res['sum']}")
+    rng = np.random.default_rng(76)
+    for dt in ("f32", "i32"):
+        am = sparse_with_empty(120, 90, seed=77, value_type=dt)
+        if dt == "f32":
+            bd = rng.uniform(-2, 2, (120, 90)).astype(np.float32)
+            bd[rng.random(bd.shape) < 0.05] = 0.0
+        else:
+            bd = rng.integers(-5, 6, (120, 90)).astype(np.int32)
+        d = {"b": bd}
+        d.update(csr_dict("a", am))
+        for op in ("plus", "minus", "multiplies", "divides", "min", "max", "second"):
+            with tempfile.TemporaryDirectory() as td:
+                fa, fb, fc = (os.path.join(td, x) for x in ("a.binary", "b.dense", "c.binary"))
+                gen.write_binary(fa, am)
+                gen.write_dense(fb, bd)
+                if dt == "i32" and op == "divides":
+                    continue  # integer division by zero is undefined in the reference
+                subprocess.run([O.REF_BIN, "binop", op, fa, fb, dt, fc], check=True, capture_output=True)
+                c = gen.read_binary(fc, np.float32 if dt == "f32" else np.int32)
+                cg = gen.read_binary(fc + ".get", np.float32 if dt == "f32" else np.int32)
+            d[f"vals_{op}"] = c.vals
+            d[f"get_{op}"] = cg.vals
+        np.savez_compressed(os.path.join(OUT, f"binop_sparse120x90_{dt}.npz"), **d)
+        print(f"binop_sparse120x90_{dt}")
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["io"]:
         io_fixtures()
+    elif sys.argv[1:] == ["containers"]:
+        container_fixtures()
     else:
         main()
         io_fixtures()
+        container_fixtures()

@@ -96,3 +96,48 @@ def test_oracle_matches_live_reference_fresh_seed():
         assert np.array_equal(rp, c.row_ptr.astype(np.int64))
         assert np.array_equal(ci, c.col_ind)
         assert same_bits(cv, c.vals)
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "rowwise_*.npz"))), ids=os.path.basename)
+def test_oracle_rowwise_matches_reference(path):
+    """rowwise_gemm, cached_rowwise_gemm and batched_rowwise_gemm all equal
+    the ascending-stage restatement, bit for bit."""
+    d = np.load(path)
+    a = load_csr(d, "a")
+    tiles = [int(t) for t in d["tiles"]]
+    c = O.spmm_rowwise(a, d["b"], np.zeros_like(d["c_plain"]), *tiles)
+    for variant in ("plain", "cached", "batched"):
+        assert same_bits(c, d[f"c_{variant}"]), variant
+
+
+def test_oracle_rowwise_order_differs_from_summa():
+    """On a grid with more than one stage the ascending order is a different
+    FP32 sum from the SUMMA loop's rotated order (so the two are told apart)."""
+    d = np.load(os.path.join(GOLD, "rowwise_rmat10_n64_t256.npz"))
+    a = load_csr(d, "a")
+    tiles = [int(t) for t in d["tiles"]]
+    c = O.spmm_tiled(a, d["b"], np.zeros_like(d["c_plain"]), *tiles)
+    assert not same_bits(c, d["c_plain"])
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "dsum_*.npz"))), ids=os.path.basename)
+def test_oracle_dsum_matches_reference(path):
+    d = np.load(path)
+    s32, s64, sabs = O.dmatrix_sum(d["x"], *[int(t) for t in d["tiles"]])
+    assert np.array_equal(np.array([s32], np.float32).view(np.uint32), d["bits"].reshape(1))
+    # the sequential FP32 sum is within its rounding bound of the FP64 sum
+    n = d["x"].size
+    assert abs(float(s32) - s64) <= (n - 1) * 2.0 ** -24 * sabs
+
+
+@pytest.mark.parametrize("dt", ["f32", "i32"])
+def test_oracle_binary_op_matches_reference(dt):
+    d = np.load(os.path.join(GOLD, f"binop_sparse120x90_{dt}.npz"))
+    a = load_csr(d, "a")
+    for key in d.files:
+        if key.startswith("vals_"):
+            op = key[5:]
+            got = O.binary_op(a, d["b"], op)
+            assert same_bits(got, d[key]), op
+            # SPMatrix::get adds every value to 0: -0 comes back as +0
+            assert same_bits(O.gather_value(got), d["get_" + op]), op
