@@ -68,6 +68,8 @@ SIGNATURES = {
     "bclx_spgemm_numeric": [vp, vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
                             i32, i32],
     "bclx_spgemm_plan_destroy": [vp],
+    "bclx_spgemm_symbolic_sub": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
+                                 vp, vp, ctypes.POINTER(vp), ctypes.POINTER(i64)],
     "bclx_spgemm_numeric_staged": [vp, vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut),
                                    i32],
     "bclx_spgemm_plan_tune": [vp, i32, i32, i32],

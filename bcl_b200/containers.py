@@ -622,6 +622,118 @@ def spgemm(a: SPMatrix, b: SPMatrix, stages: str = "fused", keep_plan: bool = Fa
     return c
 
 
+# ---- distributed products (one process per GPU) ------------------------------------
+
+
+def process_grid(world: int) -> Tuple[int, int]:
+    """pm x pn process grid for `world` processes, as square as possible
+    (pm <= pn), the shape of the reference's default BlockSquare layout."""
+    pm = int(world ** 0.5)
+    while world % pm:
+        pm -= 1
+    return pm, world // pm
+
+
+def owned_tiles(gm: int, gn: int, rank: int, pm: int, pn: int):
+    """Tile rows and columns whose C tiles process `rank` owns in the
+    reference's block-cyclic layout: tile (i, j) belongs to process
+    (j % pn) + (i % pm) * pn (SPMatrix.hpp:230-237).  The owned tiles are the
+    Cartesian product of the two lists."""
+    r, c = divmod(rank, pn)
+    return [i for i in range(gm) if i % pm == r], [j for j in range(gn) if j % pn == c]
+
+
+def _sub_spgrid(x: SPMatrix, rows, cols):
+    """Tile rows `rows` x tile columns `cols` of x as a grid view: a gathered
+    descriptor array (the tiles themselves are not copied)."""
+    td = x.desc.device
+    r = torch.as_tensor(list(rows), dtype=torch.int64, device=td)
+    c = torch.as_tensor(list(cols), dtype=torch.int64, device=td)
+    desc = x.desc[(r[:, None] * x.gn + c[None, :]).reshape(-1)].contiguous()
+    m = sum(min(x.tm, x.m - i * x.tm) for i in rows)
+    n = sum(min(x.tn, x.n - j * x.tn) for j in cols)
+    return SpGrid(m, n, x.tm, x.tn, len(rows), len(cols), desc.data_ptr(), _NP_TO_DT[x.dtype], 0), desc
+
+
+def spgemm_sub(a: SPMatrix, b: SPMatrix, tile_rows, tile_cols) -> SPMatrix:
+    """The C tiles (i, j), i in tile_rows, j in tile_cols (increasing global
+    tile indices), of C = A * B, bit-identical to those tiles of the whole
+    product (each keeps its stage order k = (k_ + i + j) mod G): what one
+    process of the reference's stationary-C loop computes
+    (spgemm.hpp:194-224).  The result is an SPMatrix of those tiles in
+    sub-grid order (bclx_spgemm_symbolic_sub)."""
+    _check_grids(a, b)
+    tile_rows, tile_cols = list(tile_rows), list(tile_cols)
+    if any(q <= p for p, q in zip(tile_rows, tile_rows[1:])) or any(q <= p for p, q in zip(tile_cols, tile_cols[1:])):
+        raise ValueError("tile rows and columns must be increasing")
+    h = context(a.device).use_current_stream()
+    ag, adesc = _sub_spgrid(a, tile_rows, range(a.gn))
+    bg, bdesc = _sub_spgrid(b, range(b.gm), tile_cols)
+    td = a.tile_row_ptr.device
+    gm, gn = len(tile_rows), len(tile_cols)
+    trp = torch.empty((gm * gn, a.tm + 1), dtype=torch.int32, device=td)
+    toff = torch.empty(gm * gn + 1, dtype=torch.int64, device=td)
+    out = SpGridOut(ag.m, bg.n, a.tm, b.tn, gm, gn, trp.data_ptr(), toff.data_ptr(), None, None,
+                    _NP_TO_DT[a.dtype], 0)
+    rows_arr = (ctypes.c_int64 * max(gm, 1))(*tile_rows)
+    cols_arr = (ctypes.c_int64 * max(gn, 1))(*tile_cols)
+    plan = ctypes.c_void_p()
+    nnz = ctypes.c_int64()
+    call("bclx_spgemm_symbolic_sub", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), rows_arr, cols_arr,
+         ctypes.byref(plan), ctypes.byref(nnz))
+    pl = SpgemmPlan(plan)
+    ci = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=td)
+    v = torch.empty(max(nnz.value, 1), dtype=_TORCH_OF[_NP_TO_DT[a.dtype]], device=td)
+    out.col_ind, out.vals = ci.data_ptr(), v.data_ptr()
+    call("bclx_spgemm_numeric", h, pl.h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), 0, 0)
+    pl.close()
+    del adesc, bdesc  # (the numeric pass is ordered on the stream before any reuse)
+    return SPMatrix(ag.m, bg.n, a.tm, b.tn, a.dtype, a.device, trp, toff, ci, v)
+
+
+def spgemm_distributed(a: SPMatrix, b: SPMatrix, rank: int, world: int, pgrid=None):
+    """This process's C tiles of C = A * B under the reference's block-cyclic
+    ownership, A's tile rows and B's tile columns being available here (A
+    and B replicated, as for A * A with A loaded on every process): no data
+    exchange is needed.  Returns (C sub-grid, tile rows, tile columns)."""
+    pm, pn = pgrid or process_grid(world)
+    rows, cols = owned_tiles(a.gm, b.gn, rank, pm, pn)
+    if not rows or not cols:
+        return None, rows, cols
+    return spgemm_sub(a, b, rows, cols), rows, cols
+
+
+def assemble_tiles(m: int, n: int, tm: int, tn: int, parts) -> CSR:
+    """The whole matrix on the host from sub-grid results: parts is a list of
+    (tile_rows, tile_cols, tile_row_ptr, tile_offset, col_ind, vals) host
+    arrays, one per process (SPMatrix::get of a distributed matrix)."""
+    gm, gn = _ceil_div(m, tm), _ceil_div(n, tn)
+    tiles = {}
+    if sum(len(p[0]) * len(p[1]) for p in parts) != gm * gn:
+        raise RuntimeError("the parts do not cover every tile exactly once")
+    for rows, cols, trp, toff, ci, v in parts:
+        trp = np.asarray(trp).reshape(len(rows) * len(cols), tm + 1)
+        for a_, i in enumerate(rows):
+            for b_, j in enumerate(cols):
+                t = a_ * len(cols) + b_
+                tiles[(i, j)] = (trp[t], ci[toff[t]:toff[t + 1]], v[toff[t]:toff[t + 1]])
+    if len(tiles) != gm * gn:
+        raise RuntimeError("the parts do not cover every tile exactly once")
+    rp = [0]
+    cis, vs = [], []
+    for i in range(gm):
+        for r in range(min(tm, m - i * tm)):
+            for j in range(gn):
+                trow, ci, v = tiles[(i, j)]
+                s, e = int(trow[r]), int(trow[r + 1])
+                cis.append(np.asarray(ci[s:e], np.int64) + j * tn)
+                vs.append(np.asarray(v[s:e]))
+            rp.append(rp[-1] + sum(len(x) for x in cis[len(cis) - gn:]))
+    ci = np.concatenate(cis).astype(np.int32) if cis else np.zeros(0, np.int32)
+    val = np.concatenate(vs) if vs else np.zeros(0, np.float32)
+    return CSR(m, n, np.asarray(rp, np.int32), ci, val)
+
+
 def spgemm_learned(a: SPMatrix, b: SPMatrix, predictor="default", keep_plan: bool = False):
     """C = A * B through the learned product: a row-nnz predictor sizes the
     work instead of a symbolic pass; rows it mispredicts are redone exactly,

@@ -67,11 +67,23 @@ struct Geom {
   int64_t n_row_items;  // gm * gn * tm
   int64_t nfb;          // fine blocks per (full) tile width: ceil(tn / kFineCols)
   // Stage map (or null: every stage): for C tile t = ti*gn + tj, scount[t]
-  // positions kk (ascending) of the rotated order k = (kk + ti + tj) mod gk
+  // positions kk (ascending) of the rotated order k = (kk + rotation) mod gk
   // whose A_ik and B_kj tiles both have entries, in smap[t*gk ...].
   const int32_t* smap = nullptr;
   const int32_t* scount = nullptr;
+  // Sub-grid products (or null: C's tile (ti, tj) is global tile (ti, tj)):
+  // the global tile row / column of each C tile row / column, which sets
+  // the rotated stage order k = (kk + gi + gj) mod gk.
+  const int32_t* rot_i = nullptr;
+  const int32_t* rot_j = nullptr;
 };
+
+// Rotation of C tile (ti, tj): stage position kk is k = (kk + rotation) mod gk.
+__device__ __forceinline__ int64_t tile_rotation(const Geom& g, int64_t ti, int64_t tj) {
+  const int64_t gi = g.rot_i ? (int64_t)__ldg(g.rot_i + ti) : ti;
+  const int64_t gj = g.rot_j ? (int64_t)__ldg(g.rot_j + tj) : tj;
+  return (gi + gj) % g.gk;
+}
 
 __device__ __forceinline__ int stage_count(const Geom& g, int64_t ti, int64_t tj) {
   return g.scount ? __ldg(g.scount + ti * g.gn + tj) : (int)g.gk;
@@ -123,7 +135,8 @@ __device__ __forceinline__ void b_block_range(const int32_t* trows, const int32_
 
 struct RowInfo {
   int64_t ti, tj, r;
-  int w;  // width of the C tile (columns)
+  int64_t rot;  // the C tile's stage rotation (tile_rotation)
+  int w;        // width of the C tile (columns)
 };
 
 __device__ __forceinline__ RowInfo decode_row(const Geom& g, int64_t ri) {
@@ -132,6 +145,7 @@ __device__ __forceinline__ RowInfo decode_row(const Geom& g, int64_t ri) {
   x.r = ri - t * g.tm;
   x.ti = t / g.gn;
   x.tj = t - x.ti * g.gn;
+  x.rot = tile_rotation(g, x.ti, x.tj);
   int64_t w = g.n - x.tj * g.tn;
   x.w = (int)(w < g.tn ? w : g.tn);
   return x;
@@ -195,7 +209,7 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
     const VT* bva = nullptr;
     if (si < w1) {
       kk = stage_at(g, x.ti, x.tj, si);
-      const int64_t k = (kk + x.ti + x.tj) % g.gk;
+      const int64_t k = (kk + x.rot) % g.gk;
       const bclx_csr_t At = A.tile(x.ti, k);
       as = __ldg(At.row_ptr + x.r);
       alen = __ldg(At.row_ptr + x.r + 1) - as;
@@ -319,7 +333,7 @@ __device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridVi
     const int32_t* brp = nullptr;
     const int32_t* bci = nullptr;
     if (si < ns) {
-      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.ti + x.tj) % g.gk;
+      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.rot) % g.gk;
       const bclx_csr_t At = A.tile(x.ti, k);
       as = __ldg(At.row_ptr + x.r);
       alen = __ldg(At.row_ptr + x.r + 1) - as;
@@ -386,7 +400,7 @@ __device__ __forceinline__ void walk_columns_ranged(const SpGridView& A, const S
     const int32_t* brp = nullptr;
     const int32_t* bci = nullptr;
     if (si < ns) {
-      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.ti + x.tj) % g.gk;
+      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.rot) % g.gk;
       const bclx_csr_t At = A.tile(x.ti, k);
       as = __ldg(At.row_ptr + x.r);
       alen = __ldg(At.row_ptr + x.r + 1) - as;
@@ -464,7 +478,7 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
         const int32_t* acol = nullptr;
         const int32_t* brp = nullptr;
         if (si < ns) {
-          const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.ti + x.tj) % g.gk;
+          const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.rot) % g.gk;
           const bclx_csr_t At = A.tile(x.ti, k);
           as = __ldg(At.row_ptr + x.r);
           alen = __ldg(At.row_ptr + x.r + 1) - as;
@@ -527,9 +541,9 @@ __global__ void k_btable(SpGridView B, Geom g, int32_t* __restrict__ tab) {
   for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < nrows; x += (int64_t)gridDim.x * blockDim.x) {
     const int64_t kt = x / g.tk, r = x - kt * g.tk;
     const int64_t k = kt / g.gn, j = kt - k * g.gn;
-    if (r >= B.rows_of(k)) continue;
-    int32_t* trow = tab + x * (g.nfb + 1);
     const bclx_csr_t Bt = B.tile(k, j);
+    if (r >= Bt.m) continue;  // the tile's own row count (sub-grids may reorder B's tiles)
+    int32_t* trow = tab + x * (g.nfb + 1);
     const int32_t b0 = __ldg(Bt.row_ptr + r), b1 = __ldg(Bt.row_ptr + r + 1);
     int b = 0;
     for (int32_t q = b0; q < b1; q++) {
@@ -1148,7 +1162,7 @@ __global__ void __launch_bounds__(256) k_heavy_block_ub(SpGridView A, SpGridView
     __syncwarp();
     const int ns = stage_count(g, x.ti, x.tj);
     for (int si = 0; si < ns; si++) {
-      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.ti + x.tj) % g.gk;
+      const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.rot) % g.gk;
       const bclx_csr_t At = A.tile(x.ti, k);
       const int32_t a0 = __ldg(At.row_ptr + x.r), a1 = __ldg(At.row_ptr + x.r + 1);
       if (tab) {
@@ -1384,6 +1398,7 @@ struct bclx_spgemm_plan_s {
   int32_t* tab = nullptr;
   int32_t* smap_own = nullptr;    // stage map (Geom::smap / scount) owned by this plan
   int32_t* scount_own = nullptr;
+  int32_t* rot_own = nullptr;     // sub-grid tile maps (Geom::rot_i, then rot_j) owned by this plan
   unsigned long long* queue = nullptr;  // work-queue heads, one per stage launch
   // numeric tuning (bclx_spgemm_plan_tune)
   int grab = 1, blocks_per_sm = 4, long_seg = kLongSegDefault;
@@ -1457,10 +1472,10 @@ struct bclx_spgemm_plan_s {
     temp_val = redo_val = nullptr;
     void* ps[] = {queue, light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
                   heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset,
-                  smap_own, scount_own};
+                  smap_own, scount_own, rot_own};
     for (void* p : ps) scratch_free(ctx, p);
     queue = nullptr;
-    smap_own = scount_own = nullptr;
+    smap_own = scount_own = rot_own = nullptr;
     light_list = heavy_list = vheavy_list = heavy_tmp = counters = row_count = heavy_nitems = tab = id_rp = id_ci = nullptr;
     products_dev = nullptr;
     row_offset = heavy_first = acc_tile_offset = nullptr;
@@ -1581,8 +1596,9 @@ __global__ void k_stage_map(SpGridView A, SpGridView B, Geom g, int32_t* __restr
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t ti = t / g.gn, tj = t - ti * g.gn;
     int32_t c = 0;
+    const int64_t rot = tile_rotation(g, ti, tj);
     for (int64_t kk = 0; kk < g.gk; kk++) {
-      const int64_t k = (kk + ti + tj) % g.gk;
+      const int64_t k = (kk + rot) % g.gk;
       if (A.tile(ti, k).nnz > 0 && B.tile(k, tj).nnz > 0) smap[t * g.gk + c++] = (int32_t)kk;
     }
     scount[t] = c;
@@ -1758,18 +1774,43 @@ static Geom make_geom(const bclx_spgrid_out_t* c, int64_t gk, int64_t tk) {
 
 extern "C" {
 
-int bclx_spgemm_symbolic(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b, bclx_spgrid_out_t* out,
-                         bclx_spgemm_plan_t* plan, int64_t* nnz) {
+static int symbolic_entry(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b, bclx_spgrid_out_t* out,
+                          const int64_t* tile_rows, const int64_t* tile_cols, bclx_spgemm_plan_t* plan,
+                          int64_t* nnz) {
   Context* ctx = reinterpret_cast<Context*>(c);
   if (!ctx || !plan || !nnz) return BCLX_ERR_INVALID;
   *plan = nullptr;
   BCLX_TRY(check_grids(a, b, out));
   if (!out->tile_row_ptr || !out->tile_offset) return BCLX_ERR_INVALID;
+  const int64_t G = a->grid_n;
+  if (tile_rows) {
+    // global tile indices: increasing (so only the last may be a ragged edge tile) and in range
+    for (int64_t i = 0; i < out->grid_m; i++)
+      if (tile_rows[i] < 0 || tile_rows[i] >= INT32_MAX || (i > 0 && tile_rows[i] <= tile_rows[i - 1]))
+        return BCLX_ERR_INVALID;
+    for (int64_t j = 0; j < out->grid_n; j++)
+      if (tile_cols[j] < 0 || tile_cols[j] >= INT32_MAX || (j > 0 && tile_cols[j] <= tile_cols[j - 1]))
+        return BCLX_ERR_INVALID;
+  }
   BCLX_CK(cudaSetDevice(ctx->device));
   auto* P = new bclx_spgemm_plan_s();
   P->ctx = ctx;
-  int rc = symbolic_impl(ctx, make_view(*a), make_view(*b), make_geom(out, a->grid_n, a->tile_n), a->dtype,
-                         out->tile_row_ptr, out->tile_offset, P);
+  Geom g = make_geom(out, G, a->tile_n);
+  int rc = BCLX_OK;
+  if (tile_rows) {
+    std::vector<int32_t> maps((size_t)(out->grid_m + out->grid_n));
+    for (int64_t i = 0; i < out->grid_m; i++) maps[(size_t)i] = (int32_t)(tile_rows[i] % G);
+    for (int64_t j = 0; j < out->grid_n; j++) maps[(size_t)(out->grid_m + j)] = (int32_t)(tile_cols[j] % G);
+    rc = scratch_alloc_n(ctx, &P->rot_own, maps.size());
+    if (rc == BCLX_OK && cudaMemcpyAsync(P->rot_own, maps.data(), sizeof(int32_t) * maps.size(),
+                                         cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+      rc = BCLX_ERR_CUDA;
+    if (rc == BCLX_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = BCLX_ERR_CUDA;  // host copy
+    g.rot_i = P->rot_own;
+    g.rot_j = P->rot_own + out->grid_m;
+  }
+  if (rc == BCLX_OK)
+    rc = symbolic_impl(ctx, make_view(*a), make_view(*b), g, a->dtype, out->tile_row_ptr, out->tile_offset, P);
   if (rc != BCLX_OK) {
     P->release();
     delete P;
@@ -1778,6 +1819,18 @@ int bclx_spgemm_symbolic(bclx_context_t c, const bclx_spgrid_t* a, const bclx_sp
   *nnz = P->nnz;
   *plan = P;
   return BCLX_OK;
+}
+
+int bclx_spgemm_symbolic(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b, bclx_spgrid_out_t* out,
+                         bclx_spgemm_plan_t* plan, int64_t* nnz) {
+  return symbolic_entry(c, a, b, out, nullptr, nullptr, plan, nnz);
+}
+
+int bclx_spgemm_symbolic_sub(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b,
+                             bclx_spgrid_out_t* out, const int64_t* tile_rows, const int64_t* tile_cols,
+                             bclx_spgemm_plan_t* plan, int64_t* nnz) {
+  if (!tile_rows || !tile_cols) return BCLX_ERR_INVALID;
+  return symbolic_entry(c, a, b, out, tile_rows, tile_cols, plan, nnz);
 }
 
 int bclx_spgemm_numeric(bclx_context_t c, bclx_spgemm_plan_t P, const bclx_spgrid_t* a, const bclx_spgrid_t* b,

@@ -170,6 +170,20 @@ BCLX_API int bclx_spgemm_numeric(bclx_context_t ctx, bclx_spgemm_plan_t plan, co
                         const bclx_spgrid_t* b, bclx_spgrid_out_t* c, int32_t stage_begin,
                         int32_t stage_end);
 BCLX_API int bclx_spgemm_plan_destroy(bclx_spgemm_plan_t plan);
+/* A sub-grid of C's tiles, as one process of the reference's distributed
+ * loop computes its own C tiles (stationary C, spgemm.hpp:194-224, with
+ * tile (i, j) owned by process (j mod pn) + (i mod pm) * pn,
+ * SPMatrix.hpp:230-237): c is the grid_m x grid_n block of C tiles whose
+ * global tile rows / columns are tile_rows[0..grid_m) / tile_cols[0..grid_n)
+ * (host arrays, increasing); a holds A's tiles of those tile rows (all k),
+ * b holds B's tiles of those tile columns (all k), in that order, as
+ * descriptor arrays (a sub-grid view: no copy).  Every C tile keeps the
+ * global product's stage order k = (k_ + i + j) mod G with its global
+ * (i, j), so the sub-grid is bit-identical to those tiles of the whole
+ * product.  Then bclx_spgemm_numeric as usual. */
+BCLX_API int bclx_spgemm_symbolic_sub(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_spgrid_t* b,
+                                      bclx_spgrid_out_t* c, const int64_t* tile_rows, const int64_t* tile_cols,
+                                      bclx_spgemm_plan_t* plan, int64_t* nnz);
 /* Batched SUMMA form: the numeric pass as one launch per stage k_ (each launch
  * covers all grid_m*grid_n tile products of that stage, adding into C), in
  * order.  use_graph = 1 captures the G launches once into a CUDA graph kept
