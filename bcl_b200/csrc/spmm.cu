@@ -127,6 +127,53 @@ __device__ __forceinline__ void cp_async4_nb(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
 
+// L2 eviction policies (createpolicy): streamed data (A entries, C rows:
+// touched once) goes first; the B rows most referenced by A's columns stay.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_normal() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ void cp_async16_hint(void* smem, const void* gmem, uint64_t pol) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16_hint_nb(void* smem, const void* gmem, uint64_t pol) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "l"(pol));
+}
+__device__ __forceinline__ void cp_async4_hint_nb(void* smem, const void* gmem, uint64_t pol) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "l"(pol));
+}
+__device__ __forceinline__ uint4 ldg16_hint(const void* p, uint64_t pol) {
+  uint4 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;\n"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void stg16_hint(void* p, uint4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.u32 [%0], {%1, %2, %3, %4}, %5;\n" ::"l"(p), "r"(v.x), "r"(v.y),
+               "r"(v.z), "r"(v.w), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void l2_prefetch_last(const void* p) {
+  asm volatile("prefetch.global.L2::evict_last [%0];\n" ::"l"(p));
+}
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
 template <int N>
@@ -146,12 +193,23 @@ struct StageLane {
   const int32_t* acol;
   const float* aval;
   const ST* bt;
+  int64_t kbase;  // global index of the B tile's first row (k * tile height)
+};
+
+// B-row reuse hints: deg[global B row] = how many A entries reference it;
+// rows referenced at least thr times are kept in L2 (evict_last), the rest
+// are loaded with the normal policy, and A and C (each touched once) are
+// streamed with evict_first.  deg == null: every access uses the normal
+// policy.
+struct RowHints {
+  const int32_t* deg;
+  const int32_t* thr;  // device scalar
 };
 
 template <typename ST>
 __device__ __forceinline__ StageLane<ST> stage_lane(const SpGridView& A, const DGridView& B, int64_t ti, int64_t tj,
                                                     int64_t r, int64_t kk, bool valid) {
-  StageLane<ST> s{0, nullptr, nullptr, nullptr};
+  StageLane<ST> s{0, nullptr, nullptr, nullptr, 0};
   const int64_t gk = A.gn;
   if (valid && kk < gk) {
     const int64_t k = B.natural_order ? kk : (kk + ti + tj) % gk;
@@ -161,6 +219,7 @@ __device__ __forceinline__ StageLane<ST> stage_lane(const SpGridView& A, const D
     s.acol = At.col_ind + as;
     s.aval = reinterpret_cast<const float*>(At.vals) + as;
     s.bt = reinterpret_cast<const ST*>(B.tile(k, tj));
+    s.kbase = k * A.tn;
   }
   return s;
 }
@@ -195,7 +254,8 @@ __device__ __forceinline__ bool tiles_aligned(const DGridView& B, const DGridVie
 template <typename ST, bool GROUP, int UNROLL = kSpmmUnroll>
 __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
                                           int64_t tj, int64_t r0, int R, int c0, int W, bool vec,
-                                          const uint8_t* __restrict__ skip) {
+                                          const uint8_t* __restrict__ skip, const RowHints& hints, int32_t thr,
+                                          uint64_t pol_stream, uint64_t pol_hot, uint64_t pol_cold) {
   if (!GROUP) R = 1;
   using V = Vec<ST>;
   constexpr int VN = V::N;
@@ -220,7 +280,9 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
     if (cur < 0 || !own) return;
     ST* p = crow0 + cur * C.ld;
     if (vec) {
-      V::store(p + col, acc);
+      uint4 w;
+      V::store(reinterpret_cast<ST*>(&w), acc);
+      stg16_hint(p + col, w, pol_stream);
     } else {
 #pragma unroll
       for (int x = 0; x < VN; x++)
@@ -253,14 +315,14 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
     // stage the C slices of the rows that have entries
     if (!GROUP) {
       if (vec && !staged) {
-        if (own) cp_async16(cs + lane, crow0 + col);
+        if (own) cp_async16_hint(cs + lane, crow0 + col, pol_stream);
         staged = true;
       }
     } else {
       for (int q = 0; q < R; q++) {
         const int32_t hi = __shfl_sync(kFull, aincl, q * gk + gk - 1);
         const int32_t lo = __shfl_sync(kFull, aexcl, q * gk);
-        if (vec && own && hi > lo) cp_async16(cs + q * 32 + lane, crow0 + q * C.ld + col);
+        if (vec && own && hi > lo) cp_async16_hint(cs + q * 32 + lane, crow0 + q * C.ld + col, pol_stream);
       }
     }
     const int32_t nch = (atot + 31) >> 5;
@@ -284,8 +346,8 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
         const int slot = (x % kARing) * 32 + lane;
         asrc[slot] = (uint8_t)src;
         if (e < atot) {
-          cp_async4_nb(&ar[slot].x, sacol + off);
-          cp_async4_nb(&ar[slot].y, saval + off);
+          cp_async4_hint_nb(&ar[slot].x, sacol + off, pol_stream);
+          cp_async4_hint_nb(&ar[slot].y, saval + off, pol_stream);
         }
       }
       cp_async_commit();
@@ -298,21 +360,31 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
       const int slot = (x % kARing) * 32 + lane;
       const int src = asrc[slot];
       const ST* sbt = reinterpret_cast<const ST*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.bt), src));
+      const int64_t kb = (int64_t)__shfl_sync(kFull, (unsigned long long)sl.kbase, src);
       const int32_t e = x * 32 + lane;
       float v = 0.f;
       const ST* brow = sbt;
+      bool hot = false;
       if (e < atot) {
         const uint2 a = ar[slot];
         v = __uint_as_float(a.y);
         brow = sbt + (int64_t)(int32_t)a.x * B.ld;
+        if (hints.deg) hot = __ldg(hints.deg + kb + (int32_t)a.x) >= thr;
       }
       const ST* last = reinterpret_cast<const ST*>(
           __shfl_sync(kFull, reinterpret_cast<unsigned long long>(brow), (atot - 1) & 31));
       if (e >= atot) brow = last;
       const uint64_t pa = reinterpret_cast<uint64_t>(brow);
-      tb[(x % kTabBufs) * 32 + lane] =
-          make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), __float_as_uint(v), GROUP ? (uint32_t)(src / gk) : 0u);
-      l2_prefetch_slice(vec && e < atot ? brow + c0 : nullptr, pbytes);
+      tb[(x % kTabBufs) * 32 + lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), __float_as_uint(v),
+                                                  (GROUP ? (uint32_t)(src / gk) : 0u) | (hot ? 0x80000000u : 0u));
+      if (vec && e < atot) {
+        if (hot) {
+          const char* q = reinterpret_cast<const char*>(brow + c0);
+          for (int o = 0; o < pbytes; o += 128) l2_prefetch_last(q + o);
+        } else {
+          l2_prefetch_slice(brow + c0, pbytes);
+        }
+      }
     };
     // pipeline fill: chunks 0 .. kARing-1 staged, 0 and 1 built, kARing staged
     for (int x = 0; x < kARing; x++) issue_a(x);
@@ -337,10 +409,10 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
 #pragma unroll
           for (int u = 0; u < UNROLL; u++) {
             const ST* rp = reinterpret_cast<const ST*>((uint64_t)ent[u].x | ((uint64_t)ent[u].y << 32));
-            raw[u] = __ldg(reinterpret_cast<const uint4*>(rp + bcol));
+            raw[u] = ldg16_hint(rp + bcol, (ent[u].w & 0x80000000u) ? pol_hot : pol_cold);
           }
           auto apply = [&](int u) {
-            if (GROUP && (int)ent[u].w != cur) enter((int)ent[u].w);
+            if (GROUP && (int)(ent[u].w & 0xffu) != cur) enter((int)(ent[u].w & 0xffu));
             float b[VN];
             V::unpack_raw(raw[u], b);
             const float vs = __uint_as_float(ent[u].z);
@@ -359,7 +431,7 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
       } else {
         for (int u = 0; u < ne; u++) {
           const uint4 en = t[u];
-          if (GROUP && (int)en.w != cur) enter((int)en.w);
+          if (GROUP && (int)(en.w & 0xffu) != cur) enter((int)(en.w & 0xffu));
           const ST* rp = reinterpret_cast<const ST*>((uint64_t)en.x | ((uint64_t)en.y << 32));
           const float vs = __uint_as_float(en.z);
 #pragma unroll
@@ -377,12 +449,23 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
 // flight while the current item runs), so warps that draw short rows take
 // more of them: the cost of a (row group, panel) item varies by orders of
 // magnitude on power-law matrices.
+//
+// Launched after k_spmm_long as its programmatic dependent (the long-row
+// blocks are placed on their SMs first); before exiting, every block waits
+// for k_spmm_long to finish (griddepcontrol.wait), so later work in the
+// stream sees both kernels done.  Launched normally, the wait returns at once.
 template <typename ST, bool GROUP>
 __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int R, int64_t ngroups,
-           int row_align_ok, const uint8_t* __restrict__ long_flag, unsigned long long* __restrict__ next_item) {
+           int row_align_ok, const uint8_t* __restrict__ long_flag, unsigned long long* __restrict__ next_item,
+           RowHints hints) {
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
+  const bool hinted = hints.deg != nullptr;
+  const int32_t thr = hinted ? __ldg(hints.thr) : 0;
+  const uint64_t pol_n = policy_evict_normal();
+  const uint64_t pol_stream = hinted ? policy_evict_first() : pol_n;
+  const uint64_t pol_hot = hinted ? policy_evict_last() : pol_n;
   unsigned long long it = 0;
   if (lane == 0) it = atomicAdd(next_item, 1ULL);
   it = __shfl_sync(kFull, it, 0);
@@ -400,10 +483,12 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     if (r0 < C.rows_of(ti) && c0 < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
       // rows flagged long are k_spmm_long's (it takes the aligned ones)
-      spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr);
+      spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr, hints, thr, pol_stream,
+                           pol_hot, pol_n);
     }
     it = __shfl_sync(kFull, nx, 0);
   }
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
 }
 
 // ---- long rows ----------------------------------------------------------------
@@ -470,7 +555,9 @@ __global__ void k_spmm_find_long(SpGridView A, int long_row, int very_long_row, 
 // group two steps back.  The stages are at most 32 (one lane each).
 template <typename ST>
 __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, const DGridView& B,
-                                              const DGridView& C, int64_t ti, int64_t tj, int64_t r, int c0, int W) {
+                                              const DGridView& C, int64_t ti, int64_t tj, int64_t r, int c0, int W,
+                                              const RowHints& hints, int32_t thr, uint64_t pol_stream,
+                                              uint64_t pol_hot, uint64_t pol_cold) {
   using V = Vec<ST>;
   constexpr int VN = V::N;
   const int lane = lane_id();
@@ -502,8 +589,8 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
     const int slot = x % kLongASlots;
     S.src[slot][lane] = (uint8_t)src;
     if (e < atot) {
-      cp_async4_nb(&S.a[slot][lane].x, sacol + off);
-      cp_async4_nb(&S.a[slot][lane].y, saval + off);
+      cp_async4_hint_nb(&S.a[slot][lane].x, sacol + off, pol_stream);
+      cp_async4_hint_nb(&S.a[slot][lane].y, saval + off, pol_stream);
     }
   };
   auto build = [&](int32_t x) {  // A(x) has landed
@@ -511,11 +598,13 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
     const int slot = x % kLongASlots;
     const int src = S.src[slot][lane];
     const ST* sbt = reinterpret_cast<const ST*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.bt), src));
+    const int64_t kb = (int64_t)__shfl_sync(kFull, (unsigned long long)sl.kbase, src);
     const int32_t e = x * 32 + lane;
     if (e < atot) {
       const uint2 a = S.a[slot][lane];
       const uint64_t pa = reinterpret_cast<uint64_t>(sbt + (int64_t)(int32_t)a.x * B.ld);
-      S.tab[x % kLongTSlots][lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), a.y, 0u);
+      const bool hot = hints.deg && __ldg(hints.deg + kb + (int32_t)a.x) >= thr;
+      S.tab[x % kLongTSlots][lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), a.y, hot ? 1u : 0u);
     }
   };
   auto issue_b = [&](int32_t x) {  // table of chunk x built, then a __syncwarp
@@ -524,7 +613,7 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
     const int bslot = x % kLongBSlots, tslot = x % kLongTSlots;
     auto copy = [&](int u, const uint4& t) {
       const ST* rp = reinterpret_cast<const ST*>((uint64_t)t.x | ((uint64_t)t.y << 32));
-      cp_async16_nb(&S.b[bslot][u][lane], rp + col);
+      cp_async16_hint_nb(&S.b[bslot][u][lane], rp + col, t.w ? pol_hot : pol_cold);
     };
     if (ne == 32) {
 #pragma unroll
@@ -594,12 +683,21 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
 
 // Items (listed row, C tile column, panel), a row's items consecutive, taken
 // from a device counter in list order.
+// Every block, once placed, lets k_spmm (its programmatic dependent) launch:
+// the long-row blocks each need a whole SM's shared memory, so they take
+// their SMs before k_spmm's blocks fill the GPU.
 template <typename ST>
 __global__ void __launch_bounds__(kLongWarps * 32)
     k_spmm_long(SpGridView A, DGridView B, DGridView C, const int64_t* __restrict__ list,
                 const int32_t* __restrict__ count, int npanels, int row_align_ok,
-                unsigned long long* __restrict__ next_item) {
+                unsigned long long* __restrict__ next_item, RowHints hints) {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   extern __shared__ __align__(16) unsigned char long_smem[];
+  const bool hinted = hints.deg != nullptr;
+  const int32_t thr = hinted ? __ldg(hints.thr) : 0;
+  const uint64_t pol_n = policy_evict_normal();
+  const uint64_t pol_stream = hinted ? policy_evict_first() : pol_n;
+  const uint64_t pol_hot = hinted ? policy_evict_last() : pol_n;
   LongSmem& S = reinterpret_cast<LongSmem*>(long_smem)[threadIdx.x >> 5];
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
@@ -623,24 +721,10 @@ __global__ void __launch_bounds__(kLongWarps * 32)
     const int W = (int)C.cols_of(tj);
     if (panel * PW < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
-      if (vec) spmm_long_row<ST>(S, A, B, C, ti, tj, r, panel * PW, W);  // otherwise k_spmm did it element-wise
+      if (vec)  // otherwise k_spmm did it element-wise
+        spmm_long_row<ST>(S, A, B, C, ti, tj, r, panel * PW, W, hints, thr, pol_stream, pol_hot, pol_n);
     }
     it = __shfl_sync(kFull, nx, 0);
-  }
-}
-
-// A short pause on the main stream (bounded by the global timer and an
-// iteration cap; it waits for nothing).
-constexpr unsigned kLongHeadStartNs = 4000;
-
-__global__ void k_spmm_head_start(unsigned ns) {
-  uint64_t t0;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-  for (int i = 0; i < 4096; i++) {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    if (t - t0 >= ns) break;
-    __nanosleep(256);
   }
 }
 
@@ -673,6 +757,61 @@ static int spmm_rows_per_item(const Context* ctx, const DGridView& C, int64_t gk
   return r;
 }
 
+// ---- B-row reuse hints --------------------------------------------------------
+
+constexpr int kDegBins = 32;
+
+// deg[k * tile width + c] counts the A entries of column c of tile column k
+// (the B row each one reads).
+__global__ void k_col_degree(SpGridView A, int32_t* __restrict__ deg) {
+  const int64_t ntiles = A.gm * A.gn;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = 0; t < ntiles; t++) {
+    const bclx_csr_t At = A.tile(t / A.gn, t % A.gn);
+    int32_t* d = deg + (t % A.gn) * A.tn;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < At.nnz; e += stride)
+      atomicAdd(d + __ldg(At.col_ind + e), 1);
+  }
+}
+
+// Rows per power-of-two degree bin (bin b: degrees in [2^b, 2^(b+1))).
+__global__ void k_deg_hist(const int32_t* __restrict__ deg, int64_t n, unsigned long long* __restrict__ hist) {
+  __shared__ unsigned int h[kDegBins];
+  if (threadIdx.x < kDegBins) h[threadIdx.x] = 0;
+  __syncthreads();
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t d = __ldg(deg + c);
+    if (d > 0) atomicAdd(&h[31 - __clz(d)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < kDegBins && h[threadIdx.x]) atomicAdd(hist + threadIdx.x, (unsigned long long)h[threadIdx.x]);
+}
+
+// The degree threshold: the most referenced rows, whole bins from the top,
+// as many as fit in budget_rows, and never rows read only once.
+__global__ void k_deg_threshold(const unsigned long long* __restrict__ hist, long long budget_rows,
+                                int32_t* __restrict__ thr) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long cum = 0;
+  int b = kDegBins - 1;
+  for (; b >= 0; b--) {
+    if (cum + hist[b] > (unsigned long long)budget_rows) break;
+    cum += hist[b];
+  }
+  const long long t = b < 0 ? 1 : (1ll << (b + 1));
+  *thr = (int32_t)(t < 2 ? 2 : (t > INT32_MAX ? INT32_MAX : t));
+}
+
+// Hints pay when B does not fit in L2 (otherwise every row stays anyway).
+// BCLX_SPMM_HOT_FRACTION: the share of L2 given to the most referenced B
+// rows (default 0.5; 0 turns the hints off).
+static double spmm_hot_fraction() {
+  const char* e = std::getenv("BCLX_SPMM_HOT_FRACTION");
+  return e && *e ? std::atof(e) : 0.5;
+}
+
+// ---- launch --------------------------------------------------------------------
+
 template <typename ST>
 static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, const DGridView& C, int align_ok) {
   constexpr int VN = Vec<ST>::N;
@@ -690,50 +829,84 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   BCLX_TRY(scratch_alloc_n(ctx, &ctr, 3));
   BCLX_CK(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), ctx->stream));
   int32_t* cnt = reinterpret_cast<int32_t*>(ctr + 2);
+
+  // B-row reuse hints when B is larger than L2
+  RowHints hints{nullptr, nullptr};
+  int32_t* deg = nullptr;
+  unsigned long long* hist = nullptr;
+  {
+    int l2 = 0;
+    BCLX_CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->device));
+    const double frac = spmm_hot_fraction();
+    const int64_t row_bytes = C.n * (int64_t)sizeof(ST);
+    const int64_t b_bytes = B.m * row_bytes;
+    if (align_ok && frac > 0 && l2 > 0 && b_bytes > (int64_t)l2) {
+      const int64_t nb = A.gn * A.tn;  // global B rows, padded to whole tiles
+      BCLX_TRY(scratch_alloc_n(ctx, &deg, (size_t)nb + 1));
+      BCLX_TRY(scratch_alloc_n(ctx, &hist, kDegBins));
+      BCLX_CK(cudaMemsetAsync(deg, 0, sizeof(int32_t) * ((size_t)nb + 1), ctx->stream));
+      BCLX_CK(cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * kDegBins, ctx->stream));
+      k_col_degree<<<(unsigned)ctx->num_sms * 8, 256, 0, ctx->stream>>>(A, deg);
+      note_launch();
+      BCLX_CK_LAUNCH();
+      k_deg_hist<<<(unsigned)ctx->num_sms * 4, 256, 0, ctx->stream>>>(deg, nb, hist);
+      note_launch();
+      BCLX_CK_LAUNCH();
+      const long long budget_rows = (long long)(frac * (double)l2 / (double)row_bytes);
+      k_deg_threshold<<<1, 32, 0, ctx->stream>>>(hist, budget_rows, deg + nb);
+      note_launch();
+      BCLX_CK_LAUNCH();
+      hints.deg = deg;
+      hints.thr = deg + nb;
+    }
+  }
+
   uint8_t* flag = nullptr;
   int64_t* list = nullptr;
+  const unsigned grid = (unsigned)(want < cap ? want : cap);
   if (long_path) {
-    // On the side stream: find the long rows, then run them; k_spmm waits
-    // only for the list (an event after k_spmm_find_long), so the long-row
-    // blocks, next in their stream, are dispatched before k_spmm's blocks
-    // fill the SMs.
-    BCLX_TRY(ensure_side_stream(ctx));
+    // One stream: find the long rows, run them, and launch k_spmm as
+    // k_spmm_long's programmatic dependent, so that it starts once every
+    // long-row block has its SM (and finishes only after k_spmm_long).
     BCLX_TRY(scratch_alloc_n(ctx, &flag, (size_t)arows));
     BCLX_TRY(scratch_alloc_n(ctx, &list, (size_t)arows));
-    BCLX_CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
-    BCLX_CK(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
     k_spmm_find_long<<<(unsigned)std::min<int64_t>(ceil_div(arows, 256), (int64_t)ctx->num_sms * 16), 256, 0,
-                       ctx->side>>>(A, kSpmmLongRow, kSpmmVeryLongRow, flag, list, cnt);
+                       ctx->stream>>>(A, kSpmmLongRow, kSpmmVeryLongRow, flag, list, cnt);
     note_launch();
     BCLX_CK_LAUNCH();
-    BCLX_CK(cudaEventRecord(ctx->fork2_ev, ctx->side));
     const size_t lsmem = sizeof(LongSmem) * kLongWarps;
     BCLX_CK(cudaFuncSetAttribute(k_spmm_long<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
-    k_spmm_long<ST><<<(unsigned)spmm_long_blocks(ctx), kLongWarps * 32, lsmem, ctx->side>>>(A, B, C, list, cnt,
-                                                                                           npanels, align_ok, ctr + 1);
-    note_launch();
-    BCLX_CK_LAUNCH();
-    BCLX_CK(cudaEventRecord(ctx->join_ev, ctx->side));
-    BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->fork2_ev, 0));
-    // k_spmm starts a few microseconds after the list is ready: the long-row
-    // blocks, which need a whole SM's shared memory, are placed first
-    k_spmm_head_start<<<1, 32, 0, ctx->stream>>>(kLongHeadStartNs);
+    k_spmm_long<ST><<<(unsigned)spmm_long_blocks(ctx), kLongWarps * 32, lsmem, ctx->stream>>>(
+        A, B, C, list, cnt, npanels, align_ok, ctr + 1, hints);
     note_launch();
     BCLX_CK_LAUNCH();
   }
-  const unsigned grid = (unsigned)(want < cap ? want : cap);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kSpmmWarps * 32);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = long_path ? 1 : 0;
+  const uint8_t* lflag = flag;
   if (R > 1)
-    k_spmm<ST, true><<<grid, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, R, ngroups, align_ok, flag,
-                                                                 ctr);
+    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true>, A, B, C, n_items, npanels, R, ngroups, align_ok, lflag, ctr,
+                               hints));
   else
-    k_spmm<ST, false><<<grid, kSpmmWarps * 32, 0, ctx->stream>>>(A, B, C, n_items, npanels, 1, ngroups, align_ok, flag,
-                                                                  ctr);
+    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, false>, A, B, C, n_items, npanels, 1, ngroups, align_ok, lflag, ctr,
+                               hints));
   note_launch();
   BCLX_CK_LAUNCH();
   if (long_path) {
-    BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
     scratch_free(ctx, flag);
     scratch_free(ctx, list);
+  }
+  if (deg) {
+    scratch_free(ctx, deg);
+    scratch_free(ctx, hist);
   }
   scratch_free(ctx, ctr);
   return BCLX_OK;

@@ -72,6 +72,9 @@ def parse_args():
     p.add_argument("--path", default="fused", choices=["fused", "per_stage", "batched_graph", "learned"],
                    help="SpGEMM form timed as the step (default: all stages fused)")
     p.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
+    p.add_argument("--shard", action="store_true",
+                   help="N>1: the ranks share ONE product, each computing its block-cyclic C tiles "
+                        "(strong scaling; default: each rank runs its own product)")
     return p.parse_args()
 
 
@@ -273,7 +276,8 @@ def bench_spgemm(args, wl, dist, device):
     from bcl_b200 import _lib, gen
     from bcl_b200.containers import BlockCustom, SPMatrix, spgemm, spgemm_numeric, spgemm_symbolic
 
-    a = spgemm_matrix(wl, args.seed + dist.rank)
+    shard = bool(getattr(args, "shard", False)) and args.path == "fused"
+    a = spgemm_matrix(wl, args.seed if shard else args.seed + dist.rank)
     n = a.m
     G = wl["grid"]
     ts = -(-n // G)
@@ -294,6 +298,15 @@ def bench_spgemm(args, wl, dist, device):
     learned_st = {}
 
     def step(record=None):
+        if shard:
+            # this rank's C tiles of the one product (the reference's block-cyclic owner)
+            from bcl_b200.containers import spgemm_distributed
+            if record:
+                record[0].record(stream)
+            C, _, _ = spgemm_distributed(A, A, dist.rank, dist.world)
+            if record:
+                record[1].record(stream)
+            return (C.nnz() if C is not None else 0), None
         if args.path == "learned":
             # the learned product: prediction in place of the symbolic pass
             from bcl_b200.containers import learned_stats, spgemm_learned
@@ -355,10 +368,19 @@ def bench_spgemm(args, wl, dist, device):
     num_ms = [e[2].elapsed_time(e[3]) for e in ev]
     total_s = dist.max(sum(step_ms) / 1e3)
     ms_per_step = total_s * 1e3 / args.steps
-    value = job_rate(dist.world, flops, args.steps, total_s) / 1e9
+    if shard:  # one product per step, shared by all ranks
+        value = flops * args.steps / total_s / 1e9
+    else:
+        value = job_rate(dist.world, flops, args.steps, total_s) / 1e9
 
     c_tiles = G * G
-    alg = spgemm_alg_bytes(a_nnz, a_nnz, n, n, ts, ts, nnz_c, c_tiles)
+    if shard:
+        from bcl_b200.containers import owned_tiles, process_grid
+        rows_o, cols_o = owned_tiles(G, G, dist.rank, *process_grid(dist.world))
+        c_tiles = len(rows_o) * len(cols_o)
+        alg = spgemm_alg_bytes(a_nnz[rows_o, :], a_nnz[:, cols_o], n, n, ts, ts, nnz_c, c_tiles) if c_tiles else 0
+    else:
+        alg = spgemm_alg_bytes(a_nnz, a_nnz, n, n, ts, ts, nnz_c, c_tiles)
     hbm_peak, peak_kind = peaks()
     num_avg_s = statistics.mean(num_ms) / 1e3
     traffic = workload_traffic(args.workload, args.path)
@@ -377,7 +399,7 @@ def bench_spgemm(args, wl, dist, device):
     torch.cuda.empty_cache()
     # end to end: host CSR tiles in pinned memory -> device -> product -> host
     try:
-        e2e = bench_spgemm_e2e(args, A, stream, flops, dist)
+        e2e = bench_spgemm_e2e(args, A, stream, flops, dist, shard)
     except Exception as e:  # e.g. pinned host memory for a very large C
         e2e = {"value": None, "unit": "GFLOP/s", "error": repr(e)[:300]}
 
@@ -387,9 +409,13 @@ def bench_spgemm(args, wl, dist, device):
     cfg = {"workload": wl["desc"], "tile_grid": f"{G}x{G}", "tile": ts, "nnz_A": a.nnz, "nnz_C": nnz_c,
            "intermediate_products": products, "path": "fused SUMMA: one symbolic + one numeric launch per product",
            "l2": "flushed between steps (256 MiB write outside the timed events)",
-           "parallelism": f"independent products per GPU x{dist.world}"}
+           "parallelism": (f"one product shared by {dist.world} GPUs (block-cyclic C tiles, A replicated)"
+                           if shard else f"independent products per GPU x{dist.world}")}
+    if shard:
+        cfg["nnz_C"] = f"{nnz_c} on rank 0"
     line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": dist.world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "strong" if shard else "weak",
             "vs_baseline": None, "dtype": wl["value_type"], "data": "synthetic (seeded R-MAT)", "config": cfg,
             "hbm_gbs": alg / (total_s / args.steps) / 1e9 * dist.world,
             "roofline": roofline, "clocks": clk, "e2e": e2e, "gpu_launches": int(launches),
@@ -402,9 +428,9 @@ def bench_spgemm(args, wl, dist, device):
     return line
 
 
-def bench_spgemm_e2e(args, A, stream, flops, dist):
+def bench_spgemm_e2e(args, A, stream, flops, dist, shard=False):
     import torch
-    from bcl_b200.containers import SPMatrix, spgemm
+    from bcl_b200.containers import SPMatrix, spgemm, spgemm_distributed
 
     host = {k: getattr(A, k).cpu().pin_memory() for k in ("tile_row_ptr", "tile_offset", "col_ind", "vals")}
     dev = {k: torch.empty_like(v, device="cuda") for k, v in host.items()}
@@ -416,7 +442,9 @@ def bench_spgemm_e2e(args, A, stream, flops, dist):
             dev[k].copy_(host[k], non_blocking=True)
         Ad = SPMatrix(A.m, A.n, A.tm, A.tn, A.dtype, A.device, dev["tile_row_ptr"], dev["tile_offset"],
                       dev["col_ind"], dev["vals"])
-        C = spgemm(Ad, Ad)
+        C = spgemm_distributed(Ad, Ad, dist.rank, dist.world)[0] if shard else spgemm(Ad, Ad)
+        if C is None:
+            return 0
         nnz = C.nnz()
         d2h = 0
         for k in ("tile_row_ptr", "tile_offset", "col_ind", "vals"):
@@ -439,7 +467,8 @@ def bench_spgemm_e2e(args, A, stream, flops, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     t = dist.max(e0.elapsed_time(e1) / 1e3)
-    return {"value": job_rate(dist.world, flops, args.steps, t) / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+    rate = flops * args.steps / t if shard else job_rate(dist.world, flops, args.steps, t)
+    return {"value": rate / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3 / args.steps}
 
 
@@ -826,7 +855,8 @@ def bench_spmm_e2e(args, A, B, C, stream, flops, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     t = dist.max(e0.elapsed_time(e1) / 1e3)
-    return {"value": job_rate(dist.world, flops, args.steps, t) / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+    rate = flops * args.steps / t if shard else job_rate(dist.world, flops, args.steps, t)
+    return {"value": rate / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3 / args.steps}
 
 
