@@ -718,18 +718,10 @@ __global__ void __launch_bounds__(256)
 
 // ---- numeric ------------------------------------------------------------------------------
 
-constexpr int kHashSlots = kVcap;            // slots of the hash accumulator (one per output at most)
-constexpr unsigned short kEmptyKey = 0xffffu;  // free slot (column offsets are < kMaxCols)
-constexpr int kHashFillLimit = 448;          // hash-mode items with more outputs give up (learned: redone exactly)
-constexpr int kHashCountDefault = 256;       // light rows up to this many outputs use the hash accumulator
-
 template <typename VT, int WORDS>
 struct WarpSmem {
   uint32_t bm[WORDS];
-  union {
-    uint16_t pre[WORDS];                // rank mode: per-word exclusive prefix counts
-    unsigned short key[kHashSlots];     // hash mode: column offset (from the item's first column) per slot
-  };
+  uint16_t pre[WORDS];
   VT acc[kVcap];
   VT part[kVcap];
   unsigned char tag[kVcap];
@@ -738,61 +730,17 @@ struct WarpSmem {
   int32_t ss[32];
 };
 
-// Hash-mode slot of column offset x (from the item's first column):
-// Fibonacci hashing into kHashSlots slots, linear probing.  A free slot is
-// claimed (when `insert`) with a 16-bit compare-and-swap and the column's bit
-// is set in the item's bitmap; `fresh` tells the caller the slot was just
-// claimed (its value fields are not initialised yet).  Returns -1 when x is
-// not in the table and cannot be put there (inserting not allowed, or no free
-// slot after a full sweep).
-__device__ __forceinline__ int hash_claim(unsigned short* __restrict__ key, uint32_t* __restrict__ bm, int x,
-                                          bool insert, bool& fresh) {
-  unsigned h = ((unsigned)x * 2654435761u) >> 23;
-  fresh = false;
-  for (int probe = 0; probe < kHashSlots; probe++) {
-    const unsigned short k = key[h];
-    if (k == (unsigned short)x) return (int)h;
-    if (k == kEmptyKey) {
-      if (!insert) return -1;
-      const unsigned short old = atomicCAS(key + h, kEmptyKey, (unsigned short)x);
-      if (old == kEmptyKey) {
-        atomicOr(bm + (x >> 5), 1u << (x & 31));
-        fresh = true;
-        return (int)h;
-      }
-      if (old == (unsigned short)x) return (int)h;
-    }
-    h = (h + 1) & (kHashSlots - 1);
-  }
-  return -1;
-}
-
-// Slot of a column offset that is in the table (bounded sweep).
-__device__ __forceinline__ int hash_find(const unsigned short* __restrict__ key, int x) {
-  unsigned h = ((unsigned)x * 2654435761u) >> 23;
-  for (int probe = 1; probe < kHashSlots && key[h] != (unsigned short)x; probe++) h = (h + 1) & (kHashSlots - 1);
-  return (int)h;
-}
-
 #ifndef BCLX_NUMERIC_MIN_BLOCKS
 #define BCLX_NUMERIC_MIN_BLOCKS 4
 #endif
-// Two accumulator modes per item (warp-uniform choice):
-//  * rank mode: the item's column bitmap is complete before the product walk
-//    (loaded from the symbolic pass for heavy items, rebuilt by an order-free
-//    walk for light rows); column j's value lives at its output rank.
-//  * hash mode (one product walk): values live in a hash table keyed by
-//    column, and the bitmap is built as columns are first seen; at the end
-//    the bitmap gives every column's rank and the entries are written in
-//    column order.  Used for light rows of at most `hash_count` outputs when
-//    the launch covers every stage, and for every item of the learned pass.
 // LEARNED: the learned product's single pass.  Heavy items come from the
-// predicted cut (their counts are unknown); an item with more outputs than
-// its temp slots (or than the hash table takes) marks its row in row_failed
-// and stops (that row is redone by the exact path).  Outputs go to temp
-// slots (light row l at light_slot[l], heavy item idx at heavy_slot_base +
-// item_off[idx], after all light slots; an item's slot count, at most kVcap,
-// comes from the prediction), counts to item_count / row_count_w.
+// predicted cut (their counts are unknown): each builds its bitmap from its
+// own products, and an item with more than kVcap outputs marks its row in
+// row_failed and stops (that row is redone by the exact path).  Outputs go
+// to temp slots (light row l at light_slot[l], heavy item idx at
+// heavy_slot_base + item_off[idx], after all light slots; an item's slot
+// count, at most kVcap, comes from the prediction),
+// counts to item_count / row_count_w.
 template <typename VT, int WORDS, bool LEARNED>
 __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     k_numeric(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
@@ -801,7 +749,7 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
               const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, const int32_t* __restrict__ tab,
               const int32_t* __restrict__ row_count, const int64_t* __restrict__ row_offset,
               int32_t* __restrict__ out_col, VT* __restrict__ out_val, int s0, int s1,
-              unsigned long long* __restrict__ queue, int grab, int long_seg, int hash_count,
+              unsigned long long* __restrict__ queue, int grab, int long_seg,
               const int64_t* __restrict__ light_slot, int32_t* __restrict__ item_count,
               int32_t* __restrict__ row_count_w, int32_t* __restrict__ row_failed, int64_t heavy_slot_base,
               const int64_t* __restrict__ item_off) {
@@ -809,7 +757,6 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
   WarpSmem<VT, WORDS>& S = reinterpret_cast<WarpSmem<VT, WORDS>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = lane_id();
   const int64_t n_total = n_heavy_items + n_light;
-  const bool all_stages = s0 == 0 && s1 >= g.gk;
   // persistent warps: take `grab` consecutive items at a time from the queue
   int64_t next = 0, stop = 0;
   for (;;) {
@@ -860,157 +807,16 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     }
     const int w0 = lo >> 5;
     const int words = ((hi - lo) + 31) >> 5;
-    const bool hmode = LEARNED || (!heavy && all_stages && cnt <= hash_count);
 
-    if (hmode) {
-      // ---- hash mode: one walk over the products ----
-      {
-        uint4* k4 = reinterpret_cast<uint4*>(S.key);
-        const uint4 e4 = make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
-        for (int q = lane; q < kHashSlots * 2 / 16; q += 32) k4[q] = e4;
-        for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
-      }
-      __syncwarp();
-      // keys this lane has seen inserted (a lower bound of the table's
-      // fill; new keys are taken while it is below kHashFillLimit), and
-      // whether a product found no slot (the item cannot be finished here)
-      int n_ins = 0;
-      bool dropped = false;
-      auto update = [&](bool valid, int32_t j, VT a, VT b, int stage) {
-        const unsigned peers = __match_any_sync(kFull, valid ? j : -1);
-        const bool single = peers == (1u << lane);
-        if (__any_sync(kFull, valid && !single)) {
-          S.sa[lane] = a;
-          S.sb[lane] = b;
-          S.ss[lane] = stage;
-          __syncwarp();
-        }
-        const bool lead = valid && lane == __ffs(peers) - 1;
-        bool fresh = false;
-        int slot = -1;
-        if (lead) {
-          slot = hash_claim(S.key, S.bm, j - lo, n_ins < kHashFillLimit, fresh);
-          dropped |= slot < 0;
-        }
-        n_ins += __popc(__ballot_sync(kFull, fresh));
-        if (slot >= 0) {
-          VT v = VT(0), ac = VT(0);
-          int t = kNoStage;
-          if (!fresh) {
-            v = S.part[slot];
-            t = S.tag[slot];
-            ac = S.acc[slot];
-          }
-          if (single) {
-            if (t != stage) {
-              if (t != kNoStage) ac = vadd(ac, v);
-              v = VT(0);
-              t = stage;
-            }
-            v = madd(a, b, v);
-          } else {
-            unsigned gmask = peers;
-            do {
-              const int mb = __ffs(gmask) - 1;
-              gmask &= gmask - 1;
-              const int st = S.ss[mb];
-              if (st != t) {
-                if (t != kNoStage) ac = vadd(ac, v);
-                v = VT(0);
-                t = st;
-              }
-              v = madd(S.sa[mb], S.sb[mb], v);
-            } while (gmask);
-          }
-          S.part[slot] = v;
-          S.tag[slot] = (unsigned char)t;
-          S.acc[slot] = ac;
-        }
-        __syncwarp();
-      };
-      auto update_direct = [&](int32_t j, VT a, VT b, int stage) {
-        bool fresh = false;
-        const int slot = hash_claim(S.key, S.bm, j - lo, n_ins < kHashFillLimit, fresh);
-        dropped |= slot < 0;
-        n_ins += fresh ? 1 : 0;
-        if (slot >= 0) {
-          VT v = VT(0), ac = VT(0);
-          int t = kNoStage;
-          if (!fresh) {
-            v = S.part[slot];
-            t = S.tag[slot];
-            ac = S.acc[slot];
-          }
-          if (t != stage) {
-            if (t != kNoStage) ac = vadd(ac, v);
-            v = VT(0);
-            t = stage;
-          }
-          S.part[slot] = madd(a, b, v);
-          S.tag[slot] = (unsigned char)t;
-          S.acc[slot] = ac;
-        }
-      };
-      if (heavy)
-        walk_products<VT, true>(A, B, g, x, s0, s1, fb_lo, fb_hi, tab, long_seg, update, update_direct);
-      else
-        walk_products<VT, false>(A, B, g, x, s0, s1, 0, 0, nullptr, long_seg, update, update_direct);
-      __syncwarp();
-      // ranks from the bitmap (contiguous words per lane)
-      const int per = (words + 31) >> 5;
-      const int wa = lane * per;
-      const int wb = min(wa + per, words);
-      int loc = 0;
-      for (int w = wa; w < wb; w++) loc += __popc(S.bm[w]);
-      const int inc = warp_inclusive_scan(loc);
-      int pos = inc - loc;
-      if (LEARNED) {
-        // a dropped column or more outputs than temp slots: the row is redone
-        // by the exact path (light rows have at most kHashFillLimit products
-        // and always fit)
-        const int c = __shfl_sync(kFull, inc, 31);
-        if (__any_sync(kFull, dropped) || c > icap) {
-          if (lane == 0 && heavy) row_failed[hslot] = 1;
-          __syncwarp();
-          continue;
-        }
-        if (lane == 0) {
-          if (heavy) {
-            item_count[idx] = c;
-            atomicAdd(&row_count_w[ri], c);
-          } else {
-            row_count_w[ri] = c;
-          }
-        }
-      }
-      // last fold
-      for (int q = lane; q < kHashSlots; q += 32) {
-        if (S.key[q] != kEmptyKey) {
-          VT v = S.acc[q];
-          if (S.tag[q] != kNoStage) v = vadd(v, S.part[q]);
-          S.acc[q] = v;
-        }
-      }
-      __syncwarp();
-      // entries in column order
-      for (int w = wa; w < wb; w++) {
-        uint32_t bits = S.bm[w];
-        while (bits) {
-          const int bpos = __ffs(bits) - 1;
-          bits &= bits - 1;
-          const int xx = w * 32 + bpos;
-          out_col[off + pos] = lo + xx;
-          out_val[off + pos] = S.acc[hash_find(S.key, xx)];
-          pos++;
-        }
-      }
-      __syncwarp();
-      continue;
-    }
-
-    // ---- rank mode ----
     // 1. column bitmap of the item (word w covers columns lo + 32w ..)
-    if (heavy) {
+    if (heavy && LEARNED) {
+      for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
+      __syncwarp();
+      walk_columns_ranged(A, B, g, x, fb_lo, fb_hi, tab, [&](int32_t j) {
+        const int xx = j - lo;
+        atomicOr(&S.bm[xx >> 5], 1u << (xx & 31));
+      });
+    } else if (heavy) {
       for (int w = lane; w < words; w += 32) S.bm[w] = __ldg(hb + w0 + w);
     } else {
       for (int w = lane; w < words; w += 32) S.bm[w] = 0u;
@@ -1038,8 +844,23 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
         S.pre[w] = (uint16_t)ex;
         ex += __popc(S.bm[w]);
       }
+      if (LEARNED) cnt = __shfl_sync(kFull, inc, 31);
     }
     __syncwarp();
+    if (LEARNED) {
+      if (heavy && cnt > icap) {  // the prediction cut this item too wide, or sized it too small
+        if (lane == 0) row_failed[hslot] = 1;
+        continue;
+      }
+      if (lane == 0) {
+        if (heavy) {
+          item_count[idx] = cnt;
+          atomicAdd(&row_count_w[ri], cnt);
+        } else {
+          row_count_w[ri] = cnt;
+        }
+      }
+    }
 
     // 3. sorted columns (first stage range only) and the accumulators
     if (s0 == 0) {
@@ -1364,15 +1185,6 @@ __global__ void k_fill_desc(bclx_csr_t* __restrict__ d, int n, bclx_csr_t v) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = v;
 }
 
-// Light rows with at most this many outputs use the hash accumulator
-// (BCLX_HASH_COUNT overrides the default; 0 turns the hash mode off).
-static int default_hash_count() {
-  const char* e = std::getenv("BCLX_HASH_COUNT");
-  if (!e || !*e) return kHashCountDefault;
-  const long v = std::strtol(e, nullptr, 10);
-  return v < 0 ? 0 : (v > kHashFillLimit ? kHashFillLimit : (int)v);
-}
-
 }  // namespace bclx
 
 using namespace bclx;
@@ -1402,7 +1214,6 @@ struct bclx_spgemm_plan_s {
   unsigned long long* queue = nullptr;  // work-queue heads, one per stage launch
   // numeric tuning (bclx_spgemm_plan_tune)
   int grab = 1, blocks_per_sm = 4, long_seg = kLongSegDefault;
-  int hash_count = default_hash_count();  // light rows with at most this many outputs use the hash accumulator
   int light_ub_max = kLightUb;         // light-row class bound (products), set at symbolic time
   // CUDA graph of the staged numeric pass (bclx_spgemm_numeric_staged)
   cudaGraphExec_t graph = nullptr;
@@ -1570,9 +1381,7 @@ static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView&
   kern<<<grid_for(ctx, n_total, kWarpsNum, bps), kWarpsNum * 32, smem, ctx->stream>>>(
       A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, P->n_heavy_items, P->heavy_items, P->heavy_bitmaps,
       P->hbm_words, P->tab, P->row_count, P->row_offset, out_col, reinterpret_cast<VT*>(out_val), s0, s1, q,
-      P->grab < 1 ? 1 : P->grab, P->long_seg < 1 ? 1 : P->long_seg,
-      P->hash_count < 0 ? 0 : (P->hash_count > kHashFillLimit ? kHashFillLimit : P->hash_count),
-      LEARNED ? P->light_slot : nullptr,
+      P->grab < 1 ? 1 : P->grab, P->long_seg < 1 ? 1 : P->long_seg, LEARNED ? P->light_slot : nullptr,
       LEARNED ? P->item_count : nullptr, LEARNED ? P->row_count : nullptr, LEARNED ? P->row_failed : nullptr,
       P->heavy_slot_base, LEARNED ? P->item_off : nullptr);
   note_launch();
@@ -2287,7 +2096,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   if (nri > 0) {
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
-        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, 8192 + 1, kHashFillLimit, P->feat, P->ub,
+        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, 8192 + 1, kLightUb, P->feat, P->ub,
         P->queue + 1);
     note_launch();
     BCLX_CK_LAUNCH();

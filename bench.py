@@ -567,6 +567,7 @@ def cusparse_spmm_leg(a, b_dev, ours_s, c_ours, stream, reps=5):
     same A and B; reports its time, our time ratio, and the relative
     Frobenius difference between its C and ours."""
     out = {}
+    import torch  # noqa: F401  (the CSR tensor and the product)
     try:
         M = torch_csr(a, b_dev.dtype)
         C = M @ b_dev
