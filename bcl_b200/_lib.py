@@ -81,6 +81,8 @@ SIGNATURES = {
     "bclx_spgemm_learned_run": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut), vp,
                                 ctypes.POINTER(vp), ctypes.POINTER(i64)],
     "bclx_spgemm_learned_finish": [vp, vp, ctypes.POINTER(SpGridOut)],
+    "bclx_spgemm_learned_run_sub": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut), vp,
+                                    vp, vp, ctypes.POINTER(vp), ctypes.POINTER(i64)],
     "bclx_spgemm_learned_stats": [vp, ctypes.POINTER(i64)],
     "bclx_spgemm_row_features": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(SpGrid), ctypes.POINTER(SpGridOut), vp,
                                  vp],

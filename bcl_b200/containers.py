@@ -655,14 +655,19 @@ def _sub_spgrid(x: SPMatrix, rows, cols):
     return SpGrid(m, n, x.tm, x.tn, len(rows), len(cols), desc.data_ptr(), _NP_TO_DT[x.dtype], 0), desc
 
 
-def spgemm_sub(a: SPMatrix, b: SPMatrix, tile_rows, tile_cols) -> SPMatrix:
+def spgemm_sub(a: SPMatrix, b: SPMatrix, tile_rows, tile_cols, form: str = "fused", predictor="default",
+               keep_plan: bool = False):
     """The C tiles (i, j), i in tile_rows, j in tile_cols (increasing global
     tile indices), of C = A * B, bit-identical to those tiles of the whole
     product (each keeps its stage order k = (k_ + i + j) mod G): what one
     process of the reference's stationary-C loop computes
-    (spgemm.hpp:194-224).  The result is an SPMatrix of those tiles in
-    sub-grid order (bclx_spgemm_symbolic_sub)."""
+    (spgemm.hpp:194-224), or one block of a product computed block by block.
+    The result is an SPMatrix of those tiles in sub-grid order
+    (bclx_spgemm_symbolic_sub, or bclx_spgemm_learned_run_sub with
+    form="learned")."""
     _check_grids(a, b)
+    if form == "learned":
+        return _spgemm_learned_sub(a, b, tile_rows, tile_cols, predictor, keep_plan)
     tile_rows, tile_cols = list(tile_rows), list(tile_cols)
     if any(q <= p for p, q in zip(tile_rows, tile_rows[1:])) or any(q <= p for p, q in zip(tile_cols, tile_cols[1:])):
         raise ValueError("tile rows and columns must be increasing")
@@ -689,6 +694,51 @@ def spgemm_sub(a: SPMatrix, b: SPMatrix, tile_rows, tile_cols) -> SPMatrix:
     pl.close()
     del adesc, bdesc  # (the numeric pass is ordered on the stream before any reuse)
     return SPMatrix(ag.m, bg.n, a.tm, b.tn, a.dtype, a.device, trp, toff, ci, v)
+
+
+def _spgemm_learned_sub(a, b, tile_rows, tile_cols, predictor, keep_plan):
+    if predictor == "default":
+        from . import learned
+        predictor = learned.get_default()
+    tile_rows, tile_cols = list(tile_rows), list(tile_cols)
+    h = context(a.device).use_current_stream()
+    ag, adesc = _sub_spgrid(a, tile_rows, range(a.gn))
+    bg, bdesc = _sub_spgrid(b, range(b.gm), tile_cols)
+    td = a.tile_row_ptr.device
+    gm, gn = len(tile_rows), len(tile_cols)
+    trp = torch.empty((gm * gn, a.tm + 1), dtype=torch.int32, device=td)
+    toff = torch.empty(gm * gn + 1, dtype=torch.int64, device=td)
+    out = SpGridOut(ag.m, bg.n, a.tm, b.tn, gm, gn, trp.data_ptr(), toff.data_ptr(), None, None,
+                    _NP_TO_DT[a.dtype], 0)
+    rows_arr = (ctypes.c_int64 * max(gm, 1))(*tile_rows)
+    cols_arr = (ctypes.c_int64 * max(gn, 1))(*tile_cols)
+    prm = ctypes.c_void_p(predictor.params.data_ptr()) if predictor is not None else None
+    plan = ctypes.c_void_p()
+    nnz = ctypes.c_int64()
+    call("bclx_spgemm_learned_run_sub", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), rows_arr,
+         cols_arr, prm, ctypes.byref(plan), ctypes.byref(nnz))
+    pl = SpgemmPlan(plan)
+    k = int(nnz.value)
+    ci = torch.empty(max(k, 1), dtype=torch.int32, device=td)
+    v = torch.empty(max(k, 1), dtype=_TORCH_OF[_NP_TO_DT[a.dtype]], device=td)
+    out.col_ind, out.vals = ci.data_ptr(), v.data_ptr()
+    call("bclx_spgemm_learned_finish", h, pl.h, ctypes.byref(out))
+    del adesc, bdesc
+    c = SPMatrix(ag.m, bg.n, a.tm, b.tn, a.dtype, a.device, trp, toff, ci, v)
+    if keep_plan:
+        return c, pl
+    pl.close()
+    return c
+
+
+def spgemm_blocks(a: SPMatrix, b: SPMatrix, block_rows: int, form: str = "fused", predictor="default"):
+    """C = A * B computed one block of `block_rows` C tile rows at a time
+    (for products whose working space does not fit beside the whole C):
+    yields (tile rows, SPMatrix of that block's tiles).  The blocks together
+    are the whole product, bit for bit."""
+    for i0 in range(0, a.gm, block_rows):
+        rows = list(range(i0, min(i0 + block_rows, a.gm)))
+        yield rows, spgemm_sub(a, b, rows, range(b.gn), form=form, predictor=predictor)
 
 
 def spgemm_distributed(a: SPMatrix, b: SPMatrix, rank: int, world: int, pgrid=None):

@@ -1583,6 +1583,31 @@ static Geom make_geom(const bclx_spgrid_out_t* c, int64_t gk, int64_t tk) {
 
 extern "C" {
 
+// Sub-grid tile maps: global tile indices increasing (so only the last may
+// be a ragged edge tile) and in range.
+static bool maps_ok(const bclx_spgrid_out_t* out, const int64_t* tile_rows, const int64_t* tile_cols) {
+  for (int64_t i = 0; i < out->grid_m; i++)
+    if (tile_rows[i] < 0 || tile_rows[i] >= INT32_MAX || (i > 0 && tile_rows[i] <= tile_rows[i - 1])) return false;
+  for (int64_t j = 0; j < out->grid_n; j++)
+    if (tile_cols[j] < 0 || tile_cols[j] >= INT32_MAX || (j > 0 && tile_cols[j] <= tile_cols[j - 1])) return false;
+  return true;
+}
+
+// Device copies of the maps (owned by the plan) into g.rot_i / g.rot_j.
+static int attach_maps(Context* ctx, bclx_spgemm_plan_s* P, Geom& g, const bclx_spgrid_out_t* out,
+                       const int64_t* tile_rows, const int64_t* tile_cols) {
+  std::vector<int32_t> maps((size_t)(out->grid_m + out->grid_n));
+  for (int64_t i = 0; i < out->grid_m; i++) maps[(size_t)i] = (int32_t)(tile_rows[i] % g.gk);
+  for (int64_t j = 0; j < out->grid_n; j++) maps[(size_t)(out->grid_m + j)] = (int32_t)(tile_cols[j] % g.gk);
+  BCLX_TRY(scratch_alloc_n(ctx, &P->rot_own, maps.size()));
+  BCLX_CK(cudaMemcpyAsync(P->rot_own, maps.data(), sizeof(int32_t) * maps.size(), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  BCLX_CK(cudaStreamSynchronize(ctx->stream));  // the host vector goes out of scope
+  g.rot_i = P->rot_own;
+  g.rot_j = P->rot_own + out->grid_m;
+  return BCLX_OK;
+}
+
 static int symbolic_entry(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b, bclx_spgrid_out_t* out,
                           const int64_t* tile_rows, const int64_t* tile_cols, bclx_spgemm_plan_t* plan,
                           int64_t* nnz) {
@@ -1591,33 +1616,12 @@ static int symbolic_entry(bclx_context_t c, const bclx_spgrid_t* a, const bclx_s
   *plan = nullptr;
   BCLX_TRY(check_grids(a, b, out));
   if (!out->tile_row_ptr || !out->tile_offset) return BCLX_ERR_INVALID;
-  const int64_t G = a->grid_n;
-  if (tile_rows) {
-    // global tile indices: increasing (so only the last may be a ragged edge tile) and in range
-    for (int64_t i = 0; i < out->grid_m; i++)
-      if (tile_rows[i] < 0 || tile_rows[i] >= INT32_MAX || (i > 0 && tile_rows[i] <= tile_rows[i - 1]))
-        return BCLX_ERR_INVALID;
-    for (int64_t j = 0; j < out->grid_n; j++)
-      if (tile_cols[j] < 0 || tile_cols[j] >= INT32_MAX || (j > 0 && tile_cols[j] <= tile_cols[j - 1]))
-        return BCLX_ERR_INVALID;
-  }
+  if (tile_rows && !maps_ok(out, tile_rows, tile_cols)) return BCLX_ERR_INVALID;
   BCLX_CK(cudaSetDevice(ctx->device));
   auto* P = new bclx_spgemm_plan_s();
   P->ctx = ctx;
-  Geom g = make_geom(out, G, a->tile_n);
-  int rc = BCLX_OK;
-  if (tile_rows) {
-    std::vector<int32_t> maps((size_t)(out->grid_m + out->grid_n));
-    for (int64_t i = 0; i < out->grid_m; i++) maps[(size_t)i] = (int32_t)(tile_rows[i] % G);
-    for (int64_t j = 0; j < out->grid_n; j++) maps[(size_t)(out->grid_m + j)] = (int32_t)(tile_cols[j] % G);
-    rc = scratch_alloc_n(ctx, &P->rot_own, maps.size());
-    if (rc == BCLX_OK && cudaMemcpyAsync(P->rot_own, maps.data(), sizeof(int32_t) * maps.size(),
-                                         cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
-      rc = BCLX_ERR_CUDA;
-    if (rc == BCLX_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = BCLX_ERR_CUDA;  // host copy
-    g.rot_i = P->rot_own;
-    g.rot_j = P->rot_own + out->grid_m;
-  }
+  Geom g = make_geom(out, a->grid_n, a->tile_n);
+  int rc = tile_rows ? attach_maps(ctx, P, g, out, tile_rows, tile_cols) : BCLX_OK;
   if (rc == BCLX_OK)
     rc = symbolic_impl(ctx, make_view(*a), make_view(*b), g, a->dtype, out->tile_row_ptr, out->tile_offset, P);
   if (rc != BCLX_OK) {
@@ -2076,6 +2080,10 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   BCLX_TRY(build_stage_map(ctx, A, B, P, g));
   P->g = g;
   P->dtype = dtype;
+  // The B-row table depends on B alone: built on the side stream from the
+  // start, beside classification and the prediction.
+  BCLX_TRY(ensure_side_stream(ctx));
+  BCLX_TRY(build_btable(ctx, B, g, P, ctx->side));
   P->hbm_words = (g.tn + 31) / 32;
   const int64_t nri = g.n_row_items;
   BCLX_TRY(scratch_alloc_n(ctx, &P->light_list, nri));
@@ -2140,8 +2148,10 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   BCLX_TRY(scratch_alloc_n(ctx, &P->light_ub, P->n_light));
   BCLX_TRY(scratch_alloc_n(ctx, &P->light_slot, P->n_light + 1));
   const unsigned hb = grid_for(ctx, P->n_heavy / 32 + 1, 8, 8);
+  // the side stream (B-row table) joins before the table is read
+  BCLX_CK(cudaEventRecord(ctx->join_ev, ctx->side));
+  BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
   if (P->n_heavy > 0) {
-    BCLX_TRY(build_btable(ctx, B, g, P));
     BCLX_TRY(scratch_alloc_n(ctx, &P->block_ub, (size_t)P->n_heavy * g.nfb));
     k_heavy_block_ub<<<grid_for(ctx, P->n_heavy, 8, 16), 256, 0, ctx->stream>>>(A, B, g, P->heavy_list,
                                                                                (int)P->n_heavy, P->tab, P->block_ub);
@@ -2308,18 +2318,23 @@ static int learned_finish_impl(Context* ctx, bclx_spgemm_plan_s* P, int32_t* out
 
 extern "C" {
 
-int bclx_spgemm_learned_run(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b, bclx_spgrid_out_t* out,
-                            const float* mlp_params, bclx_spgemm_plan_t* plan, int64_t* nnz) {
+static int learned_entry(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b, bclx_spgrid_out_t* out,
+                         const int64_t* tile_rows, const int64_t* tile_cols, const float* mlp_params,
+                         bclx_spgemm_plan_t* plan, int64_t* nnz) {
   Context* ctx = reinterpret_cast<Context*>(c);
   if (!ctx || !plan || !nnz) return BCLX_ERR_INVALID;
   *plan = nullptr;
   BCLX_TRY(check_grids(a, b, out));
   if (!out->tile_row_ptr || !out->tile_offset) return BCLX_ERR_INVALID;
+  if (tile_rows && !maps_ok(out, tile_rows, tile_cols)) return BCLX_ERR_INVALID;
   BCLX_CK(cudaSetDevice(ctx->device));
   auto* P = new bclx_spgemm_plan_s();
   P->ctx = ctx;
-  int rc = learned_impl(ctx, make_view(*a), make_view(*b), make_geom(out, a->grid_n, a->tile_n), a->dtype, mlp_params,
-                        out->tile_row_ptr, out->tile_offset, P);
+  Geom g = make_geom(out, a->grid_n, a->tile_n);
+  int rc = tile_rows ? attach_maps(ctx, P, g, out, tile_rows, tile_cols) : BCLX_OK;
+  if (rc == BCLX_OK)
+    rc = learned_impl(ctx, make_view(*a), make_view(*b), g, a->dtype, mlp_params, out->tile_row_ptr,
+                      out->tile_offset, P);
   if (rc != BCLX_OK) {
     P->release();
     delete P;
@@ -2328,6 +2343,18 @@ int bclx_spgemm_learned_run(bclx_context_t c, const bclx_spgrid_t* a, const bclx
   *nnz = P->nnz;
   *plan = P;
   return BCLX_OK;
+}
+
+int bclx_spgemm_learned_run(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b, bclx_spgrid_out_t* out,
+                            const float* mlp_params, bclx_spgemm_plan_t* plan, int64_t* nnz) {
+  return learned_entry(c, a, b, out, nullptr, nullptr, mlp_params, plan, nnz);
+}
+
+int bclx_spgemm_learned_run_sub(bclx_context_t c, const bclx_spgrid_t* a, const bclx_spgrid_t* b,
+                                bclx_spgrid_out_t* out, const int64_t* tile_rows, const int64_t* tile_cols,
+                                const float* mlp_params, bclx_spgemm_plan_t* plan, int64_t* nnz) {
+  if (!tile_rows || !tile_cols) return BCLX_ERR_INVALID;
+  return learned_entry(c, a, b, out, tile_rows, tile_cols, mlp_params, plan, nnz);
 }
 
 int bclx_spgemm_learned_finish(bclx_context_t c, bclx_spgemm_plan_t P, bclx_spgrid_out_t* out) {

@@ -223,6 +223,14 @@ BCLX_API int bclx_spgemm_learned_run(bclx_context_t ctx, const bclx_spgrid_t* a,
                                      bclx_spgrid_out_t* c, const float* mlp_params, bclx_spgemm_plan_t* plan,
                                      int64_t* nnz);
 BCLX_API int bclx_spgemm_learned_finish(bclx_context_t ctx, bclx_spgemm_plan_t plan, bclx_spgrid_out_t* c);
+/* The learned product of a sub-grid of C's tiles (tile_rows / tile_cols as
+ * in bclx_spgemm_symbolic_sub): a process's own C tiles, or one block of C
+ * tile rows of a product whose temporary slots would not fit beside the
+ * whole C (the blocks are computed and kept one after another).  Then
+ * bclx_spgemm_learned_finish. */
+BCLX_API int bclx_spgemm_learned_run_sub(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_spgrid_t* b,
+                                         bclx_spgrid_out_t* c, const int64_t* tile_rows, const int64_t* tile_cols,
+                                         const float* mlp_params, bclx_spgemm_plan_t* plan, int64_t* nnz);
 /* [0] heavy rows, [1] predicted heavy items, [2] rows redone exactly
  * (mispredictions), [3] temp entries allocated, [4] nnz, [5] redo items. */
 BCLX_API int bclx_spgemm_learned_stats(bclx_spgemm_plan_t plan, int64_t* out6);

@@ -59,3 +59,21 @@ def test_sub_grids_ragged_and_fine_grid():
         whole = assemble_tiles(a.m, a.n, ts, ts, sub_parts(A, 4))
         rp, ci, cv = O.gemm_tiled(a, a, ts, ts, ts)
         assert_csr_identical(whole, rp, ci, cv)
+
+
+@pytest.mark.parametrize("form", ["fused", "learned"])
+def test_blocked_product_matches_whole(form):
+    """A product computed one block of C tile rows at a time (fused and
+    learned forms) equals the whole product bit for bit."""
+    from bcl_b200.containers import BlockCustom, SPMatrix, assemble_tiles, spgemm_blocks
+    a = gen.rmat(12, seed=73)
+    ts = 512
+    A = SPMatrix.from_csr(a, BlockCustom((ts, ts)))
+    parts = []
+    for rows, C in spgemm_blocks(A, A, 3, form=form):
+        n = C.nnz()
+        parts.append((rows, list(range(A.gn)), C.tile_row_ptr.cpu().numpy(), C.tile_offset.cpu().numpy(),
+                      C.col_ind[:n].cpu().numpy(), C.vals[:n].cpu().numpy()))
+    whole = assemble_tiles(a.m, a.n, ts, ts, parts)
+    rp, ci, cv = O.gemm_tiled(a, a, ts, ts, ts)
+    assert_csr_identical(whole, rp, ci, cv)
