@@ -13,6 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbclx.so")
 
 # status codes (bclx_status_t)
+(TUNE_LIGHT_UB, TUNE_LEARN_TARGET, TUNE_BTABLE_MAX_BYTES, TUNE_SPMM_ROWS, TUNE_SPMM_LONG_ROW,
+ TUNE_SPMM_LONG_BLOCKS, TUNE_SPMM_HOT_PERMILLE) = range(7)
 OK, ERR_INVALID, ERR_DTYPE, ERR_CUDA, ERR_NO_MEMORY, ERR_INDEX_OVERFLOW, ERR_DEVICE_TIMEOUT, ERR_NO_DEVICE = range(8)
 STATUS_NAMES = {
     OK: "BCLX_OK", ERR_INVALID: "BCLX_ERR_INVALID", ERR_DTYPE: "BCLX_ERR_DTYPE", ERR_CUDA: "BCLX_ERR_CUDA",
@@ -60,6 +62,8 @@ SIGNATURES = {
     "bclx_context_set_stream": [vp, vp],
     "bclx_context_synchronize": [vp],
     "bclx_context_release_cached": [vp],
+    "bclx_context_set_tuning": [vp, i32, i64],
+    "bclx_context_get_tuning": [vp, i32, ctypes.POINTER(i64)],
     "bclx_last_error": [],
     "bclx_version": [],
     "bclx_launch_count": [],

@@ -64,6 +64,35 @@ class Context:
         """Return the scratch pool's cached device memory to the driver."""
         call("bclx_context_release_cached", self.use_current_stream())
 
+    TUNING_KEYS = {"light_ub": _lib.TUNE_LIGHT_UB, "learn_target": _lib.TUNE_LEARN_TARGET,
+                   "btable_max_bytes": _lib.TUNE_BTABLE_MAX_BYTES, "spmm_rows": _lib.TUNE_SPMM_ROWS,
+                   "spmm_long_row": _lib.TUNE_SPMM_LONG_ROW, "spmm_long_blocks": _lib.TUNE_SPMM_LONG_BLOCKS,
+                   "spmm_hot_permille": _lib.TUNE_SPMM_HOT_PERMILLE}
+
+    def set_tuning(self, **knobs) -> None:
+        """bclx_context_set_tuning for each name=value (None: the default)."""
+        for k, v in knobs.items():
+            call("bclx_context_set_tuning", self.h, self.TUNING_KEYS[k], -1 if v is None else int(v))
+
+    def get_tuning(self, name: str) -> int:
+        v = ctypes.c_int64()
+        call("bclx_context_get_tuning", self.h, self.TUNING_KEYS[name], ctypes.byref(v))
+        return int(v.value)
+
+    def tuned(self, **knobs):
+        """Context manager: the knobs set inside the block, the previous values after."""
+        import contextlib
+
+        @contextlib.contextmanager
+        def cm():
+            old = {k: self.get_tuning(k) for k in knobs}
+            self.set_tuning(**knobs)
+            try:
+                yield self
+            finally:
+                self.set_tuning(**old)
+        return cm()
+
     def __del__(self):
         try:
             if getattr(self, "h", None):
@@ -603,13 +632,23 @@ def spgemm(a: SPMatrix, b: SPMatrix, stages: str = "fused", keep_plan: bool = Fa
     (all G*G tile products of that stage), adding into C between them;
     ``"batched_graph"`` does the same through a CUDA graph kept by the plan.
     All forms are bit-identical.  ``tuning`` = (grab, blocks_per_sm,
-    long_seg), or "auto" for the autotuner's cached choice."""
-    plan, out, trp, toff, nnz = spgemm_symbolic(a, b)
+    long_seg), a dict of those and "light_ub", or "auto" for the autotuner's
+    cached choice."""
+    params = None
     if tuning == "auto":
         from . import autotune
-        tuning = autotune.lookup(a, b, plan)
-    if tuning:
-        plan.tune(*tuning)
+        params = autotune.lookup(a, b)
+    elif isinstance(tuning, dict):
+        params = tuning
+    elif tuning:
+        params = dict(zip(("grab", "blocks_per_sm", "long_seg"), tuning))
+    if params and "light_ub" in params:
+        with context(a.device).tuned(light_ub=params["light_ub"]):
+            plan, out, trp, toff, nnz = spgemm_symbolic(a, b)
+    else:
+        plan, out, trp, toff, nnz = spgemm_symbolic(a, b)
+    if params:
+        plan.tune(params.get("grab", 1), params.get("blocks_per_sm", 4), params.get("long_seg", 32))
     td = a.tile_row_ptr.device
     ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=td)
     v = torch.empty(max(nnz, 1), dtype=_TORCH_OF[_NP_TO_DT[a.dtype]], device=td)
@@ -906,16 +945,26 @@ def spgemm_plain(a: SPMatrix, b: SPMatrix) -> SPMatrix:
     return SPMatrix(a.m, b.n, tm, tn, a.dtype, a.device, trp, torch.from_numpy(toff).to(td), ci, v)
 
 
-def spmm(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:
+def spmm(a: SPMatrix, b: DMatrix, c: DMatrix, tuning=None) -> None:
     """C += A * B over tile grids in one launch (BCL::gemm(SPMatrix, DMatrix,
-    DMatrix&), spgemm.hpp:153-179)."""
+    DMatrix&), spgemm.hpp:153-179).  ``tuning``: a dict of SpMM context
+    knobs (spmm_rows, spmm_long_row, spmm_long_blocks, spmm_hot_permille) or
+    "auto" for the autotuner's cached choice; results do not depend on it."""
     if a.n != b.m or a.m != c.m or b.n != c.n:
         raise RuntimeError("BCL::gemm: shape mismatch")
     if a.dtype != np.float32:
         raise TypeError("SpMM needs FP32 sparse values")
-    h = context(a.device).use_current_stream()
+    if tuning == "auto":
+        from . import autotune
+        tuning = autotune.lookup(a, b, "spmm")
+    ctx = context(a.device)
+    h = ctx.use_current_stream()
     ag, bg, cg = a.spgrid(), b.dgrid(), c.dgrid()
-    call("bclx_spmm_grid", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(cg))
+    if tuning:
+        with ctx.tuned(**tuning):
+            call("bclx_spmm_grid", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(cg))
+    else:
+        call("bclx_spmm_grid", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(cg))
 
 
 def rowwise_gemm(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:

@@ -51,7 +51,12 @@ struct Context {
   // on first use), with events to fork from and join back to the main stream.
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, fork2_ev = nullptr, join_ev = nullptr;
+  // bclx_context_set_tuning values (-1: the default)
+  int64_t tune[BCLX_TUNE_KEYS] = {-1, -1, -1, -1, -1, -1, -1};
 };
+
+// The value in effect for a tuning knob (the context's, else the default).
+int64_t tuning(const Context* ctx, int key);
 
 // Create ctx->side and its events if they do not exist yet.
 int ensure_side_stream(Context* ctx);

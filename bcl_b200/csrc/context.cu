@@ -2,11 +2,55 @@
 // exclusive scan used to turn per-row counts into CSR offsets.
 #include "common.cuh"
 
+#include <cstdlib>
+
 #include <atomic>
 #include <cstring>
 #include <string>
 
 namespace bclx {
+
+static int64_t env_or(const char* name, int64_t dflt) {
+  const char* e = std::getenv(name);
+  return e && *e ? std::strtoll(e, nullptr, 10) : dflt;
+}
+
+// Defaults of the tuning knobs (environment variables override some, for
+// experiments without code changes).
+static int64_t tuning_default(const Context* ctx, int key) {
+  switch (key) {
+    case BCLX_TUNE_LIGHT_UB: return 512;
+    case BCLX_TUNE_LEARN_TARGET: return 320;
+    case BCLX_TUNE_BTABLE_MAX_BYTES: return env_or("BCLX_BTABLE_MAX_BYTES", int64_t(2) << 30);
+    case BCLX_TUNE_SPMM_ROWS: return env_or("BCLX_SPMM_ROWS", 0);
+    case BCLX_TUNE_SPMM_LONG_ROW: return 1024;
+    case BCLX_TUNE_SPMM_LONG_BLOCKS: return env_or("BCLX_SPMM_LONG_BLOCKS", ctx->num_sms / 2);
+    case BCLX_TUNE_SPMM_HOT_PERMILLE: {
+      const char* e = std::getenv("BCLX_SPMM_HOT_FRACTION");
+      return e && *e ? (int64_t)(std::atof(e) * 1000.0 + 0.5) : 500;
+    }
+    default: return 0;
+  }
+}
+
+static bool tuning_in_range(const Context* ctx, int key, int64_t v) {
+  switch (key) {
+    case BCLX_TUNE_LIGHT_UB: return v >= 32 && v <= 512;
+    case BCLX_TUNE_LEARN_TARGET: return v >= 64 && v <= 448;
+    case BCLX_TUNE_BTABLE_MAX_BYTES: return true;
+    case BCLX_TUNE_SPMM_ROWS: return v == 0 || v == 1 || v == 2 || v == 4;
+    case BCLX_TUNE_SPMM_LONG_ROW: return v >= 64 && v <= INT32_MAX;
+    case BCLX_TUNE_SPMM_LONG_BLOCKS: return v >= 1 && v <= ctx->num_sms;
+    case BCLX_TUNE_SPMM_HOT_PERMILLE: return v <= 900;
+    default: return false;
+  }
+}
+
+int64_t tuning(const Context* ctx, int key) {
+  if (key < 0 || key >= BCLX_TUNE_KEYS) return 0;
+  return ctx->tune[key] >= 0 ? ctx->tune[key] : tuning_default(ctx, key);
+}
+
 
 static thread_local std::string g_last_error;
 
@@ -223,6 +267,21 @@ int bclx_context_destroy(bclx_context_t c) {
     if (e) cudaEventDestroy(e);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   delete ctx;
+  return BCLX_OK;
+}
+
+int bclx_context_set_tuning(bclx_context_t c, int32_t key, int64_t value) {
+  Context* ctx = reinterpret_cast<Context*>(c);
+  if (!ctx || key < 0 || key >= BCLX_TUNE_KEYS) return BCLX_ERR_INVALID;
+  if (value >= 0 && !tuning_in_range(ctx, key, value)) return BCLX_ERR_INVALID;
+  ctx->tune[key] = value < 0 ? -1 : value;
+  return BCLX_OK;
+}
+
+int bclx_context_get_tuning(bclx_context_t c, int32_t key, int64_t* value) {
+  Context* ctx = reinterpret_cast<Context*>(c);
+  if (!ctx || !value || key < 0 || key >= BCLX_TUNE_KEYS) return BCLX_ERR_INVALID;
+  *value = tuning(ctx, key);
   return BCLX_OK;
 }
 

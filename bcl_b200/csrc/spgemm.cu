@@ -958,7 +958,8 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
 
 // ---- learned product ---------------------------------------------------------------------
 
-constexpr float kLearnTarget = 320.f;  // outputs aimed at per heavy item (the accumulator holds 512)
+// outputs aimed at per heavy item (the accumulator holds kVcap): the
+// context's BCLX_TUNE_LEARN_TARGET, 320 by default
 constexpr float kLearnMargin = 1.15f;  // head room on the predicted count
 constexpr float kCapMargin = 1.25f;    // head room of an item's temp slots over its estimate
 constexpr float kCapSlack = 32.f;
@@ -1014,7 +1015,7 @@ __global__ void __launch_bounds__(256) k_heavy_block_ub(SpGridView A, SpGridView
   }
 }
 
-// Heavy rows cut into fine-block ranges of about kLearnTarget expected
+// Heavy rows cut into fine-block ranges of about `target` expected
 // outputs, greedy left to right.  A block of width w receiving p products is
 // expected to hold w*(1 - exp(-p/w)) distinct columns (p products spread over
 // w columns); the network's predicted row count (pred = log2(1 + count))
@@ -1036,7 +1037,7 @@ __global__ void k_learned_cut(Geom g, const int32_t* __restrict__ heavy_list, in
                               const float* __restrict__ pred, const int32_t* __restrict__ ub,
                               const int32_t* __restrict__ bub, int32_t* __restrict__ n_items,
                               const int64_t* __restrict__ first, HeavyItem* __restrict__ items,
-                              int32_t* __restrict__ item_cap) {
+                              int32_t* __restrict__ item_cap, float target) {
   const int nfb_g = (int)g.nfb;
   for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n_heavy; h += (int64_t)gridDim.x * blockDim.x) {
     const int64_t ri = heavy_list[h];
@@ -1060,7 +1061,7 @@ __global__ void k_learned_cut(Geom g, const int32_t* __restrict__ heavy_list, in
       const float w = (float)min(kFineCols, x.w - b * kFineCols);
       const float p = (float)bu[b];
       const float e = pred ? fminf(w, kappa * w * (1.f - __expf(-p / w))) : fminf(w, p);
-      if (b > start && cur + e > kLearnTarget) {
+      if (b > start && cur + e > target) {
         if (FILL) {
           const int cap = item_capacity(cur, pred != nullptr);
           item_cap[out] = cap;
@@ -1431,20 +1432,17 @@ static int build_stage_map(Context* ctx, const SpGridView& A, const SpGridView& 
   return BCLX_OK;
 }
 
-// B-row table (k_btable) when it fits kBTableMaxBytes; otherwise none and the
-// walks find column-block ranges by binary search.
-// BCLX_BTABLE_MAX_BYTES overrides the cap (0: never build the table).
-static int64_t btable_cap() {
-  const char* e = std::getenv("BCLX_BTABLE_MAX_BYTES");
-  return e && *e ? std::strtoll(e, nullptr, 10) : kBTableMaxBytes;
-}
+// B-row table (k_btable) when it fits the context's BCLX_TUNE_BTABLE_MAX_BYTES
+// (default 2 GiB); otherwise none and the walks find column-block ranges by
+// binary search.
+static int64_t btable_cap(const Context* ctx) { return tuning(ctx, BCLX_TUNE_BTABLE_MAX_BYTES); }
 
 // With `side`, the table is allocated in stream order on the main stream and
 // built on `side` after a fork event.
 static int build_btable(Context* ctx, const SpGridView& B, const Geom& g, bclx_spgemm_plan_s* P,
                         cudaStream_t side = nullptr) {
   const int64_t nbrows = g.gk * g.gn * g.tk;
-  if ((int64_t)sizeof(int32_t) * nbrows * (g.nfb + 1) > btable_cap()) {
+  if ((int64_t)sizeof(int32_t) * nbrows * (g.nfb + 1) > btable_cap(ctx)) {
     P->tab = nullptr;
     return BCLX_OK;
   }
@@ -1487,6 +1485,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   BCLX_CK(cudaMemsetAsync(P->row_count, 0, sizeof(int32_t) * (nri > 0 ? nri : 1), ctx->stream));
   // rows of tiles wider than 8192 columns always take the block path
   const int heavy_min_cols = 8192 + 1;
+  P->light_ub_max = (int)tuning(ctx, BCLX_TUNE_LIGHT_UB);
   if (nri > 0) {
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
@@ -2104,7 +2103,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   if (nri > 0) {
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
-        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, 8192 + 1, kLightUb, P->feat, P->ub,
+        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, 8192 + 1, (int)tuning(ctx, BCLX_TUNE_LIGHT_UB), P->feat, P->ub,
         P->queue + 1);
     note_launch();
     BCLX_CK_LAUNCH();
@@ -2158,7 +2157,8 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
     note_launch();
     BCLX_CK_LAUNCH();
     k_learned_cut<false><<<hb, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, params ? P->pred : nullptr,
-                                                      P->ub, P->block_ub, P->heavy_nitems, nullptr, nullptr, nullptr);
+                                                      P->ub, P->block_ub, P->heavy_nitems, nullptr, nullptr, nullptr,
+                                                      (float)tuning(ctx, BCLX_TUNE_LEARN_TARGET));
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -2184,7 +2184,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   if (P->n_heavy > 0) {
     k_learned_cut<true><<<hb, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, params ? P->pred : nullptr,
                                                      P->ub, P->block_ub, nullptr, P->heavy_first, P->heavy_items,
-                                                     P->item_cap);
+                                                     P->item_cap, (float)tuning(ctx, BCLX_TUNE_LEARN_TARGET));
     note_launch();
     BCLX_CK_LAUNCH();
   }

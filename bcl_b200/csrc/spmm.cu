@@ -500,15 +500,15 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
 // (row, C tile column, panel), with the B-row slices themselves copied into
 // shared memory by cp.async two chunks (64 entries) ahead: the loads in
 // flight cost no registers, and a chunk's multiply-adds read shared memory.
-// Rows of kSpmmVeryLongRow entries or more are listed first, so that the
+// Rows of 8 times the long-row threshold or more are listed first, so that the
 // longest chains start first.
 
 constexpr int kLongWarps = 4;
 constexpr int kLongBSlots = 3;  // chunks of B slices per warp: applied, in flight, being issued
 constexpr int kLongTSlots = 3;  // chunks of table entries per warp (with the B slices)
 constexpr int kLongASlots = 6;  // chunks of staged A entries per warp
-constexpr int kSpmmLongRow = 1024;           // entries over all stages
-constexpr int kSpmmVeryLongRow = 8192;       // listed at the front
+// A row is long from BCLX_TUNE_SPMM_LONG_ROW entries over all stages (1024 by
+// default); rows of 8 times that are listed at the front.
 constexpr int64_t kSpmmLongMinRows = 65536;  // smaller products do not use the long-row path
 
 struct LongSmem {
@@ -729,10 +729,9 @@ __global__ void __launch_bounds__(kLongWarps * 32)
 }
 
 // Blocks of k_spmm_long (one per SM: its shared memory fills the SM): half
-// the SMs by default, the rest run k_spmm.  BCLX_SPMM_LONG_BLOCKS overrides.
+// the SMs by default, the rest run k_spmm (BCLX_TUNE_SPMM_LONG_BLOCKS).
 static int spmm_long_blocks(const Context* ctx) {
-  const char* e = std::getenv("BCLX_SPMM_LONG_BLOCKS");
-  const int b = e && *e ? std::atoi(e) : ctx->num_sms / 2;
+  const int b = (int)tuning(ctx, BCLX_TUNE_SPMM_LONG_BLOCKS);
   return std::max(1, std::min(b, ctx->num_sms));
 }
 
@@ -743,14 +742,11 @@ static int64_t spmm_long_min_rows() {
 
 // Rows per k_spmm warp item: grouping short rows shares one prologue (tile
 // descriptors, row pointers, A loads) among them, while the items still
-// cover every resident warp.  BCLX_SPMM_ROWS overrides (1, 2, 4).
+// cover every resident warp.  BCLX_TUNE_SPMM_ROWS (1, 2, 4) overrides.
 static int spmm_rows_per_item(const Context* ctx, const DGridView& C, int64_t gk, int npanels) {
   auto fits = [&](int r) { return r <= kSpmmMaxRows && r * gk <= 32; };
-  const char* e = std::getenv("BCLX_SPMM_ROWS");
-  if (e && *e) {
-    const int r = std::atoi(e);
-    if ((r == 1 || r == 2 || r == 4) && fits(r)) return r;
-  }
+  const int want = (int)tuning(ctx, BCLX_TUNE_SPMM_ROWS);
+  if ((want == 1 || want == 2 || want == 4) && fits(want)) return want;
   const int64_t resident = (int64_t)ctx->num_sms * 4 * kSpmmWarps;
   int r = 1;
   while (fits(2 * r) && C.gm * C.gn * ceil_div(C.tm, (int64_t)(2 * r)) * npanels >= resident) r *= 2;
@@ -802,12 +798,11 @@ __global__ void k_deg_threshold(const unsigned long long* __restrict__ hist, lon
   *thr = (int32_t)(t < 2 ? 2 : (t > INT32_MAX ? INT32_MAX : t));
 }
 
-// Hints pay when B does not fit in L2 (otherwise every row stays anyway).
-// BCLX_SPMM_HOT_FRACTION: the share of L2 given to the most referenced B
-// rows (default 0.5; 0 turns the hints off).
-static double spmm_hot_fraction() {
-  const char* e = std::getenv("BCLX_SPMM_HOT_FRACTION");
-  return e && *e ? std::atof(e) : 0.5;
+// Hints pay when B does not fit in L2 (otherwise every row stays anyway):
+// BCLX_TUNE_SPMM_HOT_PERMILLE of L2 goes to the most referenced B rows
+// (default 500; 0 turns the hints off).
+static double spmm_hot_fraction(const Context* ctx) {
+  return (double)tuning(ctx, BCLX_TUNE_SPMM_HOT_PERMILLE) / 1000.0;
 }
 
 // ---- launch --------------------------------------------------------------------
@@ -824,6 +819,7 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   const int64_t cap = (int64_t)ctx->num_sms * 4;  // resident blocks: warps take items from a counter
   const int64_t arows = A.gm * A.tm;
   const bool long_path = align_ok && A.gn <= 32 && arows >= spmm_long_min_rows();
+  const int long_row = (int)tuning(ctx, BCLX_TUNE_SPMM_LONG_ROW);
   // counters: [0] k_spmm items, [1] k_spmm_long items, [2] listed very long / other long rows (2 x int32)
   unsigned long long* ctr = nullptr;
   BCLX_TRY(scratch_alloc_n(ctx, &ctr, 3));
@@ -837,7 +833,7 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   {
     int l2 = 0;
     BCLX_CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->device));
-    const double frac = spmm_hot_fraction();
+    const double frac = spmm_hot_fraction(ctx);
     const int64_t row_bytes = C.n * (int64_t)sizeof(ST);
     const int64_t b_bytes = B.m * row_bytes;
     if (align_ok && frac > 0 && l2 > 0 && b_bytes > (int64_t)l2) {
@@ -871,7 +867,7 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
     BCLX_TRY(scratch_alloc_n(ctx, &flag, (size_t)arows));
     BCLX_TRY(scratch_alloc_n(ctx, &list, (size_t)arows));
     k_spmm_find_long<<<(unsigned)std::min<int64_t>(ceil_div(arows, 256), (int64_t)ctx->num_sms * 16), 256, 0,
-                       ctx->stream>>>(A, kSpmmLongRow, kSpmmVeryLongRow, flag, list, cnt);
+                       ctx->stream>>>(A, long_row, long_row * 8, flag, list, cnt);
     note_launch();
     BCLX_CK_LAUNCH();
     const size_t lsmem = sizeof(LongSmem) * kLongWarps;

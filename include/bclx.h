@@ -141,6 +141,21 @@ BCLX_API int bclx_context_synchronize(bclx_context_t ctx);
  * device memory to the driver (the pool keeps freed scratch for reuse).
  * Counterpart of freeing a BCL segment (BCL::finalize, backends/mpi/backend.hpp:120-130). */
 BCLX_API int bclx_context_release_cached(bclx_context_t ctx);
+/* Tuning knobs of a context, read by the later calls on it (no reference
+ * counterpart; the autotuner, bcl_b200/autotune.py, searches them).  A value
+ * below 0 restores the default; out-of-range values are BCLX_ERR_INVALID. */
+typedef enum {
+  BCLX_TUNE_LIGHT_UB = 0,          /* SpGEMM: a row with at most this many products is light (32..512; 512) */
+  BCLX_TUNE_LEARN_TARGET = 1,      /* learned product: outputs aimed at per heavy item (64..448; 320) */
+  BCLX_TUNE_BTABLE_MAX_BYTES = 2,  /* SpGEMM: largest B-row table built (0..; 2 GiB, or BCLX_BTABLE_MAX_BYTES) */
+  BCLX_TUNE_SPMM_ROWS = 3,         /* SpMM: rows per warp item (0 = by product size, 1, 2, 4) */
+  BCLX_TUNE_SPMM_LONG_ROW = 4,     /* SpMM: entries from which a row goes to the long-row kernel (64..; 1024) */
+  BCLX_TUNE_SPMM_LONG_BLOCKS = 5,  /* SpMM: blocks of the long-row kernel (1..SMs; half the SMs) */
+  BCLX_TUNE_SPMM_HOT_PERMILLE = 6, /* SpMM: per mille of L2 kept for the most referenced B rows (0..900; 500) */
+  BCLX_TUNE_KEYS = 7
+} bclx_tune_key_t;
+BCLX_API int bclx_context_set_tuning(bclx_context_t ctx, int32_t key, int64_t value);
+BCLX_API int bclx_context_get_tuning(bclx_context_t ctx, int32_t key, int64_t* value);
 /* Text of the last CUDA error seen on this thread (empty if none). */
 BCLX_API const char* bclx_last_error(void);
 /* Library version, e.g. 100 for 0.1.0. */

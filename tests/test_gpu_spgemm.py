@@ -252,10 +252,33 @@ def test_autotune_roundtrip(tmp_path, monkeypatch):
     a = gen.rmat(11, seed=64)
     A = SPMatrix.from_csr(a, BlockCustom((1024, 1024)))
     params, ms, table = autotune.tune(A, A, reps=1, candidates={"grab": (1, 4), "blocks_per_sm": (4,),
-                                                                "long_seg": (48,)})
-    assert len(table) == 2 and ms > 0
+                                                                "long_seg": (48,)}, light_ubs=(256, 512))
+    assert len(table) == 2 and ms > 0 and params["light_ub"] in (256, 512)
     C, plan = spgemm(A, A, tuning="auto", keep_plan=True)
-    assert autotune.lookup(A, A, plan) == tuple(params)
+    assert autotune.lookup(A, A) == params
     plan.close()
     rp, ci, cv = O.gemm_tiled(a, a, 1024, 1024, 1024)
     assert_csr_identical(C.get(), rp, ci, cv)
+
+
+@pytest.mark.parametrize("light_ub", [32, 128, 512])
+def test_light_row_bound_does_not_change_results(light_ub):
+    """The light/heavy classification bound moves rows between the warp and
+    the cut-item paths; the result stays bit-identical."""
+    from bcl_b200.containers import BlockCustom, SPMatrix, context, spgemm
+    a = gen.rmat(12, seed=65)
+    A = SPMatrix.from_csr(a, BlockCustom((1024, 1024)))
+    with context().tuned(light_ub=light_ub):
+        C = spgemm(A, A)
+    rp, ci, cv = O.gemm_tiled(a, a, 1024, 1024, 1024)
+    assert_csr_identical(C.get(), rp, ci, cv)
+
+
+def test_tuning_knobs_reject_out_of_range():
+    from bcl_b200 import _lib
+    from bcl_b200.containers import context
+    ctx = context()
+    for key, bad in ((_lib.TUNE_LIGHT_UB, 1000), (_lib.TUNE_LEARN_TARGET, 10), (_lib.TUNE_SPMM_ROWS, 3),
+                     (_lib.TUNE_SPMM_HOT_PERMILLE, 950), (_lib.TUNE_SPMM_LONG_BLOCKS, 100000)):
+        assert _lib.load().bclx_context_set_tuning(ctx.h, key, bad) == _lib.ERR_INVALID
+    assert ctx.get_tuning("light_ub") == 512

@@ -210,3 +210,61 @@ def test_spmm_tile_single_call_ld():
     want = O.spmm_tiled(a, b[:, :64].copy(), c0, 500, 500, 64)
     assert np.array_equal(bits(C[:, :64].cpu().numpy()), bits(want))
     assert torch.count_nonzero(C[:, 64:]) == 0
+
+
+@pytest.mark.parametrize("knobs", [dict(spmm_rows=1), dict(spmm_rows=4, spmm_long_row=64, spmm_long_blocks=20),
+                                   dict(spmm_hot_permille=0), dict(spmm_hot_permille=900, spmm_long_row=128)])
+def test_spmm_knobs_do_not_change_results(monkeypatch, knobs):
+    """Rows per item, the long-row threshold and block count, and the L2 hint
+    share (hints forced on by a small long-row product size) leave every bit
+    of C as it was."""
+    monkeypatch.setenv("BCLX_SPMM_LONG_MIN_ROWS", "1024")
+    import torch
+    from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm
+    a = gen.rmat(13, seed=11)
+    b = gen.dense(a.n, 256, seed=12)
+    c0 = gen.dense(a.m, 256, seed=13)
+    A = SPMatrix.from_csr(a, BlockCustom((2048, 2048)))
+    B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((2048, 256)))
+    C = DMatrix.from_array(torch.from_numpy(c0), BlockCustom((2048, 256)))
+    spmm(A, B, C, tuning=knobs)
+    want = O.spmm_tiled(a, b, c0, 2048, 2048, 256)
+    assert np.array_equal(bits(C.get_matrix().cpu().numpy()), bits(want))
+
+
+def test_spmm_autotune_roundtrip(tmp_path, monkeypatch):
+    monkeypatch.setenv("BCLX_CACHE", str(tmp_path))
+    import torch
+    from bcl_b200 import autotune
+    from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm
+    a = gen.rmat(12, seed=14)
+    b = gen.dense(a.n, 128, seed=15)
+    A = SPMatrix.from_csr(a, BlockCustom((1024, 1024)))
+    B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((1024, 128)))
+    C = DMatrix.zeros((a.m, 128), BlockCustom((1024, 128)))
+    params, ms = autotune.tune_spmm(A, B, C, reps=1, candidates={"spmm_rows": (1, 2), "spmm_hot_permille": (0, 500)})
+    assert ms > 0 and autotune.lookup(A, B, "spmm") == params
+    C2 = DMatrix.zeros((a.m, 128), BlockCustom((1024, 128)))
+    spmm(A, B, C2, tuning="auto")
+    want = O.spmm_tiled(a, b, np.zeros((a.m, 128), np.float32), 1024, 1024, 128)
+    assert np.array_equal(bits(C2.get_matrix().cpu().numpy()), bits(want))
+
+
+@pytest.mark.parametrize("hot", [0, 500, 900])
+def test_spmm_l2_hints_large_b(hot):
+    """B larger than L2 (R-MAT s18 x 256 FP32, 268 MB) turns the B-row reuse
+    hints on: the result on sampled rows stays bit-exact for any share of L2
+    given to the most referenced rows (0 = hints off)."""
+    import torch
+    from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm
+    a = gen.rmat(18, seed=16)
+    b = gen.dense(a.n, 256, seed=17, dist="normal")
+    ts = a.m // 4
+    A = SPMatrix.from_csr(a, BlockCustom((ts, ts)))
+    B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((ts, 256)))
+    C = DMatrix.zeros((a.m, 256), BlockCustom((ts, 256)))
+    spmm(A, B, C, tuning=dict(spmm_hot_permille=hot))
+    rows = np.unique(np.concatenate([np.random.default_rng(18).choice(a.m, 2048, replace=False), np.arange(32)]))
+    got = C.get_matrix()[torch.as_tensor(rows, device="cuda")].cpu().numpy()
+    want = O.spmm_tiled(a, b, np.zeros((rows.size, 256), np.float32), ts, ts, 256, rows=rows)
+    assert np.array_equal(bits(got), bits(want))
