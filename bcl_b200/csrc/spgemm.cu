@@ -49,7 +49,7 @@
 namespace bclx {
 
 constexpr int kLightUb = 512;        // products of a light row (so <= 512 outputs)
-constexpr int kVcap = 512;           // outputs per numeric item
+constexpr int kVcap = 512;           // outputs per numeric item (the default; BCLX_TUNE_ITEM_OUTPUTS: 512 or 1024)
 constexpr int kFineCols = 256;       // column block of heavy rows and of the B-row table
 constexpr int kMaxWords = 512;       // bitmap words per warp (tiles up to 16384 columns)
 constexpr int kMaxCols = kMaxWords * 32;
@@ -652,7 +652,7 @@ __global__ void k_tile_ptrs(Geom g, const int64_t* __restrict__ row_offset, int3
   }
 }
 
-// Heavy rows are cut at fine-block boundaries into items of <= kVcap outputs
+// Heavy rows are cut at fine-block boundaries into items of <= vcap outputs
 // (greedy left to right; leading empty blocks are skipped).  One warp per
 // heavy row (blocks of 256 threads): lanes count the fine blocks' outputs
 // from the row's bitmap, lane 0 cuts.  FILL = false counts the items,
@@ -669,7 +669,7 @@ template <bool FILL>
 __global__ void __launch_bounds__(256)
     k_cut_heavy(Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
                 const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, int32_t* __restrict__ n_items,
-                const int64_t* __restrict__ first, HeavyItem* __restrict__ items) {
+                const int64_t* __restrict__ first, HeavyItem* __restrict__ items, int vcap) {
   __shared__ int32_t cnt_all[8][kMaxCols / kFineCols];
   int32_t* cnt = cnt_all[threadIdx.x >> 5];
   const int lane = lane_id();
@@ -696,7 +696,7 @@ __global__ void __launch_bounds__(256)
       int64_t out = FILL ? first[h] : 0;
       for (int b = 0; b < nfb; b++) {
         const int c = cnt[b];
-        if (cur > 0 && cur + c > kVcap) {
+        if (cur > 0 && cur + c > vcap) {
           if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)b, rel, cur};
           nit++;
           rel += cur;
@@ -718,13 +718,13 @@ __global__ void __launch_bounds__(256)
 
 // ---- numeric ------------------------------------------------------------------------------
 
-template <typename VT, int WORDS>
+template <typename VT, int WORDS, int VCAP>
 struct WarpSmem {
   uint32_t bm[WORDS];
   uint16_t pre[WORDS];
-  VT acc[kVcap];
-  VT part[kVcap];
-  unsigned char tag[kVcap];
+  VT acc[VCAP];
+  VT part[VCAP];
+  unsigned char tag[VCAP];
   VT sa[32];
   VT sb[32];
   int32_t ss[32];
@@ -741,7 +741,7 @@ struct WarpSmem {
 // heavy_slot_base + item_off[idx], after all light slots; an item's slot
 // count, at most kVcap, comes from the prediction),
 // counts to item_count / row_count_w.
-template <typename VT, int WORDS, bool LEARNED>
+template <typename VT, int WORDS, bool LEARNED, int VCAP>
 __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     k_numeric(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
               const int32_t* __restrict__ heavy_list, int n_light, int64_t n_heavy_items,
@@ -754,7 +754,7 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
               int32_t* __restrict__ row_count_w, int32_t* __restrict__ row_failed, int64_t heavy_slot_base,
               const int64_t* __restrict__ item_off) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  WarpSmem<VT, WORDS>& S = reinterpret_cast<WarpSmem<VT, WORDS>*>(smem_raw)[threadIdx.x >> 5];
+  WarpSmem<VT, WORDS, VCAP>& S = reinterpret_cast<WarpSmem<VT, WORDS, VCAP>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = lane_id();
   const int64_t n_total = n_heavy_items + n_light;
   // persistent warps: take `grab` consecutive items at a time from the queue
@@ -772,7 +772,7 @@ __global__ void __launch_bounds__(kWarpsNum * 32, BCLX_NUMERIC_MIN_BLOCKS)
     // heavy items first (they are the larger ones)
     const bool heavy = idx < n_heavy_items;
     int64_t ri;
-    int cnt = 0, fb_lo = 0, fb_hi = 0, lo = 0, hi, hslot = 0, icap = kVcap;
+    int cnt = 0, fb_lo = 0, fb_hi = 0, lo = 0, hi, hslot = 0, icap = VCAP;
     int64_t off;
     const uint32_t* hb = nullptr;
     if (heavy) {
@@ -1216,6 +1216,7 @@ struct bclx_spgemm_plan_s {
   // numeric tuning (bclx_spgemm_plan_tune)
   int grab = 1, blocks_per_sm = 4, long_seg = kLongSegDefault;
   int light_ub_max = kLightUb;         // light-row class bound (products), set at symbolic time
+  int vcap = kVcap;                    // outputs per heavy item (512 or 1024), set at symbolic time
   // CUDA graph of the staged numeric pass (bclx_spgemm_numeric_staged)
   cudaGraphExec_t graph = nullptr;
   const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -1364,11 +1365,11 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
   return BCLX_OK;
 }
 
-template <typename VT, int WORDS, bool LEARNED = false>
+template <typename VT, int WORDS, bool LEARNED = false, int VCAP = kVcap>
 static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P,
                             int32_t* out_col, void* out_val, int s0, int s1) {
-  constexpr size_t smem = sizeof(WarpSmem<VT, WORDS>) * kWarpsNum;
-  auto kern = k_numeric<VT, WORDS, LEARNED>;
+  constexpr size_t smem = sizeof(WarpSmem<VT, WORDS, VCAP>) * kWarpsNum;
+  auto kern = k_numeric<VT, WORDS, LEARNED, VCAP>;
   static std::atomic<unsigned long long> configured{0};  // one bit per device
   const unsigned long long bit = 1ull << (ctx->device & 63);
   if (!(configured.load() & bit)) {
@@ -1393,6 +1394,10 @@ static int launch_numeric_w(Context* ctx, const SpGridView& A, const SpGridView&
 template <typename VT>
 static int launch_numeric(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P,
                           int32_t* out_col, void* out_val, int s0, int s1) {
+  if (P->vcap == 1024) {
+    if (P->g.tn <= 8192) return launch_numeric_w<VT, 256, false, 1024>(ctx, A, B, P, out_col, out_val, s0, s1);
+    return launch_numeric_w<VT, kMaxWords, false, 1024>(ctx, A, B, P, out_col, out_val, s0, s1);
+  }
   if (P->g.tn <= 8192) return launch_numeric_w<VT, 256>(ctx, A, B, P, out_col, out_val, s0, s1);
   return launch_numeric_w<VT, kMaxWords>(ctx, A, B, P, out_col, out_val, s0, s1);
 }
@@ -1486,6 +1491,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   // rows of tiles wider than 8192 columns always take the block path
   const int heavy_min_cols = 8192 + 1;
   P->light_ub_max = (int)tuning(ctx, BCLX_TUNE_LIGHT_UB);
+  P->vcap = (int)tuning(ctx, BCLX_TUNE_ITEM_OUTPUTS);
   if (nri > 0) {
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
@@ -1527,7 +1533,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   if (P->n_heavy > 0) {
     const unsigned blocks = grid_for(ctx, P->n_heavy, 8, 8);
     k_cut_heavy<false><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
-                                                        P->hbm_words, P->heavy_nitems, nullptr, nullptr);
+                                                        P->hbm_words, P->heavy_nitems, nullptr, nullptr, P->vcap);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1549,7 +1555,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_items, P->n_heavy_items));
     const unsigned blocks = grid_for(ctx, P->n_heavy, 8, 8);
     k_cut_heavy<true><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
-                                                       P->hbm_words, nullptr, P->heavy_first, P->heavy_items);
+                                                       P->hbm_words, nullptr, P->heavy_first, P->heavy_items, P->vcap);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1966,7 +1972,7 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
   BCLX_CK_LAUNCH();
   if (P.n_heavy > 0) {
     k_cut_heavy<false><<<grid_for(ctx, P.n_heavy, 8, 8), 256, 0, ctx->stream>>>(
-        g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, P.heavy_nitems, nullptr, nullptr);
+        g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, P.heavy_nitems, nullptr, nullptr, P.vcap);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -2001,7 +2007,7 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
     if (probe.ok) ar = probe;
     else P.tab = nullptr;
     k_cut_heavy<true><<<grid_for(ctx, P.n_heavy, 8, 8), 256, 0, ctx->stream>>>(
-        g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, nullptr, P.heavy_first, P.heavy_items);
+        g, P.heavy_list, (int)P.n_heavy, P.heavy_bitmaps, P.hbm_words, nullptr, P.heavy_first, P.heavy_items, P.vcap);
     note_launch();
     BCLX_CK_LAUNCH();
     if (P.tab && g.tk > 0) {
@@ -2250,7 +2256,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
     R->row_offset = P->redo_off;  // borrowed
     const unsigned rb = grid_for(ctx, nf, 8, 8);
     k_cut_heavy<false><<<rb, 256, 0, ctx->stream>>>(g, R->heavy_list, nf, R->heavy_bitmaps, R->hbm_words,
-                                                    R->heavy_nitems, nullptr, nullptr);
+                                                    R->heavy_nitems, nullptr, nullptr, R->vcap);
     note_launch();
     BCLX_CK_LAUNCH();
     BCLX_TRY(exclusive_scan_i32(ctx, R->heavy_nitems, R->heavy_first, nf));
@@ -2261,7 +2267,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
     R->n_heavy_items = rt[0];
     BCLX_TRY(scratch_alloc_n(ctx, &R->heavy_items, R->n_heavy_items));
     k_cut_heavy<true><<<rb, 256, 0, ctx->stream>>>(g, R->heavy_list, nf, R->heavy_bitmaps, R->hbm_words, nullptr,
-                                                   R->heavy_first, R->heavy_items);
+                                                   R->heavy_first, R->heavy_items, R->vcap);
     note_launch();
     BCLX_CK_LAUNCH();
     R->tab = P->tab;  // borrowed

@@ -152,7 +152,8 @@ typedef enum {
   BCLX_TUNE_SPMM_LONG_ROW = 4,     /* SpMM: entries from which a row goes to the long-row kernel (64..; 1024) */
   BCLX_TUNE_SPMM_LONG_BLOCKS = 5,  /* SpMM: blocks of the long-row kernel (1..SMs; half the SMs) */
   BCLX_TUNE_SPMM_HOT_PERMILLE = 6, /* SpMM: per mille of L2 kept for the most referenced B rows (0..900; 500) */
-  BCLX_TUNE_KEYS = 7
+  BCLX_TUNE_ITEM_OUTPUTS = 7,      /* SpGEMM: outputs per heavy-row work item (512 or 1024; 512) */
+  BCLX_TUNE_KEYS = 8
 } bclx_tune_key_t;
 BCLX_API int bclx_context_set_tuning(bclx_context_t ctx, int32_t key, int64_t value);
 BCLX_API int bclx_context_get_tuning(bclx_context_t ctx, int32_t key, int64_t* value);

@@ -282,3 +282,17 @@ def test_tuning_knobs_reject_out_of_range():
                      (_lib.TUNE_SPMM_HOT_PERMILLE, 950), (_lib.TUNE_SPMM_LONG_BLOCKS, 100000)):
         assert _lib.load().bclx_context_set_tuning(ctx.h, key, bad) == _lib.ERR_INVALID
     assert ctx.get_tuning("light_ub") == 512
+
+
+@pytest.mark.parametrize("tiles", [(1024, 1024, 1024), (2048, 8192, 8192), (4096, 16384, 16384)])
+def test_item_outputs_1024_does_not_change_results(tiles):
+    """Heavy rows cut into items of up to 1024 outputs (larger shared-memory
+    accumulators, fewer items): bit-identical."""
+    from bcl_b200.containers import BlockCustom, SPMatrix, context, spgemm
+    a = gen.rmat(13, seed=66)
+    A = SPMatrix.from_csr(a, BlockCustom(tiles[:2]))
+    B = SPMatrix.from_csr(a, BlockCustom(tiles[1:]))
+    with context().tuned(item_outputs=1024):
+        C = spgemm(A, B)
+    rp, ci, cv = O.gemm_tiled(a, a, *tiles)
+    assert_csr_identical(C.get(), rp, ci, cv)
