@@ -67,7 +67,8 @@ class Context:
     TUNING_KEYS = {"light_ub": _lib.TUNE_LIGHT_UB, "learn_target": _lib.TUNE_LEARN_TARGET,
                    "btable_max_bytes": _lib.TUNE_BTABLE_MAX_BYTES, "spmm_rows": _lib.TUNE_SPMM_ROWS,
                    "spmm_long_row": _lib.TUNE_SPMM_LONG_ROW, "spmm_long_blocks": _lib.TUNE_SPMM_LONG_BLOCKS,
-                   "spmm_hot_permille": _lib.TUNE_SPMM_HOT_PERMILLE, "item_outputs": _lib.TUNE_ITEM_OUTPUTS}
+                   "spmm_hot_permille": _lib.TUNE_SPMM_HOT_PERMILLE, "item_outputs": _lib.TUNE_ITEM_OUTPUTS,
+                   "wide_light": _lib.TUNE_WIDE_LIGHT}
 
     def set_tuning(self, **knobs) -> None:
         """bclx_context_set_tuning for each name=value (None: the default)."""
@@ -642,7 +643,7 @@ def spgemm(a: SPMatrix, b: SPMatrix, stages: str = "fused", keep_plan: bool = Fa
         params = tuning
     elif tuning:
         params = dict(zip(("grab", "blocks_per_sm", "long_seg"), tuning))
-    sym_knobs = {k: params[k] for k in ("light_ub", "item_outputs") if params and k in params}
+    sym_knobs = {k: params[k] for k in ("light_ub", "item_outputs", "wide_light") if params and k in params}
     if sym_knobs:
         with context(a.device).tuned(**sym_knobs):
             plan, out, trp, toff, nnz = spgemm_symbolic(a, b)

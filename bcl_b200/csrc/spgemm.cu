@@ -1488,8 +1488,9 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   BCLX_CK(cudaMemsetAsync(P->counters, 0, 4 * sizeof(int32_t), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P->products_dev, 0, sizeof(unsigned long long), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P->row_count, 0, sizeof(int32_t) * (nri > 0 ? nri : 1), ctx->stream));
-  // rows of tiles wider than 8192 columns always take the block path
-  const int heavy_min_cols = 8192 + 1;
+  // rows of tiles wider than 8192 columns take the heavy path unless the
+  // context allows light rows there (BCLX_TUNE_WIDE_LIGHT)
+  const int heavy_min_cols = tuning(ctx, BCLX_TUNE_WIDE_LIGHT) ? INT_MAX : 8192 + 1;
   P->light_ub_max = (int)tuning(ctx, BCLX_TUNE_LIGHT_UB);
   P->vcap = (int)tuning(ctx, BCLX_TUNE_ITEM_OUTPUTS);
   if (nri > 0) {
@@ -2109,7 +2110,8 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   if (nri > 0) {
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
-        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, 8192 + 1, (int)tuning(ctx, BCLX_TUNE_LIGHT_UB), P->feat, P->ub,
+        A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, tuning(ctx, BCLX_TUNE_WIDE_LIGHT) ? INT_MAX : 8192 + 1,
+        (int)tuning(ctx, BCLX_TUNE_LIGHT_UB), P->feat, P->ub,
         P->queue + 1);
     note_launch();
     BCLX_CK_LAUNCH();

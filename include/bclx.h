@@ -153,7 +153,8 @@ typedef enum {
   BCLX_TUNE_SPMM_LONG_BLOCKS = 5,  /* SpMM: blocks of the long-row kernel (1..SMs; half the SMs) */
   BCLX_TUNE_SPMM_HOT_PERMILLE = 6, /* SpMM: per mille of L2 kept for the most referenced B rows (0..900; 500) */
   BCLX_TUNE_ITEM_OUTPUTS = 7,      /* SpGEMM: outputs per heavy-row work item (512 or 1024; 512) */
-  BCLX_TUNE_KEYS = 8
+  BCLX_TUNE_WIDE_LIGHT = 8,        /* SpGEMM: 1 = rows of tiles wider than 8192 columns may be light (0 or 1; 0) */
+  BCLX_TUNE_KEYS = 9
 } bclx_tune_key_t;
 BCLX_API int bclx_context_set_tuning(bclx_context_t ctx, int32_t key, int64_t value);
 BCLX_API int bclx_context_get_tuning(bclx_context_t ctx, int32_t key, int64_t* value);

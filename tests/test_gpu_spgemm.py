@@ -296,3 +296,26 @@ def test_item_outputs_1024_does_not_change_results(tiles):
         C = spgemm(A, B)
     rp, ci, cv = O.gemm_tiled(a, a, *tiles)
     assert_csr_identical(C.get(), rp, ci, cv)
+
+
+def test_wide_tiles_with_light_rows_do_not_change_results():
+    """16384-wide tiles with light rows allowed (BCLX_TUNE_WIDE_LIGHT): the
+    light path with the wide bitmap template, bit-identical."""
+    from bcl_b200.containers import BlockCustom, SPMatrix, context, spgemm
+    a = gen.rmat(14, seed=67)
+    s = gen.stencil27(26)
+    for m, tiles in ((a, (4096, 16384, 16384)), (s, (16384, 16384, 16384))):
+        A = SPMatrix.from_csr(m, BlockCustom(tiles[:2]))
+        B = SPMatrix.from_csr(m, BlockCustom(tiles[1:]))
+        with context().tuned(wide_light=1):
+            C, plan = spgemm(A, B, keep_plan=True)
+        assert plan.stats()["light_rows"] > 0
+        plan.close()
+        rows = np.sort(np.random.default_rng(1).choice(m.m, 1500, replace=False))
+        rp, ci, cv = O.gemm_tiled(m, m, *tiles, rows=rows)
+        full = C.get()
+        got_rp = full.row_ptr.astype(np.int64)
+        sel = np.concatenate([np.arange(got_rp[r], got_rp[r + 1]) for r in rows])
+        assert np.array_equal(np.diff(got_rp)[rows], np.diff(rp))
+        assert np.array_equal(full.col_ind[sel], ci)
+        assert np.array_equal(full.vals[sel].view(np.uint32), cv.view(np.uint32))
