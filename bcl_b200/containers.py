@@ -782,6 +782,45 @@ def spgemm_blocks(a: SPMatrix, b: SPMatrix, block_rows: int, form: str = "fused"
         yield rows, spgemm_sub(a, b, rows, range(b.gn), form=form, predictor=predictor)
 
 
+def spgemm_to_host(a: SPMatrix, b: SPMatrix, block_rows: int = 1, host: Optional[dict] = None):
+    """C = A * B delivered to pinned host memory with the device-to-host copy
+    overlapped with the product: C is computed one block of `block_rows`
+    tile rows at a time (spgemm_sub) and each finished block's arrays are
+    copied back on a second stream while the next block is computed.
+    `host`: a dict of pinned buffers reused across calls (grown as needed).
+    Returns (host dict, [(tile rows, nnz, tile_row_ptr, tile_offset,
+    col_ind, vals) host views per block]), valid once the call returns (it
+    waits for the copies)."""
+    host = {} if host is None else host
+    copy_stream = host.get("_stream")
+    if copy_stream is None:
+        copy_stream = host["_stream"] = torch.cuda.Stream(device=a.tile_row_ptr.device)
+    compute = torch.cuda.current_stream()
+    blocks, keep = [], []
+    for q, i0 in enumerate(range(0, a.gm, block_rows)):
+        rows = list(range(i0, min(i0 + block_rows, a.gm)))
+        C = spgemm_sub(a, b, rows, range(b.gn))
+        nnz = C.nnz()
+        ev = torch.cuda.Event()
+        ev.record(compute)
+        views = []
+        with torch.cuda.stream(copy_stream):
+            copy_stream.wait_event(ev)
+            for name, t in (("tile_row_ptr", C.tile_row_ptr.reshape(-1)), ("tile_offset", C.tile_offset),
+                            ("col_ind", C.col_ind[:nnz]), ("vals", C.vals[:nnz])):
+                buf = host.get((q, name))
+                if buf is None or buf.numel() < t.numel() or buf.dtype != t.dtype:
+                    buf = host[(q, name)] = torch.empty(max(t.numel(), 1), dtype=t.dtype).pin_memory()
+                dst = buf[:t.numel()]
+                dst.copy_(t, non_blocking=True)
+                views.append(dst)
+        keep.append(C)  # the device arrays stay alive until their copies finish
+        blocks.append((rows, nnz, *views))
+    copy_stream.synchronize()
+    del keep
+    return host, blocks
+
+
 def spgemm_distributed(a: SPMatrix, b: SPMatrix, rank: int, world: int, pgrid=None):
     """This process's C tiles of C = A * B under the reference's block-cyclic
     ownership, A's tile rows and B's tile columns being available here (A
