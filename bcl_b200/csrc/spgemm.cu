@@ -345,23 +345,50 @@ __device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridVi
     const int32_t aincl = warp_inclusive_scan(alen);
     const int32_t atot = __shfl_sync(kFull, aincl, 31);
     const int32_t aexcl = aincl - alen;
-    for (int32_t e0 = 0, chunk = 0; e0 < atot; e0 += 32, chunk++) {
+    // chunk x's A column (one entry per lane) and its B tile, loaded one
+    // chunk ahead so the column load of the next chunk is in flight while
+    // the current chunk's B rows are read
+    struct Ent {
+      int32_t kc;
+      const int32_t* brp;
+      const int32_t* bci;
+    };
+    auto load_ent = [&](int32_t e0) {
+      Ent t{0, nullptr, nullptr};
       const int32_t e = e0 + lane;
       const int sl = warp_search(aincl, e);
       const int32_t sas = __shfl_sync(kFull, as, sl);
       const int32_t sax = __shfl_sync(kFull, aexcl, sl);
       const int32_t* sacol = shfl_ptr(acol, sl);
-      const int32_t* sbrp = shfl_ptr(brp, sl);
-      const int32_t* sbci = shfl_ptr(bci, sl);
+      t.brp = shfl_ptr(brp, sl);
+      t.bci = shfl_ptr(bci, sl);
+      if (e < atot) t.kc = __ldg(sacol + sas + (e - sax));
+      return t;
+    };
+    Ent nxt = atot > 0 ? load_ent(0) : Ent{0, nullptr, nullptr};
+    for (int32_t e0 = 0, chunk = 0; e0 < atot; e0 += 32, chunk++) {
+      const Ent cur = nxt;
+      const int32_t e = e0 + lane;
+      if (e0 + 32 < atot) nxt = load_ent(e0 + 32);
+      const int32_t* sbci = cur.bci;
       int32_t bs = 0, be = 0;
       if (e < atot) {
-        const int32_t kc = __ldg(sacol + sas + (e - sax));
-        bs = __ldg(sbrp + kc);
-        be = __ldg(sbrp + kc + 1);
+        bs = __ldg(cur.brp + cur.kc);
+        be = __ldg(cur.brp + cur.kc + 1);
       }
       const bool lng = be - bs >= 32;
-      if (!lng && chunk % nparts == part)
-        for (int32_t q = bs; q < be; q++) fs(__ldg(sbci + q));
+      if (!lng && chunk % nparts == part) {
+        int32_t q = bs;
+        for (; q + 4 <= be; q += 4) {  // four column loads in flight
+          const int32_t j0 = __ldg(sbci + q), j1 = __ldg(sbci + q + 1);
+          const int32_t j2 = __ldg(sbci + q + 2), j3 = __ldg(sbci + q + 3);
+          fs(j0);
+          fs(j1);
+          fs(j2);
+          fs(j3);
+        }
+        for (; q < be; q++) fs(__ldg(sbci + q));
+      }
       unsigned longm = __ballot_sync(kFull, lng);
       while (longm) {
         const int src = __ffs(longm) - 1;
