@@ -1448,7 +1448,6 @@ __global__ void k_stage_map(SpGridView A, SpGridView B, Geom g, int32_t* __restr
 }
 
 constexpr int64_t kStageMapMinGrid = 17;
-constexpr int64_t kBTableMaxBytes = 2ll << 30;  // larger tables give way to binary searches of B rows
 
 static int build_stage_map(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P, Geom& g) {
   g.smap = g.scount = nullptr;

@@ -69,6 +69,8 @@ def parse_args():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU timing")
     p.add_argument("--no-precision", action="store_true", help="skip the R-MAT scale-21 BF16/FP32 SpMM extra")
+    p.add_argument("--no-large", action="store_true",
+                   help="skip the R-MAT scale-20 and stencil-128^3 SpGEMM extras")
     p.add_argument("--path", default="fused", choices=["fused", "per_stage", "batched_graph", "learned"],
                    help="SpGEMM form timed as the step (default: all stages fused)")
     p.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
@@ -568,7 +570,76 @@ def spgemm_extras(args, A, a, ts, products, stream):
             ex["spmm_precision_rmat21"] = spmm_precision_summary(args, stream)
         except Exception as e:
             ex["spmm_precision_rmat21"] = {"error": repr(e)}
+    if not args.no_large and A.gn <= 16:
+        for name, wl_name in (("rmat20", "spgemm_rmat20"), ("stencil128", "spgemm_stencil128")):
+            try:
+                ex[f"spgemm_{name}"] = spgemm_large_summary(args, WORKLOADS[wl_name], stream)
+            except Exception as e:
+                ex[f"spgemm_{name}"] = {"error": repr(e)[:300]}
     return ex
+
+
+def spgemm_large_summary(args, wl, stream, block_rows=8):
+    """The large SpGEMM configurations (R-MAT s20 on 64x64 tiles, the
+    27-point stencil on 128^3 with 128x128 tiles): the fused product whole;
+    the fused and the learned products one block of `block_rows` C tile
+    rows at a time (the learned form's temporary slots do not fit beside the
+    whole C at s20), each block's C released before the next; the plain
+    per-tile-product loop on 16 sampled C tiles, scaled.  GFLOP/s over the
+    whole product for each, and the learned form's misprediction rate and
+    wasted temporary bytes summed over the blocks."""
+    import torch
+    from bcl_b200 import gen, learned
+    from bcl_b200.containers import BlockCustom, SPMatrix, context, learned_stats, spgemm, spgemm_sub
+    a = spgemm_matrix(wl, args.seed)
+    G = wl["grid"]
+    ts = -(-a.m // G)
+    A = SPMatrix.from_csr(a, BlockCustom((ts, ts)))
+    flops = 2.0 * gen.intermediate_products(a, a)
+    out = {"workload": wl["desc"], "intermediate_products": flops / 2, "block_rows": block_rows}
+
+    def release():
+        torch.cuda.synchronize()
+        context().release_cached()
+        torch.cuda.empty_cache()
+
+    t = time_region(lambda: spgemm(A, A), 2, stream)
+    out["fused_gflops"], out["fused_ms"] = flops / t / 1e9, t * 1e3
+    release()
+    pred = learned.get_default(train_if_missing=False)
+    blocks = [list(range(i0, min(i0 + block_rows, A.gm))) for i0 in range(0, A.gm, block_rows)]
+    for form in ("fused", "learned"):
+        tot, st_sum = 0.0, {}
+        for rows in blocks:
+            fn = (lambda: spgemm_sub(A, A, rows, range(A.gn), form=form, predictor=pred))
+            fn()  # warm (and the learned form's statistics)
+            if form == "learned":
+                _, pl = spgemm_sub(A, A, rows, range(A.gn), form=form, predictor=pred, keep_plan=True)
+                for k, v in learned_stats(pl).items():
+                    st_sum[k] = st_sum.get(k, 0) + v
+                pl.close()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1) / 1e3
+            release()
+        out[f"{form}_blocked_gflops"], out[f"{form}_blocked_ms"] = flops / tot / 1e9, tot * 1e3
+        if form == "learned":
+            out["learned"] = dict(st_sum, misprediction_rate=st_sum.get("rows_redone", 0) /
+                                  max(st_sum.get("heavy_rows", 1), 1),
+                                  wasted_bytes=max(st_sum.get("temp_entries", 0) - st_sum.get("nnz", 0), 0) * 8)
+    tp = plain_sampled_time(A, 16, args.seed)
+    out["plain_gflops"], out["plain_ms"] = flops / tp / 1e9, tp * 1e3
+    out["plain_note"] = "per-tile-product loop on 16 seeded C tiles, scaled to all tiles"
+    out["learned_over_plain"] = out["learned_blocked_gflops"] / out["plain_gflops"]
+    out["learned_over_fused_blocked"] = out["learned_blocked_gflops"] / out["fused_blocked_gflops"]
+    out["batched_over_plain"] = out["fused_gflops"] / out["plain_gflops"]
+    del A
+    release()
+    return out
 
 
 def torch_csr(a, dtype=None):
