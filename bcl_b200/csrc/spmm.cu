@@ -127,49 +127,9 @@ __device__ __forceinline__ void cp_async4_nb(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
 
-// L2 eviction policies (createpolicy): streamed data (A entries, C rows:
-// touched once) goes first; the B rows most referenced by A's columns stay.
-__device__ __forceinline__ uint64_t policy_evict_first() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ uint64_t policy_evict_last() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
-  return p;
-}
-__device__ __forceinline__ uint64_t policy_evict_normal() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;\n" : "=l"(p));
-  return p;
-}
-
-__device__ __forceinline__ void cp_async16_hint(void* smem, const void* gmem, uint64_t pol) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "l"(pol)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async16_hint_nb(void* smem, const void* gmem, uint64_t pol) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "l"(pol));
-}
-__device__ __forceinline__ void cp_async4_hint_nb(void* smem, const void* gmem, uint64_t pol) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "l"(pol));
-}
-__device__ __forceinline__ uint4 ldg16_hint(const void* p, uint64_t pol) {
-  uint4 v;
-  asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;\n"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "l"(p), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ void stg16_hint(void* p, uint4 v, uint64_t pol) {
-  asm volatile("st.global.L2::cache_hint.v4.u32 [%0], {%1, %2, %3, %4}, %5;\n" ::"l"(p), "r"(v.x), "r"(v.y),
-               "r"(v.z), "r"(v.w), "l"(pol)
-               : "memory");
-}
+// B rows that many A entries reference are asked for with an L2
+// evict-last prefetch, so that they stay in L2 longer than the streamed C
+// rows (stored with the evict-first .cs operator when the hints are on).
 __device__ __forceinline__ void l2_prefetch_last(const void* p) {
   asm volatile("prefetch.global.L2::evict_last [%0];\n" ::"l"(p));
 }
@@ -197,10 +157,10 @@ struct StageLane {
 };
 
 // B-row reuse hints: deg[global B row] = how many A entries reference it;
-// rows referenced at least thr times are kept in L2 (evict_last), the rest
-// are loaded with the normal policy, and A and C (each touched once) are
-// streamed with evict_first.  deg == null: every access uses the normal
-// policy.
+// rows referenced at least thr times are prefetched into L2 with the
+// evict-last priority, the others with the normal one, and C rows (each
+// written once) are stored with the evict-first .cs operator.  deg == null:
+// no hints.
 struct RowHints {
   const int32_t* deg;
   const int32_t* thr;  // device scalar
@@ -254,8 +214,7 @@ __device__ __forceinline__ bool tiles_aligned(const DGridView& B, const DGridVie
 template <typename ST, bool GROUP, int UNROLL = kSpmmUnroll>
 __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
                                           int64_t tj, int64_t r0, int R, int c0, int W, bool vec,
-                                          const uint8_t* __restrict__ skip, const RowHints& hints, int32_t thr,
-                                          uint64_t pol_stream, uint64_t pol_hot, uint64_t pol_cold) {
+                                          const uint8_t* __restrict__ skip, const RowHints& hints, int32_t thr) {
   if (!GROUP) R = 1;
   using V = Vec<ST>;
   constexpr int VN = V::N;
@@ -280,9 +239,13 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
     if (cur < 0 || !own) return;
     ST* p = crow0 + cur * C.ld;
     if (vec) {
-      uint4 w;
-      V::store(reinterpret_cast<ST*>(&w), acc);
-      stg16_hint(p + col, w, pol_stream);
+      if (hints.deg) {  // streamed: C rows are written once
+        uint4 w;
+        V::store(reinterpret_cast<ST*>(&w), acc);
+        __stcs(reinterpret_cast<uint4*>(p + col), w);
+      } else {
+        V::store(p + col, acc);
+      }
     } else {
 #pragma unroll
       for (int x = 0; x < VN; x++)
@@ -315,14 +278,14 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
     // stage the C slices of the rows that have entries
     if (!GROUP) {
       if (vec && !staged) {
-        if (own) cp_async16_hint(cs + lane, crow0 + col, pol_stream);
+        if (own) cp_async16(cs + lane, crow0 + col);
         staged = true;
       }
     } else {
       for (int q = 0; q < R; q++) {
         const int32_t hi = __shfl_sync(kFull, aincl, q * gk + gk - 1);
         const int32_t lo = __shfl_sync(kFull, aexcl, q * gk);
-        if (vec && own && hi > lo) cp_async16_hint(cs + q * 32 + lane, crow0 + q * C.ld + col, pol_stream);
+        if (vec && own && hi > lo) cp_async16(cs + q * 32 + lane, crow0 + q * C.ld + col);
       }
     }
     const int32_t nch = (atot + 31) >> 5;
@@ -346,8 +309,8 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
         const int slot = (x % kARing) * 32 + lane;
         asrc[slot] = (uint8_t)src;
         if (e < atot) {
-          cp_async4_hint_nb(&ar[slot].x, sacol + off, pol_stream);
-          cp_async4_hint_nb(&ar[slot].y, saval + off, pol_stream);
+          cp_async4_nb(&ar[slot].x, sacol + off);
+          cp_async4_nb(&ar[slot].y, saval + off);
         }
       }
       cp_async_commit();
@@ -409,7 +372,7 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
 #pragma unroll
           for (int u = 0; u < UNROLL; u++) {
             const ST* rp = reinterpret_cast<const ST*>((uint64_t)ent[u].x | ((uint64_t)ent[u].y << 32));
-            raw[u] = ldg16_hint(rp + bcol, (ent[u].w & 0x80000000u) ? pol_hot : pol_cold);
+            raw[u] = __ldg(reinterpret_cast<const uint4*>(rp + bcol));
           }
           auto apply = [&](int u) {
             if (GROUP && (int)(ent[u].w & 0xffu) != cur) enter((int)(ent[u].w & 0xffu));
@@ -461,11 +424,7 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
            RowHints hints) {
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
-  const bool hinted = hints.deg != nullptr;
-  const int32_t thr = hinted ? __ldg(hints.thr) : 0;
-  const uint64_t pol_n = policy_evict_normal();
-  const uint64_t pol_stream = hinted ? policy_evict_first() : pol_n;
-  const uint64_t pol_hot = hinted ? policy_evict_last() : pol_n;
+  const int32_t thr = hints.deg ? __ldg(hints.thr) : 0;
   unsigned long long it = 0;
   if (lane == 0) it = atomicAdd(next_item, 1ULL);
   it = __shfl_sync(kFull, it, 0);
@@ -483,8 +442,7 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     if (r0 < C.rows_of(ti) && c0 < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
       // rows flagged long are k_spmm_long's (it takes the aligned ones)
-      spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr, hints, thr, pol_stream,
-                           pol_hot, pol_n);
+      spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr, hints, thr);
     }
     it = __shfl_sync(kFull, nx, 0);
   }
@@ -556,8 +514,7 @@ __global__ void k_spmm_find_long(SpGridView A, int long_row, int very_long_row, 
 template <typename ST>
 __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, const DGridView& B,
                                               const DGridView& C, int64_t ti, int64_t tj, int64_t r, int c0, int W,
-                                              const RowHints& hints, int32_t thr, uint64_t pol_stream,
-                                              uint64_t pol_hot, uint64_t pol_cold) {
+                                              const RowHints& hints, int32_t thr) {
   using V = Vec<ST>;
   constexpr int VN = V::N;
   const int lane = lane_id();
@@ -567,6 +524,7 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
   float acc[VN];
   if (own) V::load_c(crow + col, acc);
   const StageLane<ST> sl = stage_lane<ST>(A, B, ti, tj, r, lane, true);
+  const int pbytes = min(32 * VN, W - c0) * (int)sizeof(ST);  // this panel's bytes of a B row
   const int32_t aincl = warp_inclusive_scan(sl.alen);
   const int32_t atot = __shfl_sync(kFull, aincl, 31);
   const int32_t aexcl = aincl - sl.alen;
@@ -589,8 +547,8 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
     const int slot = x % kLongASlots;
     S.src[slot][lane] = (uint8_t)src;
     if (e < atot) {
-      cp_async4_hint_nb(&S.a[slot][lane].x, sacol + off, pol_stream);
-      cp_async4_hint_nb(&S.a[slot][lane].y, saval + off, pol_stream);
+      cp_async4_nb(&S.a[slot][lane].x, sacol + off);
+      cp_async4_nb(&S.a[slot][lane].y, saval + off);
     }
   };
   auto build = [&](int32_t x) {  // A(x) has landed
@@ -613,7 +571,9 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
     const int bslot = x % kLongBSlots, tslot = x % kLongTSlots;
     auto copy = [&](int u, const uint4& t) {
       const ST* rp = reinterpret_cast<const ST*>((uint64_t)t.x | ((uint64_t)t.y << 32));
-      cp_async16_hint_nb(&S.b[bslot][u][lane], rp + col, t.w ? pol_hot : pol_cold);
+      if (t.w && lane * 128 < pbytes)  // a hot row's lines, marked to stay in L2
+        l2_prefetch_last(reinterpret_cast<const char*>(rp + c0) + lane * 128);
+      cp_async16_nb(&S.b[bslot][u][lane], rp + col);
     };
     if (ne == 32) {
 #pragma unroll
@@ -693,11 +653,7 @@ __global__ void __launch_bounds__(kLongWarps * 32)
                 unsigned long long* __restrict__ next_item, RowHints hints) {
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   extern __shared__ __align__(16) unsigned char long_smem[];
-  const bool hinted = hints.deg != nullptr;
-  const int32_t thr = hinted ? __ldg(hints.thr) : 0;
-  const uint64_t pol_n = policy_evict_normal();
-  const uint64_t pol_stream = hinted ? policy_evict_first() : pol_n;
-  const uint64_t pol_hot = hinted ? policy_evict_last() : pol_n;
+  const int32_t thr = hints.deg ? __ldg(hints.thr) : 0;
   LongSmem& S = reinterpret_cast<LongSmem*>(long_smem)[threadIdx.x >> 5];
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
@@ -722,7 +678,7 @@ __global__ void __launch_bounds__(kLongWarps * 32)
     if (panel * PW < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
       if (vec)  // otherwise k_spmm did it element-wise
-        spmm_long_row<ST>(S, A, B, C, ti, tj, r, panel * PW, W, hints, thr, pol_stream, pol_hot, pol_n);
+        spmm_long_row<ST>(S, A, B, C, ti, tj, r, panel * PW, W, hints, thr);
     }
     it = __shfl_sync(kFull, nx, 0);
   }

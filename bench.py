@@ -205,12 +205,12 @@ def spgemm_alg_bytes(a_nnz, b_nnz, m, k, tm, tk, nnz_c, c_tiles, vsize=4):
     gn = b_nnz.shape[1]
     rows_a = np.minimum(tm, m - np.arange(gm) * tm)
     rows_b = np.minimum(tk, k - np.arange(gk) * tk)
-    tot = 0
-    for i in range(gm):
-        for j in range(gn):
-            for kk in range(gk):
-                tot += (4 + vsize) * int(a_nnz[i, kk]) + 4 * (int(rows_a[i]) + 1)
-                tot += (4 + vsize) * int(b_nnz[kk, j]) + 4 * (int(rows_b[kk]) + 1)
+    # only the tile products with both tiles nonempty are run (the stage maps
+    # skip the others on fine grids)
+    live = (a_nnz[:, None, :] > 0) & (b_nnz.T[None, :, :] > 0)          # [i, j, k]
+    a_bytes = (4 + vsize) * a_nnz.astype(np.int64) + 4 * (rows_a[:, None].astype(np.int64) + 1)   # [i, k]
+    b_bytes = (4 + vsize) * b_nnz.astype(np.int64) + 4 * (rows_b[:, None].astype(np.int64) + 1)   # [k, j]
+    tot = int((live * (a_bytes[:, None, :] + b_bytes.T[None, :, :])).sum())
     tot += (4 + vsize) * nnz_c + 4 * c_tiles * (tm + 1)
     return tot
 
