@@ -483,16 +483,22 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
                            int32_t* __restrict__ heavy_list, int32_t* __restrict__ vheavy_list,
                            int32_t* __restrict__ counters, unsigned long long* __restrict__ products,
                            int heavy_min_cols, int light_ub, float* __restrict__ X,
-                           int32_t* __restrict__ ub_out, unsigned long long* __restrict__ queue) {
+                           int32_t* __restrict__ ub_out, unsigned long long* __restrict__ queue, int grab) {
   const int lane = lane_id();
   unsigned long long mine = 0;
-  // rows from a device counter, the next grab in flight while a row is walked
-  unsigned long long it = 0;
-  if (lane == 0) it = atomicAdd(queue, 1ULL);
-  it = __shfl_sync(kFull, it, 0);
-  while (it < (unsigned long long)g.n_row_items) {
+  // rows from a device counter, `grab` consecutive rows per atomic (one
+  // atomic per row serialises on the counter when a fine grid has hundreds
+  // of millions of mostly empty row items); the next grab is in flight while
+  // the current rows are walked
+  const unsigned long long n_rows = (unsigned long long)g.n_row_items;
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(queue, (unsigned long long)grab);
+  base = __shfl_sync(kFull, base, 0);
+  while (base < n_rows) {
     unsigned long long nx = 0;
-    if (lane == 0) nx = atomicAdd(queue, 1ULL);
+    if (lane == 0) nx = atomicAdd(queue, (unsigned long long)grab);
+    const unsigned long long end = min(base + (unsigned long long)grab, n_rows);
+    for (unsigned long long it = base; it < end; it++) {
     const int64_t ri = (int64_t)it;
     const RowInfo x = decode_row(g, ri);
     int64_t tot = 0, annz = 0;
@@ -554,7 +560,8 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
       else
         vheavy_list[atomicAdd(&counters[3], 1)] = (int32_t)ri;
     }
-    it = __shfl_sync(kFull, nx, 0);
+    }
+    base = __shfl_sync(kFull, nx, 0);
   }
   if (lane == 0 && mine) atomicAdd(products, mine);
 }
@@ -595,17 +602,19 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
     k_symbolic(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
                const int32_t* __restrict__ heavy_list, int n_light, int n_heavy, int n_vheavy,
                int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
-               unsigned long long* __restrict__ queue) {
+               unsigned long long* __restrict__ queue, int grab) {
   __shared__ uint32_t bm_all[kWarpsSym][kMaxWords];
   uint32_t* bm = bm_all[threadIdx.x >> 5];
   const int lane = lane_id();
   const unsigned long long n_items = (unsigned long long)((int64_t)n_light + n_heavy - n_vheavy);
-  unsigned long long it = 0;
-  if (lane == 0) it = atomicAdd(queue, 1ULL);
-  it = __shfl_sync(kFull, it, 0);
-  while (it < n_items) {
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(queue, (unsigned long long)grab);
+  base = __shfl_sync(kFull, base, 0);
+  while (base < n_items) {
     unsigned long long nx = 0;
-    if (lane == 0) nx = atomicAdd(queue, 1ULL);
+    if (lane == 0) nx = atomicAdd(queue, (unsigned long long)grab);
+    const unsigned long long end = min(base + (unsigned long long)grab, n_items);
+    for (unsigned long long it = base; it < end; it++) {
     const int64_t idx = n_vheavy + (int64_t)it;
     const bool heavy = idx < n_heavy;
     const int64_t ri = heavy ? heavy_list[idx] : light_list[idx - n_heavy];
@@ -625,7 +634,8 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
     cnt = warp_sum(cnt);
     if (lane == 0) row_count[ri] = cnt;
     __syncwarp();
-    it = __shfl_sync(kFull, nx, 0);
+    }
+    base = __shfl_sync(kFull, nx, 0);
   }
 }
 
@@ -1354,6 +1364,14 @@ static int check_grids(const bclx_spgrid_t* a, const bclx_spgrid_t* b, const bcl
   return BCLX_OK;
 }
 
+// Rows a warp takes from a device counter at a time: about 32 grabs per
+// resident warp over the pass, at least 1 and at most `cap`.
+static int queue_grab(Context* ctx, int64_t rows, int warps_per_block, int blocks_per_sm, int cap) {
+  const int64_t warps = (int64_t)ctx->num_sms * blocks_per_sm * warps_per_block;
+  const int64_t g = rows / (warps * 32);
+  return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
 static unsigned grid_for(Context* ctx, int64_t work_warps, int warps_per_block, int blocks_per_sm) {
   int64_t want = (work_warps + warps_per_block - 1) / warps_per_block;
   int64_t cap = (int64_t)ctx->num_sms * blocks_per_sm;
@@ -1385,7 +1403,7 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
     BCLX_CK(cudaMemsetAsync(P->queue, 0, sizeof(unsigned long long), ctx->stream));
     k_symbolic<<<grid_for(ctx, rows, kWarpsSym, 8), kWarpsSym * 32, 0, ctx->stream>>>(
         A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, (int)P->n_heavy, (int)P->n_vheavy,
-        P->row_count, P->heavy_bitmaps, P->hbm_words, P->queue);
+        P->row_count, P->heavy_bitmaps, P->hbm_words, P->queue, queue_grab(ctx, rows, kWarpsSym, 8, 8));
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1523,7 +1541,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, heavy_min_cols, P->light_ub_max,
-        nullptr, nullptr, P->queue + 1);
+        nullptr, nullptr, P->queue + 1, queue_grab(ctx, nri, 8, 16, 64));
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1971,7 +1989,7 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
   BCLX_CK(cudaMemsetAsync(P.queue + 1, 0, sizeof(unsigned long long), ctx->stream));
   k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
       A, B, g, P.light_list, P.heavy_tmp, P.vheavy_list, P.counters, P.products_dev, 8192 + 1, kLightUb, nullptr, nullptr,
-      P.queue + 1);
+      P.queue + 1, queue_grab(ctx, nri, 8, 16, 64));
   note_launch();
   BCLX_CK_LAUNCH();
   int32_t cnts[4];
@@ -2138,7 +2156,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, tuning(ctx, BCLX_TUNE_WIDE_LIGHT) ? INT_MAX : 8192 + 1,
         (int)tuning(ctx, BCLX_TUNE_LIGHT_UB), P->feat, P->ub,
-        P->queue + 1);
+        P->queue + 1, queue_grab(ctx, nri, 8, 16, 64));
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -2430,7 +2448,8 @@ int bclx_spgemm_row_features(bclx_context_t c, const bclx_spgrid_t* a, const bcl
     cudaMemsetAsync(cnt, 0, 4 * sizeof(int32_t), ctx->stream);
     cudaMemsetAsync(prod, 0, 2 * sizeof(unsigned long long), ctx->stream);
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
-        make_view(*a), make_view(*b), g, lists, lists + nri, lists + 2 * nri, cnt, prod, 8192 + 1, kLightUb, X, ub, prod + 1);
+        make_view(*a), make_view(*b), g, lists, lists + nri, lists + 2 * nri, cnt, prod, 8192 + 1, kLightUb, X, ub, prod + 1,
+        queue_grab(ctx, nri, 8, 16, 64));
     note_launch();
     if (cudaGetLastError() != cudaSuccess) rc = BCLX_ERR_CUDA;
   }

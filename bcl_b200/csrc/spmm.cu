@@ -421,16 +421,19 @@ template <typename ST, bool GROUP>
 __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int R, int64_t ngroups,
            int row_align_ok, const uint8_t* __restrict__ long_flag, unsigned long long* __restrict__ next_item,
-           RowHints hints) {
+           RowHints hints, int grab) {
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
   const int32_t thr = hints.deg ? __ldg(hints.thr) : 0;
-  unsigned long long it = 0;
-  if (lane == 0) it = atomicAdd(next_item, 1ULL);
-  it = __shfl_sync(kFull, it, 0);
-  while (it < (unsigned long long)n_items) {
+  // `grab` consecutive items per atomic on the shared counter
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(next_item, (unsigned long long)grab);
+  base = __shfl_sync(kFull, base, 0);
+  while (base < (unsigned long long)n_items) {
     unsigned long long nx = 0;
-    if (lane == 0) nx = atomicAdd(next_item, 1ULL);
+    if (lane == 0) nx = atomicAdd(next_item, (unsigned long long)grab);
+    const unsigned long long end = min(base + (unsigned long long)grab, (unsigned long long)n_items);
+    for (unsigned long long it = base; it < end; it++) {
     const int64_t item = (int64_t)it;
     const int64_t rg = item / npanels;
     const int panel = (int)(item - rg * npanels);
@@ -444,7 +447,8 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
       // rows flagged long are k_spmm_long's (it takes the aligned ones)
       spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr, hints, thr);
     }
-    it = __shfl_sync(kFull, nx, 0);
+    }
+    base = __shfl_sync(kFull, nx, 0);
   }
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
 }
@@ -844,12 +848,15 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   cfg.attrs = attr;
   cfg.numAttrs = long_path ? 1 : 0;
   const uint8_t* lflag = flag;
+  // items per grab: about 16 grabs per resident warp, 1 to 4
+  const int64_t gwarps = (int64_t)grid * kSpmmWarps;
+  const int sgrab = (int)std::max<int64_t>(1, std::min<int64_t>(4, n_items / (gwarps * 16)));
   if (R > 1)
     BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true>, A, B, C, n_items, npanels, R, ngroups, align_ok, lflag, ctr,
-                               hints));
+                               hints, sgrab));
   else
     BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, false>, A, B, C, n_items, npanels, 1, ngroups, align_ok, lflag, ctr,
-                               hints));
+                               hints, sgrab));
   note_launch();
   BCLX_CK_LAUNCH();
   if (long_path) {
