@@ -1024,24 +1024,23 @@ __global__ void __launch_bounds__(256) k_heavy_block_ub(SpGridView A, SpGridView
       const int64_t k = (stage_at(g, x.ti, x.tj, si) + x.rot) % g.gk;
       const bclx_csr_t At = A.tile(x.ti, k);
       const int32_t a0 = __ldg(At.row_ptr + x.r), a1 = __ldg(At.row_ptr + x.r + 1);
-      if (tab) {
-        const int32_t* trows = tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1);
-        for (int32_t p = a0 + lane; p < a1; p += 32) {
-          const int32_t* trow = trows + (int64_t)__ldg(At.col_ind + p) * (g.nfb + 1);
-          int32_t prev = __ldg(trow);
+      // per A entry: a B row shorter than the block count is counted column
+      // by column, a longer one from the B-row table's block starts
+      const bclx_csr_t Bt = B.tile(k, x.tj);
+      const int32_t* trows = tab ? tab + (k * g.gn + x.tj) * g.tk * (g.nfb + 1) : nullptr;
+      for (int32_t p = a0 + lane; p < a1; p += 32) {
+        const int32_t kc = __ldg(At.col_ind + p);
+        const int32_t b0 = __ldg(Bt.row_ptr + kc), b1 = __ldg(Bt.row_ptr + kc + 1);
+        if (!trows || b1 - b0 <= nfb) {
+          for (int32_t q = b0; q < b1; q++) atomicAdd(&cnt[__ldg(Bt.col_ind + q) / kFineCols], 1);
+        } else {
+          const int32_t* trow = trows + (int64_t)kc * (g.nfb + 1);
+          int32_t prev = b0;
           for (int b = 0; b < nfb; b++) {
             const int32_t nx = __ldg(trow + b + 1);
             if (nx != prev) atomicAdd(&cnt[b], nx - prev);
             prev = nx;
           }
-        }
-      } else {
-        // no table: count the B row's columns per block
-        const bclx_csr_t Bt = B.tile(k, x.tj);
-        for (int32_t p = a0 + lane; p < a1; p += 32) {
-          const int32_t kc = __ldg(At.col_ind + p);
-          const int32_t b1 = __ldg(Bt.row_ptr + kc + 1);
-          for (int32_t q = __ldg(Bt.row_ptr + kc); q < b1; q++) atomicAdd(&cnt[__ldg(Bt.col_ind + q) / kFineCols], 1);
         }
       }
     }
