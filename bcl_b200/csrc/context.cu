@@ -27,7 +27,7 @@ static int64_t tuning_default(const Context* ctx, int key) {
     case BCLX_TUNE_SPMM_LONG_BLOCKS: return env_or("BCLX_SPMM_LONG_BLOCKS", ctx->num_sms / 2);
     case BCLX_TUNE_SPMM_HOT_PERMILLE: {
       const char* e = std::getenv("BCLX_SPMM_HOT_FRACTION");
-      return e && *e ? (int64_t)(std::atof(e) * 1000.0 + 0.5) : 500;
+      return e && *e ? (int64_t)(std::atof(e) * 1000.0 + 0.5) : 0;
     }
     case BCLX_TUNE_ITEM_OUTPUTS: return env_or("BCLX_ITEM_OUTPUTS", 512);
     case BCLX_TUNE_WIDE_LIGHT: return env_or("BCLX_WIDE_LIGHT", 0);

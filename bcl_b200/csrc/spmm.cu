@@ -758,9 +758,10 @@ __global__ void k_deg_threshold(const unsigned long long* __restrict__ hist, lon
   *thr = (int32_t)(t < 2 ? 2 : (t > INT32_MAX ? INT32_MAX : t));
 }
 
-// Hints pay when B does not fit in L2 (otherwise every row stays anyway):
-// BCLX_TUNE_SPMM_HOT_PERMILLE of L2 goes to the most referenced B rows
-// (default 500; 0 turns the hints off).
+// Hints can only pay when B does not fit in L2 (otherwise every row stays
+// anyway): BCLX_TUNE_SPMM_HOT_PERMILLE of L2 goes to the most referenced B
+// rows.  Off by default: on R-MAT s21 x 256 they measured slower (FP32 6.2
+// against 5.2 ms with them off).
 static double spmm_hot_fraction(const Context* ctx) {
   return (double)tuning(ctx, BCLX_TUNE_SPMM_HOT_PERMILLE) / 1000.0;
 }
@@ -848,9 +849,9 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   cfg.attrs = attr;
   cfg.numAttrs = long_path ? 1 : 0;
   const uint8_t* lflag = flag;
-  // items per grab: about 16 grabs per resident warp, 1 to 4
-  const int64_t gwarps = (int64_t)grid * kSpmmWarps;
-  const int sgrab = (int)std::max<int64_t>(1, std::min<int64_t>(4, n_items / (gwarps * 16)));
+  // one item per grab: item costs vary by orders of magnitude on power-law
+  // matrices, and larger grabs measured slower (R-MAT s21 x 256)
+  const int sgrab = 1;
   if (R > 1)
     BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true>, A, B, C, n_items, npanels, R, ngroups, align_ok, lflag, ctr,
                                hints, sgrab));
