@@ -5,8 +5,8 @@ each candidate runs the whole product), then the numeric pass's plan
 parameters (work items a warp takes from the device queue at a time, blocks
 per SM, the B-segment length from which a segment is walked lane-parallel),
 grid-searched on one plan.  SpMM: rows per warp item, the long-row
-threshold, the long-row kernel's block count and the share of L2 kept for
-the most referenced B rows, by coordinate descent (one knob at a time, the
+threshold, the long-row kernel's block count and the schedule of the
+long-row and short-row kernels, by coordinate descent (one knob at a time, the
 others at their best so far).  The learned product: the outputs aimed at per
 heavy item.
 
@@ -37,7 +37,7 @@ SPMM_CANDIDATES = {
     "spmm_rows": (0, 1, 2, 4),
     "spmm_long_row": (512, 1024, 2048, 4096),
     "spmm_long_blocks": (37, 74, 111),
-    "spmm_hot_permille": (0, 250, 500, 700),
+    "spmm_schedule": (0, 1),
 }
 LEARN_TARGETS = (256, 320, 384)
 

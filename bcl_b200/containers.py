@@ -67,7 +67,7 @@ class Context:
     TUNING_KEYS = {"light_ub": _lib.TUNE_LIGHT_UB, "learn_target": _lib.TUNE_LEARN_TARGET,
                    "btable_max_bytes": _lib.TUNE_BTABLE_MAX_BYTES, "spmm_rows": _lib.TUNE_SPMM_ROWS,
                    "spmm_long_row": _lib.TUNE_SPMM_LONG_ROW, "spmm_long_blocks": _lib.TUNE_SPMM_LONG_BLOCKS,
-                   "spmm_hot_permille": _lib.TUNE_SPMM_HOT_PERMILLE, "item_outputs": _lib.TUNE_ITEM_OUTPUTS,
+                   "spmm_schedule": _lib.TUNE_SPMM_SCHEDULE, "item_outputs": _lib.TUNE_ITEM_OUTPUTS,
                    "wide_light": _lib.TUNE_WIDE_LIGHT}
 
     def set_tuning(self, **knobs) -> None:
@@ -989,7 +989,7 @@ def spgemm_plain(a: SPMatrix, b: SPMatrix) -> SPMatrix:
 def spmm(a: SPMatrix, b: DMatrix, c: DMatrix, tuning=None) -> None:
     """C += A * B over tile grids in one launch (BCL::gemm(SPMatrix, DMatrix,
     DMatrix&), spgemm.hpp:153-179).  ``tuning``: a dict of SpMM context
-    knobs (spmm_rows, spmm_long_row, spmm_long_blocks, spmm_hot_permille) or
+    knobs (spmm_rows, spmm_long_row, spmm_long_blocks, spmm_schedule) or
     "auto" for the autotuner's cached choice; results do not depend on it."""
     if a.n != b.m or a.m != c.m or b.n != c.n:
         raise RuntimeError("BCL::gemm: shape mismatch")

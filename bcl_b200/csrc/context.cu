@@ -25,10 +25,7 @@ static int64_t tuning_default(const Context* ctx, int key) {
     case BCLX_TUNE_SPMM_ROWS: return env_or("BCLX_SPMM_ROWS", 0);
     case BCLX_TUNE_SPMM_LONG_ROW: return 1024;
     case BCLX_TUNE_SPMM_LONG_BLOCKS: return env_or("BCLX_SPMM_LONG_BLOCKS", ctx->num_sms / 2);
-    case BCLX_TUNE_SPMM_HOT_PERMILLE: {
-      const char* e = std::getenv("BCLX_SPMM_HOT_FRACTION");
-      return e && *e ? (int64_t)(std::atof(e) * 1000.0 + 0.5) : 0;
-    }
+    case BCLX_TUNE_SPMM_SCHEDULE: return env_or("BCLX_SPMM_SCHEDULE", 0);
     case BCLX_TUNE_ITEM_OUTPUTS: return env_or("BCLX_ITEM_OUTPUTS", 512);
     case BCLX_TUNE_WIDE_LIGHT: return env_or("BCLX_WIDE_LIGHT", 0);
     default: return 0;
@@ -43,7 +40,7 @@ static bool tuning_in_range(const Context* ctx, int key, int64_t v) {
     case BCLX_TUNE_SPMM_ROWS: return v == 0 || v == 1 || v == 2 || v == 4;
     case BCLX_TUNE_SPMM_LONG_ROW: return v >= 64 && v <= INT32_MAX;
     case BCLX_TUNE_SPMM_LONG_BLOCKS: return v >= 1 && v <= ctx->num_sms;
-    case BCLX_TUNE_SPMM_HOT_PERMILLE: return v <= 900;
+    case BCLX_TUNE_SPMM_SCHEDULE: return v == 0 || v == 1;
     case BCLX_TUNE_ITEM_OUTPUTS: return v == 512 || v == 1024;
     case BCLX_TUNE_WIDE_LIGHT: return v == 0 || v == 1;
     default: return false;

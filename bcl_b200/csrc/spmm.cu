@@ -127,13 +127,6 @@ __device__ __forceinline__ void cp_async4_nb(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
 
-// B rows that many A entries reference are asked for with an L2
-// evict-last prefetch, so that they stay in L2 longer than the streamed C
-// rows (stored with the evict-first .cs operator when the hints are on).
-__device__ __forceinline__ void l2_prefetch_last(const void* p) {
-  asm volatile("prefetch.global.L2::evict_last [%0];\n" ::"l"(p));
-}
-
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
 template <int N>
@@ -144,32 +137,20 @@ __device__ __forceinline__ void cp_async_wait_group() {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // One stage of one row of C tile (ti, tj): for stage slot kk of the
-// reference's rotated order k = (k_ + ti + tj) mod gk (or k = kk when the B
-// view asks for ascending order), the A-row segment of row r in tile (ti, k)
-// and the B tile (k, tj).  Empty when !valid.
+// reference's rotated order k = (k_ + ti + tj) mod gk, the A-row segment of
+// row r in tile (ti, k) and the B tile (k, tj).  Empty when !valid.
 template <typename ST>
 struct StageLane {
   int32_t alen;
   const int32_t* acol;
   const float* aval;
   const ST* bt;
-  int64_t kbase;  // global index of the B tile's first row (k * tile height)
-};
-
-// B-row reuse hints: deg[global B row] = how many A entries reference it;
-// rows referenced at least thr times are prefetched into L2 with the
-// evict-last priority, the others with the normal one, and C rows (each
-// written once) are stored with the evict-first .cs operator.  deg == null:
-// no hints.
-struct RowHints {
-  const int32_t* deg;
-  const int32_t* thr;  // device scalar
 };
 
 template <typename ST>
 __device__ __forceinline__ StageLane<ST> stage_lane(const SpGridView& A, const DGridView& B, int64_t ti, int64_t tj,
                                                     int64_t r, int64_t kk, bool valid) {
-  StageLane<ST> s{0, nullptr, nullptr, nullptr, 0};
+  StageLane<ST> s{0, nullptr, nullptr, nullptr};
   const int64_t gk = A.gn;
   if (valid && kk < gk) {
     const int64_t k = B.natural_order ? kk : (kk + ti + tj) % gk;
@@ -179,7 +160,6 @@ __device__ __forceinline__ StageLane<ST> stage_lane(const SpGridView& A, const D
     s.acol = At.col_ind + as;
     s.aval = reinterpret_cast<const float*>(At.vals) + as;
     s.bt = reinterpret_cast<const ST*>(B.tile(k, tj));
-    s.kbase = k * A.tn;
   }
   return s;
 }
@@ -214,7 +194,7 @@ __device__ __forceinline__ bool tiles_aligned(const DGridView& B, const DGridVie
 template <typename ST, bool GROUP, int UNROLL = kSpmmUnroll>
 __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
                                           int64_t tj, int64_t r0, int R, int c0, int W, bool vec,
-                                          const uint8_t* __restrict__ skip, const RowHints& hints, int32_t thr) {
+                                          const uint8_t* __restrict__ skip) {
   if (!GROUP) R = 1;
   using V = Vec<ST>;
   constexpr int VN = V::N;
@@ -239,13 +219,7 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
     if (cur < 0 || !own) return;
     ST* p = crow0 + cur * C.ld;
     if (vec) {
-      if (hints.deg) {  // streamed: C rows are written once
-        uint4 w;
-        V::store(reinterpret_cast<ST*>(&w), acc);
-        __stcs(reinterpret_cast<uint4*>(p + col), w);
-      } else {
-        V::store(p + col, acc);
-      }
+      V::store(p + col, acc);
     } else {
 #pragma unroll
       for (int x = 0; x < VN; x++)
@@ -323,31 +297,21 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
       const int slot = (x % kARing) * 32 + lane;
       const int src = asrc[slot];
       const ST* sbt = reinterpret_cast<const ST*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.bt), src));
-      const int64_t kb = (int64_t)__shfl_sync(kFull, (unsigned long long)sl.kbase, src);
       const int32_t e = x * 32 + lane;
       float v = 0.f;
       const ST* brow = sbt;
-      bool hot = false;
       if (e < atot) {
         const uint2 a = ar[slot];
         v = __uint_as_float(a.y);
         brow = sbt + (int64_t)(int32_t)a.x * B.ld;
-        if (hints.deg) hot = __ldg(hints.deg + kb + (int32_t)a.x) >= thr;
       }
       const ST* last = reinterpret_cast<const ST*>(
           __shfl_sync(kFull, reinterpret_cast<unsigned long long>(brow), (atot - 1) & 31));
       if (e >= atot) brow = last;
       const uint64_t pa = reinterpret_cast<uint64_t>(brow);
-      tb[(x % kTabBufs) * 32 + lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), __float_as_uint(v),
-                                                  (GROUP ? (uint32_t)(src / gk) : 0u) | (hot ? 0x80000000u : 0u));
-      if (vec && e < atot) {
-        if (hot) {
-          const char* q = reinterpret_cast<const char*>(brow + c0);
-          for (int o = 0; o < pbytes; o += 128) l2_prefetch_last(q + o);
-        } else {
-          l2_prefetch_slice(brow + c0, pbytes);
-        }
-      }
+      tb[(x % kTabBufs) * 32 + lane] =
+          make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), __float_as_uint(v), GROUP ? (uint32_t)(src / gk) : 0u);
+      l2_prefetch_slice(vec && e < atot ? brow + c0 : nullptr, pbytes);
     };
     // pipeline fill: chunks 0 .. kARing-1 staged, 0 and 1 built, kARing staged
     for (int x = 0; x < kARing; x++) issue_a(x);
@@ -375,7 +339,7 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
             raw[u] = __ldg(reinterpret_cast<const uint4*>(rp + bcol));
           }
           auto apply = [&](int u) {
-            if (GROUP && (int)(ent[u].w & 0xffu) != cur) enter((int)(ent[u].w & 0xffu));
+            if (GROUP && (int)ent[u].w != cur) enter((int)ent[u].w);
             float b[VN];
             V::unpack_raw(raw[u], b);
             const float vs = __uint_as_float(ent[u].z);
@@ -394,7 +358,7 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
       } else {
         for (int u = 0; u < ne; u++) {
           const uint4 en = t[u];
-          if (GROUP && (int)(en.w & 0xffu) != cur) enter((int)(en.w & 0xffu));
+          if (GROUP && (int)en.w != cur) enter((int)en.w);
           const ST* rp = reinterpret_cast<const ST*>((uint64_t)en.x | ((uint64_t)en.y << 32));
           const float vs = __uint_as_float(en.z);
 #pragma unroll
@@ -412,28 +376,18 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
 // flight while the current item runs), so warps that draw short rows take
 // more of them: the cost of a (row group, panel) item varies by orders of
 // magnitude on power-law matrices.
-//
-// Launched after k_spmm_long as its programmatic dependent (the long-row
-// blocks are placed on their SMs first); before exiting, every block waits
-// for k_spmm_long to finish (griddepcontrol.wait), so later work in the
-// stream sees both kernels done.  Launched normally, the wait returns at once.
 template <typename ST, bool GROUP>
 __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int R, int64_t ngroups,
-           int row_align_ok, const uint8_t* __restrict__ long_flag, unsigned long long* __restrict__ next_item,
-           RowHints hints, int grab) {
+           int row_align_ok, const uint8_t* __restrict__ long_flag, unsigned long long* __restrict__ next_item) {
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
-  const int32_t thr = hints.deg ? __ldg(hints.thr) : 0;
-  // `grab` consecutive items per atomic on the shared counter
-  unsigned long long base = 0;
-  if (lane == 0) base = atomicAdd(next_item, (unsigned long long)grab);
-  base = __shfl_sync(kFull, base, 0);
-  while (base < (unsigned long long)n_items) {
+  unsigned long long it = 0;
+  if (lane == 0) it = atomicAdd(next_item, 1ULL);
+  it = __shfl_sync(kFull, it, 0);
+  while (it < (unsigned long long)n_items) {
     unsigned long long nx = 0;
-    if (lane == 0) nx = atomicAdd(next_item, (unsigned long long)grab);
-    const unsigned long long end = min(base + (unsigned long long)grab, (unsigned long long)n_items);
-    for (unsigned long long it = base; it < end; it++) {
+    if (lane == 0) nx = atomicAdd(next_item, 1ULL);
     const int64_t item = (int64_t)it;
     const int64_t rg = item / npanels;
     const int panel = (int)(item - rg * npanels);
@@ -445,11 +399,12 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     if (r0 < C.rows_of(ti) && c0 < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
       // rows flagged long are k_spmm_long's (it takes the aligned ones)
-      spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr, hints, thr);
+      spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr);
     }
-    }
-    base = __shfl_sync(kFull, nx, 0);
+    it = __shfl_sync(kFull, nx, 0);
   }
+  // launched as k_spmm_long's programmatic dependent: finish only after it
+  // (a normal launch returns here at once)
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
 }
 
@@ -462,15 +417,15 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
 // (row, C tile column, panel), with the B-row slices themselves copied into
 // shared memory by cp.async two chunks (64 entries) ahead: the loads in
 // flight cost no registers, and a chunk's multiply-adds read shared memory.
-// Rows of 8 times the long-row threshold or more are listed first, so that the
-// longest chains start first.
+// Rows of 8 times the long-row threshold or more are listed first, so that
+// the longest chains start first.
 
 constexpr int kLongWarps = 4;
 constexpr int kLongBSlots = 3;  // chunks of B slices per warp: applied, in flight, being issued
 constexpr int kLongTSlots = 3;  // chunks of table entries per warp (with the B slices)
 constexpr int kLongASlots = 6;  // chunks of staged A entries per warp
 // A row is long from BCLX_TUNE_SPMM_LONG_ROW entries over all stages (1024 by
-// default); rows of 8 times that are listed at the front.
+// default).
 constexpr int64_t kSpmmLongMinRows = 65536;  // smaller products do not use the long-row path
 
 struct LongSmem {
@@ -517,8 +472,7 @@ __global__ void k_spmm_find_long(SpGridView A, int long_row, int very_long_row, 
 // group two steps back.  The stages are at most 32 (one lane each).
 template <typename ST>
 __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, const DGridView& B,
-                                              const DGridView& C, int64_t ti, int64_t tj, int64_t r, int c0, int W,
-                                              const RowHints& hints, int32_t thr) {
+                                              const DGridView& C, int64_t ti, int64_t tj, int64_t r, int c0, int W) {
   using V = Vec<ST>;
   constexpr int VN = V::N;
   const int lane = lane_id();
@@ -528,7 +482,6 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
   float acc[VN];
   if (own) V::load_c(crow + col, acc);
   const StageLane<ST> sl = stage_lane<ST>(A, B, ti, tj, r, lane, true);
-  const int pbytes = min(32 * VN, W - c0) * (int)sizeof(ST);  // this panel's bytes of a B row
   const int32_t aincl = warp_inclusive_scan(sl.alen);
   const int32_t atot = __shfl_sync(kFull, aincl, 31);
   const int32_t aexcl = aincl - sl.alen;
@@ -560,13 +513,11 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
     const int slot = x % kLongASlots;
     const int src = S.src[slot][lane];
     const ST* sbt = reinterpret_cast<const ST*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(sl.bt), src));
-    const int64_t kb = (int64_t)__shfl_sync(kFull, (unsigned long long)sl.kbase, src);
     const int32_t e = x * 32 + lane;
     if (e < atot) {
       const uint2 a = S.a[slot][lane];
       const uint64_t pa = reinterpret_cast<uint64_t>(sbt + (int64_t)(int32_t)a.x * B.ld);
-      const bool hot = hints.deg && __ldg(hints.deg + kb + (int32_t)a.x) >= thr;
-      S.tab[x % kLongTSlots][lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), a.y, hot ? 1u : 0u);
+      S.tab[x % kLongTSlots][lane] = make_uint4((uint32_t)pa, (uint32_t)(pa >> 32), a.y, 0u);
     }
   };
   auto issue_b = [&](int32_t x) {  // table of chunk x built, then a __syncwarp
@@ -575,8 +526,6 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
     const int bslot = x % kLongBSlots, tslot = x % kLongTSlots;
     auto copy = [&](int u, const uint4& t) {
       const ST* rp = reinterpret_cast<const ST*>((uint64_t)t.x | ((uint64_t)t.y << 32));
-      if (t.w && lane * 128 < pbytes)  // a hot row's lines, marked to stay in L2
-        l2_prefetch_last(reinterpret_cast<const char*>(rp + c0) + lane * 128);
       cp_async16_nb(&S.b[bslot][u][lane], rp + col);
     };
     if (ne == 32) {
@@ -646,18 +595,15 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
 }
 
 // Items (listed row, C tile column, panel), a row's items consecutive, taken
-// from a device counter in list order.
-// Every block, once placed, lets k_spmm (its programmatic dependent) launch:
-// the long-row blocks each need a whole SM's shared memory, so they take
-// their SMs before k_spmm's blocks fill the GPU.
+// from a device counter in list order.  Every block, once placed, lets a
+// programmatic dependent (k_spmm under the dependent-launch schedule) launch.
 template <typename ST>
 __global__ void __launch_bounds__(kLongWarps * 32)
     k_spmm_long(SpGridView A, DGridView B, DGridView C, const int64_t* __restrict__ list,
                 const int32_t* __restrict__ count, int npanels, int row_align_ok,
-                unsigned long long* __restrict__ next_item, RowHints hints) {
+                unsigned long long* __restrict__ next_item) {
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   extern __shared__ __align__(16) unsigned char long_smem[];
-  const int32_t thr = hints.deg ? __ldg(hints.thr) : 0;
   LongSmem& S = reinterpret_cast<LongSmem*>(long_smem)[threadIdx.x >> 5];
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
@@ -681,10 +627,26 @@ __global__ void __launch_bounds__(kLongWarps * 32)
     const int W = (int)C.cols_of(tj);
     if (panel * PW < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
-      if (vec)  // otherwise k_spmm did it element-wise
-        spmm_long_row<ST>(S, A, B, C, ti, tj, r, panel * PW, W, hints, thr);
+      if (vec) spmm_long_row<ST>(S, A, B, C, ti, tj, r, panel * PW, W);  // otherwise k_spmm did it element-wise
     }
     it = __shfl_sync(kFull, nx, 0);
+  }
+}
+
+// Launch delay of the short-row kernel under the side-stream schedule: a
+// one-warp kernel on the main stream that returns after `ns` (global timer,
+// bounded by an iteration cap; it waits for nothing), so that the long-row
+// blocks, which each need a whole SM's shared memory, are placed first.
+constexpr unsigned kLongHeadStartNs = 4000;
+
+__global__ void k_spmm_launch_delay(unsigned ns) {
+  uint64_t t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (int i = 0; i < 4096; i++) {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 >= ns) break;
+    __nanosleep(256);
   }
 }
 
@@ -713,61 +675,15 @@ static int spmm_rows_per_item(const Context* ctx, const DGridView& C, int64_t gk
   return r;
 }
 
-// ---- B-row reuse hints --------------------------------------------------------
-
-constexpr int kDegBins = 32;
-
-// deg[k * tile width + c] counts the A entries of column c of tile column k
-// (the B row each one reads).
-__global__ void k_col_degree(SpGridView A, int32_t* __restrict__ deg) {
-  const int64_t ntiles = A.gm * A.gn;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t t = 0; t < ntiles; t++) {
-    const bclx_csr_t At = A.tile(t / A.gn, t % A.gn);
-    int32_t* d = deg + (t % A.gn) * A.tn;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < At.nnz; e += stride)
-      atomicAdd(d + __ldg(At.col_ind + e), 1);
-  }
-}
-
-// Rows per power-of-two degree bin (bin b: degrees in [2^b, 2^(b+1))).
-__global__ void k_deg_hist(const int32_t* __restrict__ deg, int64_t n, unsigned long long* __restrict__ hist) {
-  __shared__ unsigned int h[kDegBins];
-  if (threadIdx.x < kDegBins) h[threadIdx.x] = 0;
-  __syncthreads();
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t d = __ldg(deg + c);
-    if (d > 0) atomicAdd(&h[31 - __clz(d)], 1u);
-  }
-  __syncthreads();
-  if (threadIdx.x < kDegBins && h[threadIdx.x]) atomicAdd(hist + threadIdx.x, (unsigned long long)h[threadIdx.x]);
-}
-
-// The degree threshold: the most referenced rows, whole bins from the top,
-// as many as fit in budget_rows, and never rows read only once.
-__global__ void k_deg_threshold(const unsigned long long* __restrict__ hist, long long budget_rows,
-                                int32_t* __restrict__ thr) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  unsigned long long cum = 0;
-  int b = kDegBins - 1;
-  for (; b >= 0; b--) {
-    if (cum + hist[b] > (unsigned long long)budget_rows) break;
-    cum += hist[b];
-  }
-  const long long t = b < 0 ? 1 : (1ll << (b + 1));
-  *thr = (int32_t)(t < 2 ? 2 : (t > INT32_MAX ? INT32_MAX : t));
-}
-
-// Hints can only pay when B does not fit in L2 (otherwise every row stays
-// anyway): BCLX_TUNE_SPMM_HOT_PERMILLE of L2 goes to the most referenced B
-// rows.  Off by default: on R-MAT s21 x 256 they measured slower (FP32 6.2
-// against 5.2 ms with them off).
-static double spmm_hot_fraction(const Context* ctx) {
-  return (double)tuning(ctx, BCLX_TUNE_SPMM_HOT_PERMILLE) / 1000.0;
-}
-
-// ---- launch --------------------------------------------------------------------
-
+// Two schedules of the long-row and short-row kernels (BCLX_TUNE_SPMM_SCHEDULE):
+//  0 (default): the long rows on the context's side stream at the highest
+//    priority; k_spmm on the main stream after the list is ready and a
+//    4-microsecond launch delay, so the long-row blocks take their SMs first;
+//  1: one stream; k_spmm launched as k_spmm_long's programmatic dependent
+//    (it launches once every long-row block has started, and finishes only
+//    after k_spmm_long).
+// Measured on R-MAT s21 x 256 (one B200): schedule 0 4.14 ms FP32 / 2.45 ms
+// BF16, schedule 1 4.63 / 3.45 ms.
 template <typename ST>
 static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, const DGridView& C, int align_ok) {
   constexpr int VN = Vec<ST>::N;
@@ -781,63 +697,44 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   const int64_t arows = A.gm * A.tm;
   const bool long_path = align_ok && A.gn <= 32 && arows >= spmm_long_min_rows();
   const int long_row = (int)tuning(ctx, BCLX_TUNE_SPMM_LONG_ROW);
+  const bool dependent = tuning(ctx, BCLX_TUNE_SPMM_SCHEDULE) == 1;
   // counters: [0] k_spmm items, [1] k_spmm_long items, [2] listed very long / other long rows (2 x int32)
   unsigned long long* ctr = nullptr;
   BCLX_TRY(scratch_alloc_n(ctx, &ctr, 3));
   BCLX_CK(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), ctx->stream));
   int32_t* cnt = reinterpret_cast<int32_t*>(ctr + 2);
-
-  // B-row reuse hints when B is larger than L2
-  RowHints hints{nullptr, nullptr};
-  int32_t* deg = nullptr;
-  unsigned long long* hist = nullptr;
-  {
-    int l2 = 0;
-    BCLX_CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->device));
-    const double frac = spmm_hot_fraction(ctx);
-    const int64_t row_bytes = C.n * (int64_t)sizeof(ST);
-    const int64_t b_bytes = B.m * row_bytes;
-    if (align_ok && frac > 0 && l2 > 0 && b_bytes > (int64_t)l2) {
-      const int64_t nb = A.gn * A.tn;  // global B rows, padded to whole tiles
-      BCLX_TRY(scratch_alloc_n(ctx, &deg, (size_t)nb + 1));
-      BCLX_TRY(scratch_alloc_n(ctx, &hist, kDegBins));
-      BCLX_CK(cudaMemsetAsync(deg, 0, sizeof(int32_t) * ((size_t)nb + 1), ctx->stream));
-      BCLX_CK(cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * kDegBins, ctx->stream));
-      k_col_degree<<<(unsigned)ctx->num_sms * 8, 256, 0, ctx->stream>>>(A, deg);
-      note_launch();
-      BCLX_CK_LAUNCH();
-      k_deg_hist<<<(unsigned)ctx->num_sms * 4, 256, 0, ctx->stream>>>(deg, nb, hist);
-      note_launch();
-      BCLX_CK_LAUNCH();
-      const long long budget_rows = (long long)(frac * (double)l2 / (double)row_bytes);
-      k_deg_threshold<<<1, 32, 0, ctx->stream>>>(hist, budget_rows, deg + nb);
-      note_launch();
-      BCLX_CK_LAUNCH();
-      hints.deg = deg;
-      hints.thr = deg + nb;
-    }
-  }
-
   uint8_t* flag = nullptr;
   int64_t* list = nullptr;
-  const unsigned grid = (unsigned)(want < cap ? want : cap);
   if (long_path) {
-    // One stream: find the long rows, run them, and launch k_spmm as
-    // k_spmm_long's programmatic dependent, so that it starts once every
-    // long-row block has its SM (and finishes only after k_spmm_long).
     BCLX_TRY(scratch_alloc_n(ctx, &flag, (size_t)arows));
     BCLX_TRY(scratch_alloc_n(ctx, &list, (size_t)arows));
+    cudaStream_t ls = ctx->stream;
+    if (!dependent) {
+      BCLX_TRY(ensure_side_stream(ctx));
+      BCLX_CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
+      BCLX_CK(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+      ls = ctx->side;
+    }
     k_spmm_find_long<<<(unsigned)std::min<int64_t>(ceil_div(arows, 256), (int64_t)ctx->num_sms * 16), 256, 0,
-                       ctx->stream>>>(A, long_row, long_row * 8, flag, list, cnt);
+                       ls>>>(A, long_row, long_row * 8, flag, list, cnt);
     note_launch();
     BCLX_CK_LAUNCH();
+    if (!dependent) BCLX_CK(cudaEventRecord(ctx->fork2_ev, ctx->side));
     const size_t lsmem = sizeof(LongSmem) * kLongWarps;
     BCLX_CK(cudaFuncSetAttribute(k_spmm_long<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
-    k_spmm_long<ST><<<(unsigned)spmm_long_blocks(ctx), kLongWarps * 32, lsmem, ctx->stream>>>(
-        A, B, C, list, cnt, npanels, align_ok, ctr + 1, hints);
+    k_spmm_long<ST><<<(unsigned)spmm_long_blocks(ctx), kLongWarps * 32, lsmem, ls>>>(A, B, C, list, cnt, npanels,
+                                                                                    align_ok, ctr + 1);
     note_launch();
     BCLX_CK_LAUNCH();
+    if (!dependent) {
+      BCLX_CK(cudaEventRecord(ctx->join_ev, ctx->side));
+      BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->fork2_ev, 0));
+      k_spmm_launch_delay<<<1, 32, 0, ctx->stream>>>(kLongHeadStartNs);
+      note_launch();
+      BCLX_CK_LAUNCH();
+    }
   }
+  const unsigned grid = (unsigned)(want < cap ? want : cap);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(kSpmmWarps * 32);
@@ -847,26 +744,18 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = long_path ? 1 : 0;
+  cfg.numAttrs = (long_path && dependent) ? 1 : 0;
   const uint8_t* lflag = flag;
-  // one item per grab: item costs vary by orders of magnitude on power-law
-  // matrices, and larger grabs measured slower (R-MAT s21 x 256)
-  const int sgrab = 1;
   if (R > 1)
-    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true>, A, B, C, n_items, npanels, R, ngroups, align_ok, lflag, ctr,
-                               hints, sgrab));
+    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true>, A, B, C, n_items, npanels, R, ngroups, align_ok, lflag, ctr));
   else
-    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, false>, A, B, C, n_items, npanels, 1, ngroups, align_ok, lflag, ctr,
-                               hints, sgrab));
+    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, false>, A, B, C, n_items, npanels, 1, ngroups, align_ok, lflag, ctr));
   note_launch();
   BCLX_CK_LAUNCH();
   if (long_path) {
+    if (!dependent) BCLX_CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
     scratch_free(ctx, flag);
     scratch_free(ctx, list);
-  }
-  if (deg) {
-    scratch_free(ctx, deg);
-    scratch_free(ctx, hist);
   }
   scratch_free(ctx, ctr);
   return BCLX_OK;
@@ -946,10 +835,6 @@ int bclx_spmm_grid(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t*
 }
 
 int bclx_spmm_grid_rowwise(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg) {
-  if (cg && cg->grid_n != 1) {
-    set_last_error("the row-wise product needs C in one tile column (c.grid_shape()[1] == 1)");
-    return BCLX_ERR_INVALID;
-  }
   return spmm_grid_impl(c, a, b, cg, 1);
 }
 

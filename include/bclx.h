@@ -151,7 +151,7 @@ typedef enum {
   BCLX_TUNE_SPMM_ROWS = 3,         /* SpMM: rows per warp item (0 = by product size, 1, 2, 4) */
   BCLX_TUNE_SPMM_LONG_ROW = 4,     /* SpMM: entries from which a row goes to the long-row kernel (64..; 1024) */
   BCLX_TUNE_SPMM_LONG_BLOCKS = 5,  /* SpMM: blocks of the long-row kernel (1..SMs; half the SMs) */
-  BCLX_TUNE_SPMM_HOT_PERMILLE = 6, /* SpMM: per mille of L2 for the most referenced B rows (0..900; 0 = no hints) */
+  BCLX_TUNE_SPMM_SCHEDULE = 6,     /* SpMM: 0 = long rows on the side stream, 1 = dependent launch (0 or 1; 0) */
   BCLX_TUNE_ITEM_OUTPUTS = 7,      /* SpGEMM: outputs per heavy-row work item (512 or 1024; 512) */
   BCLX_TUNE_WIDE_LIGHT = 8,        /* SpGEMM: 1 = rows of tiles wider than 8192 columns may be light (0 or 1; 0) */
   BCLX_TUNE_KEYS = 9

@@ -279,7 +279,7 @@ def test_tuning_knobs_reject_out_of_range():
     from bcl_b200.containers import context
     ctx = context()
     for key, bad in ((_lib.TUNE_LIGHT_UB, 1000), (_lib.TUNE_LEARN_TARGET, 10), (_lib.TUNE_SPMM_ROWS, 3),
-                     (_lib.TUNE_SPMM_HOT_PERMILLE, 950), (_lib.TUNE_SPMM_LONG_BLOCKS, 100000)):
+                     (_lib.TUNE_SPMM_SCHEDULE, 2), (_lib.TUNE_SPMM_LONG_BLOCKS, 100000)):
         assert _lib.load().bclx_context_set_tuning(ctx.h, key, bad) == _lib.ERR_INVALID
     assert ctx.get_tuning("light_ub") == 512
 

@@ -213,11 +213,11 @@ def test_spmm_tile_single_call_ld():
 
 
 @pytest.mark.parametrize("knobs", [dict(spmm_rows=1), dict(spmm_rows=4, spmm_long_row=64, spmm_long_blocks=20),
-                                   dict(spmm_hot_permille=0), dict(spmm_hot_permille=900, spmm_long_row=128)])
+                                   dict(spmm_schedule=1), dict(spmm_schedule=1, spmm_long_row=128)])
 def test_spmm_knobs_do_not_change_results(monkeypatch, knobs):
-    """Rows per item, the long-row threshold and block count, and the L2 hint
-    share (hints forced on by a small long-row product size) leave every bit
-    of C as it was."""
+    """Rows per item, the long-row threshold and block count, and the
+    schedule (the long-row path forced on by a small product-size bound)
+    leave every bit of C as it was."""
     monkeypatch.setenv("BCLX_SPMM_LONG_MIN_ROWS", "1024")
     import torch
     from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm
@@ -242,7 +242,7 @@ def test_spmm_autotune_roundtrip(tmp_path, monkeypatch):
     A = SPMatrix.from_csr(a, BlockCustom((1024, 1024)))
     B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((1024, 128)))
     C = DMatrix.zeros((a.m, 128), BlockCustom((1024, 128)))
-    params, ms = autotune.tune_spmm(A, B, C, reps=1, candidates={"spmm_rows": (1, 2), "spmm_hot_permille": (0, 500)})
+    params, ms = autotune.tune_spmm(A, B, C, reps=1, candidates={"spmm_rows": (1, 2), "spmm_schedule": (0, 1)})
     assert ms > 0 and autotune.lookup(A, B, "spmm") == params
     C2 = DMatrix.zeros((a.m, 128), BlockCustom((1024, 128)))
     spmm(A, B, C2, tuning="auto")
@@ -250,11 +250,11 @@ def test_spmm_autotune_roundtrip(tmp_path, monkeypatch):
     assert np.array_equal(bits(C2.get_matrix().cpu().numpy()), bits(want))
 
 
-@pytest.mark.parametrize("hot", [0, 500, 900])
-def test_spmm_l2_hints_large_b(hot):
-    """B larger than L2 (R-MAT s18 x 256 FP32, 268 MB) turns the B-row reuse
-    hints on: the result on sampled rows stays bit-exact for any share of L2
-    given to the most referenced rows (0 = hints off)."""
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_spmm_schedules_large(schedule):
+    """R-MAT s18 x 256 FP32 (long rows on their own kernel) under both
+    schedules (side stream with a launch delay, programmatic dependent
+    launch): sampled rows bit-exact."""
     import torch
     from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm
     a = gen.rmat(18, seed=16)
@@ -263,7 +263,7 @@ def test_spmm_l2_hints_large_b(hot):
     A = SPMatrix.from_csr(a, BlockCustom((ts, ts)))
     B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((ts, 256)))
     C = DMatrix.zeros((a.m, 256), BlockCustom((ts, 256)))
-    spmm(A, B, C, tuning=dict(spmm_hot_permille=hot))
+    spmm(A, B, C, tuning=dict(spmm_schedule=schedule))
     rows = np.unique(np.concatenate([np.random.default_rng(18).choice(a.m, 2048, replace=False), np.arange(32)]))
     got = C.get_matrix()[torch.as_tensor(rows, device="cuda")].cpu().numpy()
     want = O.spmm_tiled(a, b, np.zeros((rows.size, 256), np.float32), ts, ts, 256, rows=rows)
