@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libbclx.so")
 
 # status codes (bclx_status_t)
 (TUNE_LIGHT_UB, TUNE_LEARN_TARGET, TUNE_BTABLE_MAX_BYTES, TUNE_SPMM_ROWS, TUNE_SPMM_LONG_ROW,
- TUNE_SPMM_LONG_BLOCKS, TUNE_SPMM_SCHEDULE, TUNE_ITEM_OUTPUTS, TUNE_WIDE_LIGHT) = range(9)
+ TUNE_SPMM_LONG_BLOCKS, TUNE_SPMM_SCHEDULE, TUNE_ITEM_OUTPUTS, TUNE_WIDE_LIGHT, TUNE_SPMM_PANEL_MAJOR) = range(10)
 OK, ERR_INVALID, ERR_DTYPE, ERR_CUDA, ERR_NO_MEMORY, ERR_INDEX_OVERFLOW, ERR_DEVICE_TIMEOUT, ERR_NO_DEVICE = range(8)
 STATUS_NAMES = {
     OK: "BCLX_OK", ERR_INVALID: "BCLX_ERR_INVALID", ERR_DTYPE: "BCLX_ERR_DTYPE", ERR_CUDA: "BCLX_ERR_CUDA",

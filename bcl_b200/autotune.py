@@ -5,8 +5,8 @@ each candidate runs the whole product), then the numeric pass's plan
 parameters (work items a warp takes from the device queue at a time, blocks
 per SM, the B-segment length from which a segment is walked lane-parallel),
 grid-searched on one plan.  SpMM: rows per warp item, the long-row
-threshold, the long-row kernel's block count and the schedule of the
-long-row and short-row kernels, by coordinate descent (one knob at a time, the
+threshold, the long-row kernel's block count, the schedule of the
+long-row and short-row kernels and the order of column panels, by coordinate descent (one knob at a time, the
 others at their best so far).  The learned product: the outputs aimed at per
 heavy item.
 
@@ -38,6 +38,7 @@ SPMM_CANDIDATES = {
     "spmm_long_row": (512, 1024, 2048, 4096),
     "spmm_long_blocks": (37, 74, 111),
     "spmm_schedule": (0, 1),
+    "spmm_panel_major": (0, 1),
 }
 LEARN_TARGETS = (256, 320, 384)
 

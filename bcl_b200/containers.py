@@ -64,11 +64,15 @@ class Context:
         """Return the scratch pool's cached device memory to the driver."""
         call("bclx_context_release_cached", self.use_current_stream())
 
+    def synchronize(self):
+        """Wait for the current stream (bclx_context_synchronize)."""
+        call("bclx_context_synchronize", self.use_current_stream())
+
     TUNING_KEYS = {"light_ub": _lib.TUNE_LIGHT_UB, "learn_target": _lib.TUNE_LEARN_TARGET,
                    "btable_max_bytes": _lib.TUNE_BTABLE_MAX_BYTES, "spmm_rows": _lib.TUNE_SPMM_ROWS,
                    "spmm_long_row": _lib.TUNE_SPMM_LONG_ROW, "spmm_long_blocks": _lib.TUNE_SPMM_LONG_BLOCKS,
                    "spmm_schedule": _lib.TUNE_SPMM_SCHEDULE, "item_outputs": _lib.TUNE_ITEM_OUTPUTS,
-                   "wide_light": _lib.TUNE_WIDE_LIGHT}
+                   "wide_light": _lib.TUNE_WIDE_LIGHT, "spmm_panel_major": _lib.TUNE_SPMM_PANEL_MAJOR}
 
     def set_tuning(self, **knobs) -> None:
         """bclx_context_set_tuning for each name=value (None: the default)."""

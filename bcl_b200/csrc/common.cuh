@@ -52,7 +52,7 @@ struct Context {
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, fork2_ev = nullptr, join_ev = nullptr;
   // bclx_context_set_tuning values (-1: the default)
-  int64_t tune[BCLX_TUNE_KEYS] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
+  int64_t tune[BCLX_TUNE_KEYS] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
 };
 
 // The value in effect for a tuning knob (the context's, else the default).

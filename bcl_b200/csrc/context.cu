@@ -28,6 +28,7 @@ static int64_t tuning_default(const Context* ctx, int key) {
     case BCLX_TUNE_SPMM_SCHEDULE: return env_or("BCLX_SPMM_SCHEDULE", 0);
     case BCLX_TUNE_ITEM_OUTPUTS: return env_or("BCLX_ITEM_OUTPUTS", 512);
     case BCLX_TUNE_WIDE_LIGHT: return env_or("BCLX_WIDE_LIGHT", 0);
+    case BCLX_TUNE_SPMM_PANEL_MAJOR: return env_or("BCLX_SPMM_PANEL_MAJOR", 0);
     default: return 0;
   }
 }
@@ -43,6 +44,7 @@ static bool tuning_in_range(const Context* ctx, int key, int64_t v) {
     case BCLX_TUNE_SPMM_SCHEDULE: return v == 0 || v == 1;
     case BCLX_TUNE_ITEM_OUTPUTS: return v == 512 || v == 1024;
     case BCLX_TUNE_WIDE_LIGHT: return v == 0 || v == 1;
+    case BCLX_TUNE_SPMM_PANEL_MAJOR: return v == 0 || v == 1;
     default: return false;
   }
 }

@@ -379,7 +379,8 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
 template <typename ST, bool GROUP>
 __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int R, int64_t ngroups,
-           int row_align_ok, const uint8_t* __restrict__ long_flag, unsigned long long* __restrict__ next_item) {
+           int row_align_ok, int panel_major, const uint8_t* __restrict__ long_flag,
+           unsigned long long* __restrict__ next_item) {
   constexpr int PW = 32 * Vec<ST>::N;
   const int lane = lane_id();
   unsigned long long it = 0;
@@ -389,8 +390,16 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     unsigned long long nx = 0;
     if (lane == 0) nx = atomicAdd(next_item, 1ULL);
     const int64_t item = (int64_t)it;
-    const int64_t rg = item / npanels;
-    const int panel = (int)(item - rg * npanels);
+    int64_t rg;
+    int panel;
+    if (panel_major) {  // all row groups of panel 0, then of panel 1, ...
+      const int64_t n_rg = n_items / npanels;
+      panel = (int)(item / n_rg);
+      rg = item - panel * n_rg;
+    } else {  // the panels of a row group one after another
+      rg = item / npanels;
+      panel = (int)(item - rg * npanels);
+    }
     const int64_t t = rg / ngroups;
     const int64_t r0 = (rg - t * ngroups) * R;
     const int64_t ti = t / C.gn, tj = t - ti * C.gn;
@@ -683,7 +692,13 @@ static int spmm_rows_per_item(const Context* ctx, const DGridView& C, int64_t gk
 //    (it launches once every long-row block has started, and finishes only
 //    after k_spmm_long).
 // Measured on R-MAT s21 x 256 (one B200): schedule 0 4.14 ms FP32 / 2.45 ms
-// BF16, schedule 1 4.63 / 3.45 ms.
+// BF16, schedule 1 4.63 / 3.45 ms.  Also measured, and slower: one-warp
+// long-row blocks small enough to share every SM with four k_spmm blocks
+// (k_spmm capped at 56 registers, both kernels at the largest shared-memory
+// carveout): 5.08 / 3.91 ms, k_spmm alone losing 15 % to the smaller L1;
+// and one cp.async.bulk copy per 512-byte B slice, completing on an
+// mbarrier, in place of the per-lane copies: 6.8 ms for k_spmm_long alone
+// against 1.9.
 template <typename ST>
 static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, const DGridView& C, int align_ok) {
   constexpr int VN = Vec<ST>::N;
@@ -746,10 +761,13 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   cfg.attrs = attr;
   cfg.numAttrs = (long_path && dependent) ? 1 : 0;
   const uint8_t* lflag = flag;
+  const int pmajor = (int)tuning(ctx, BCLX_TUNE_SPMM_PANEL_MAJOR);
   if (R > 1)
-    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true>, A, B, C, n_items, npanels, R, ngroups, align_ok, lflag, ctr));
+    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true>, A, B, C, n_items, npanels, R, ngroups, align_ok, pmajor, lflag,
+                               ctr));
   else
-    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, false>, A, B, C, n_items, npanels, 1, ngroups, align_ok, lflag, ctr));
+    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, false>, A, B, C, n_items, npanels, 1, ngroups, align_ok, pmajor, lflag,
+                               ctr));
   note_launch();
   BCLX_CK_LAUNCH();
   if (long_path) {

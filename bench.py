@@ -74,6 +74,9 @@ def parse_args():
     p.add_argument("--path", default="fused", choices=["fused", "per_stage", "batched_graph", "learned"],
                    help="SpGEMM form timed as the step (default: all stages fused)")
     p.add_argument("--scale", type=int, default=None, help="override the R-MAT scale (profiling runs)")
+    p.add_argument("--tune", action="store_true",
+                   help="run the autotuner on the workload before timing and use its choice "
+                        "(default: the library's defaults)")
     p.add_argument("--shard", action="store_true",
                    help="N>1: the ranks share ONE product, each computing its block-cyclic C tiles "
                         "(strong scaling; default: each rank runs its own product)")
@@ -299,6 +302,17 @@ def bench_spgemm(args, wl, dist, device):
         pred = _learned.get_default(train_if_missing=False)
     learned_st = {}
 
+    from bcl_b200 import autotune
+    from bcl_b200.containers import context as _context
+    ctx = _context(device)
+    plan_params = None
+    tuning_src = "library defaults"
+    if getattr(args, "tune", False) and args.path == "fused" and not shard:
+        best, _, _ = autotune.tune(A, A, reps=1)
+        ctx.set_tuning(light_ub=best["light_ub"])
+        plan_params = (best["grab"], best["blocks_per_sm"], best["long_seg"])
+        tuning_src = "autotuned on this product before timing (bcl_b200.autotune.tune)"
+
     def step(record=None):
         if shard:
             # this rank's C tiles of the one product (the reference's block-cyclic owner)
@@ -322,6 +336,8 @@ def bench_spgemm(args, wl, dist, device):
             return C.nnz(), None
         t0 = time.perf_counter()
         plan, out, trp, toff, nnz = spgemm_symbolic(A, A)
+        if plan_params:
+            plan.tune(*plan_params)
         t1 = time.perf_counter()
         # the output arrays are the caller's; reuse them while they are large enough
         if outbuf.get("cap", -1) < nnz:
@@ -413,6 +429,10 @@ def bench_spgemm(args, wl, dist, device):
            "l2": "flushed between steps (256 MiB write outside the timed events)",
            "parallelism": (f"one product shared by {dist.world} GPUs (block-cyclic C tiles, A replicated)"
                            if shard else f"independent products per GPU x{dist.world}")}
+    cfg["tuning"] = dict({k: ctx.get_tuning(k) for k in ("light_ub", "item_outputs", "wide_light",
+                                                          "btable_max_bytes")},
+                         source=tuning_src,
+                         plan=dict(zip(("grab", "blocks_per_sm", "long_seg"), plan_params or autotune.DEFAULT)))
     if shard:
         cfg["nnz_C"] = f"{nnz_c} on rank 0"
     line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": dist.world, "steps": args.steps,
@@ -824,13 +844,14 @@ def spmm_summary(args, stream):
     B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((ts, N)))
     C = DMatrix.zeros((n, N), BlockCustom((ts, N)))
     flops = 2.0 * a.nnz * N
-    alg = G * G * G * 0  # per-product model below
+    # compulsory bytes: A (indices, values, row pointers) and B read once, C read and written once
+    alg = 8 * a.nnz + 4 * (ts + 1) * G * G + 4 * n * N + 8 * n * N
     # reference model per tile product: indices + values of A_ik, B_kj, C_ij read and written once
     tile_nnz = tile_nnz_grid(a, ts, ts)
-    alg = 0
+    ref_model = 0
     for i in range(G):
         for k in range(G):
-            alg += 8 * int(tile_nnz[i, k]) + 4 * (ts + 1) + 4 * ts * N + 8 * ts * N
+            ref_model += 8 * int(tile_nnz[i, k]) + 4 * (ts + 1) + 4 * ts * N + 8 * ts * N
     t = time_region(lambda: spmm(A, B, C), 20, stream)
     tp = time_region(lambda: spmm_plain(A, B, C), 5, stream)
     B16 = DMatrix.from_array(torch.from_numpy(b), BlockCustom((ts, N)), dtype=torch.bfloat16)
@@ -841,7 +862,7 @@ def spmm_summary(args, stream):
     cus = cusparse_spmm_leg(a, B.get_matrix(), t, C0.get_matrix(), stream, reps=20)
     hbm, _ = peaks()
     return {"workload": wl["desc"], "gflops": flops / t / 1e9, "alg_gbs": alg / t / 1e9, "frac_hbm": alg / t / 1e9 / hbm,
-            "ms": t * 1e3, "plain_gflops": flops / tp / 1e9, "bf16_gflops": flops / t16 / 1e9,
+            "bytes_model": "compulsory", "reference_model_gbs": ref_model / t / 1e9, "ms": t * 1e3, "plain_gflops": flops / tp / 1e9, "bf16_gflops": flops / t16 / 1e9,
             "bf16_speedup": t / t16, "cusparse": cus}
 
 
@@ -886,6 +907,14 @@ def bench_spmm(args, wl, dist, device):
     flops = 2.0 * a.nnz * N
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    from bcl_b200 import autotune
+    from bcl_b200.containers import context as _context
+    ctx = _context(device)
+    tuning_src = "library defaults"
+    if getattr(args, "tune", False):
+        best, _ = autotune.tune_spmm(A, B, C)
+        ctx.set_tuning(**best)
+        tuning_src = "autotuned on this product before timing (bcl_b200.autotune.tune_spmm)"
     for _ in range(args.warmup):
         spmm(A, B, C)
     torch.cuda.synchronize()
@@ -912,20 +941,27 @@ def bench_spmm(args, wl, dist, device):
     kern_s = statistics.mean(step_ms) / 1e3  # the step is the product's kernels
     model = spmm_model_bytes(a, ts, G, N, es)
     compulsory = 8 * a.nnz + 4 * (ts + 1) * G * G + es * a.n * N + 2 * es * a.m * N
-    roofline = {"bound": "hbm", "achieved": model / kern_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                "frac": model / kern_s / 1e9 / hbm_peak, "traffic": workload_traffic(args.workload),
+    # the roofline counts compulsory bytes (A, B once; C read and written
+    # once); the reference's per-tile-product model counts each B tile once per
+    # C tile that uses it, bytes a kernel need not move, and is kept beside it
+    roofline = {"bound": "hbm", "achieved": compulsory / kern_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": compulsory / kern_s / 1e9 / hbm_peak, "traffic": workload_traffic(args.workload),
                 "kernel": "k_spmm + k_spmm_long (one product, all SUMMA stages)", "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": model,
-                "bytes_model": "reference per-tile-product model (spmm.hpp:383-394): A_ik, B_kj, C_ij once per product",
-                "compulsory_bytes_per_launch": compulsory,
-                "compulsory_gbs": compulsory / kern_s / 1e9, "kernel_ms": kern_s * 1e3}
+                "algorithmic_bytes_per_launch": compulsory,
+                "bytes_model": "compulsory: A and B read once, C read and written once",
+                "reference_model_bytes_per_launch": model,
+                "reference_model": "per-tile-product model (spmm.hpp:383-394): A_ik, B_kj, C_ij once per product",
+                "reference_model_gbs": model / kern_s / 1e9, "kernel_ms": kern_s * 1e3}
     e2e = bench_spmm_e2e(args, A, B, C, stream, flops, dist)
     cfg = {"workload": wl["desc"], "tile_grid": f"{G}x{G}", "tile": ts, "nnz_A": a.nnz, "N": N,
            "path": "k_spmm (short rows, grouped per warp) + k_spmm_long (rows of >= 1024 entries, side "
                    "stream): every C row sums its stages in rotated order, C += A*B in place",
            "l2": "flushed between steps (256 MiB write outside the timed events)" if wl["matrix"] == "er"
                  else "inputs larger than L2 (B %d MB)" % (a.n * N * es >> 20),
-           "parallelism": f"independent products per GPU x{dist.world}"}
+           "parallelism": f"independent products per GPU x{dist.world}",
+           "tuning": dict({k: ctx.get_tuning(k) for k in ("spmm_rows", "spmm_long_row", "spmm_long_blocks",
+                                                          "spmm_schedule", "spmm_panel_major")},
+                          source=tuning_src)}
     line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if wl["dtype"] == "f32" else "bf16 storage, f32 accumulate",

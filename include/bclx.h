@@ -154,7 +154,8 @@ typedef enum {
   BCLX_TUNE_SPMM_SCHEDULE = 6,     /* SpMM: 0 = long rows on the side stream, 1 = dependent launch (0 or 1; 0) */
   BCLX_TUNE_ITEM_OUTPUTS = 7,      /* SpGEMM: outputs per heavy-row work item (512 or 1024; 512) */
   BCLX_TUNE_WIDE_LIGHT = 8,        /* SpGEMM: 1 = rows of tiles wider than 8192 columns may be light (0 or 1; 0) */
-  BCLX_TUNE_KEYS = 9
+  BCLX_TUNE_SPMM_PANEL_MAJOR = 9,  /* SpMM: 1 = every row's first column panel before any row's second (0 or 1; 0) */
+  BCLX_TUNE_KEYS = 10
 } bclx_tune_key_t;
 BCLX_API int bclx_context_set_tuning(bclx_context_t ctx, int32_t key, int64_t value);
 BCLX_API int bclx_context_get_tuning(bclx_context_t ctx, int32_t key, int64_t* value);

@@ -213,11 +213,12 @@ def test_spmm_tile_single_call_ld():
 
 
 @pytest.mark.parametrize("knobs", [dict(spmm_rows=1), dict(spmm_rows=4, spmm_long_row=64, spmm_long_blocks=20),
-                                   dict(spmm_schedule=1), dict(spmm_schedule=1, spmm_long_row=128)])
+                                   dict(spmm_schedule=1), dict(spmm_schedule=1, spmm_long_row=128),
+                                   dict(spmm_panel_major=1), dict(spmm_panel_major=1, spmm_rows=2)])
 def test_spmm_knobs_do_not_change_results(monkeypatch, knobs):
-    """Rows per item, the long-row threshold and block count, and the
-    schedule (the long-row path forced on by a small product-size bound)
-    leave every bit of C as it was."""
+    """Rows per item, the long-row threshold and block count, the schedule
+    (the long-row path forced on by a small product-size bound) and the
+    panel order leave every bit of C as it was."""
     monkeypatch.setenv("BCLX_SPMM_LONG_MIN_ROWS", "1024")
     import torch
     from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm
@@ -250,11 +251,11 @@ def test_spmm_autotune_roundtrip(tmp_path, monkeypatch):
     assert np.array_equal(bits(C2.get_matrix().cpu().numpy()), bits(want))
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
-def test_spmm_schedules_large(schedule):
+@pytest.mark.parametrize("schedule,panel_major", [(0, 0), (1, 0), (0, 1)])
+def test_spmm_schedules_large(schedule, panel_major):
     """R-MAT s18 x 256 FP32 (long rows on their own kernel) under both
     schedules (side stream with a launch delay, programmatic dependent
-    launch): sampled rows bit-exact."""
+    launch) and both panel orders: sampled rows bit-exact."""
     import torch
     from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix, spmm
     a = gen.rmat(18, seed=16)
@@ -263,8 +264,9 @@ def test_spmm_schedules_large(schedule):
     A = SPMatrix.from_csr(a, BlockCustom((ts, ts)))
     B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((ts, 256)))
     C = DMatrix.zeros((a.m, 256), BlockCustom((ts, 256)))
-    spmm(A, B, C, tuning=dict(spmm_schedule=schedule))
+    spmm(A, B, C, tuning=dict(spmm_schedule=schedule, spmm_panel_major=panel_major))
     rows = np.unique(np.concatenate([np.random.default_rng(18).choice(a.m, 2048, replace=False), np.arange(32)]))
     got = C.get_matrix()[torch.as_tensor(rows, device="cuda")].cpu().numpy()
     want = O.spmm_tiled(a, b, np.zeros((rows.size, 256), np.float32), ts, ts, 256, rows=rows)
     assert np.array_equal(bits(got), bits(want))
+
