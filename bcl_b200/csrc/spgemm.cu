@@ -319,8 +319,10 @@ __device__ __forceinline__ void walk_products(const SpGridView& A, const SpGridV
 // Order-free walk for the symbolic pass: calls fs(j) for every product
 // column of C-tile row `x` (all stages).  Short B segments are looped over by
 // their own lane, long ones by the whole warp.  With nparts walkers (the warps
-// of a block) each takes every nparts-th chunk of short segments and an
-// interleaved share of every long segment.
+// of a block): when the row has at least 2 * nparts chunks of 32 A entries,
+// each walker takes every nparts-th chunk whole (short and long segments);
+// otherwise every walker reads every chunk and takes every nparts-th chunk of
+// short segments and an interleaved share of every long segment.
 template <typename FS>
 __device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridView& B, const Geom& g,
                                              const RowInfo& x, int part, int nparts, FS&& fs) {
@@ -365,11 +367,17 @@ __device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridVi
       if (e < atot) t.kc = __ldg(sacol + sas + (e - sax));
       return t;
     };
-    Ent nxt = atot > 0 ? load_ent(0) : Ent{0, nullptr, nullptr};
-    for (int32_t e0 = 0, chunk = 0; e0 < atot; e0 += 32, chunk++) {
+    // whole chunks per walker, or every chunk read by every walker
+    const bool own = nparts > 1 && atot >= 64 * nparts;
+    const int32_t first = own ? 32 * part : 0;
+    const int32_t stride = own ? 32 * nparts : 32;
+    const int wpart = own ? 0 : part;  // this walker's share within a chunk
+    const int wparts = own ? 1 : nparts;
+    Ent nxt = first < atot ? load_ent(first) : Ent{0, nullptr, nullptr};
+    for (int32_t e0 = first, chunk = 0; e0 < atot; e0 += stride, chunk++) {
       const Ent cur = nxt;
       const int32_t e = e0 + lane;
-      if (e0 + 32 < atot) nxt = load_ent(e0 + 32);
+      if (e0 + stride < atot) nxt = load_ent(e0 + stride);
       const int32_t* sbci = cur.bci;
       int32_t bs = 0, be = 0;
       if (e < atot) {
@@ -377,7 +385,7 @@ __device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridVi
         be = __ldg(cur.brp + cur.kc + 1);
       }
       const bool lng = be - bs >= 32;
-      if (!lng && chunk % nparts == part) {
+      if (!lng && chunk % wparts == wpart) {
         int32_t q = bs;
         for (; q + 4 <= be; q += 4) {  // four column loads in flight
           const int32_t j0 = __ldg(sbci + q), j1 = __ldg(sbci + q + 1);
@@ -395,8 +403,8 @@ __device__ __forceinline__ void walk_columns(const SpGridView& A, const SpGridVi
         longm &= longm - 1;
         const int32_t lb = __shfl_sync(kFull, bs, src), le = __shfl_sync(kFull, be, src);
         const int32_t* lci = shfl_ptr(sbci, src);
-        const int32_t step = 32 * nparts;
-        int32_t q = lb + lane + 32 * part;
+        const int32_t step = 32 * wparts;
+        int32_t q = lb + lane + 32 * wpart;
         for (; q + 3 * step < le; q += 4 * step) {
           const int32_t j0 = __ldg(lci + q), j1 = __ldg(lci + q + step);
           const int32_t j2 = __ldg(lci + q + 2 * step), j3 = __ldg(lci + q + 3 * step);
