@@ -494,10 +494,12 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
                            int32_t* __restrict__ ub_out, unsigned long long* __restrict__ queue, int grab) {
   const int lane = lane_id();
   unsigned long long mine = 0;
-  // rows from a device counter, `grab` consecutive rows per atomic (one
-  // atomic per row serialises on the counter when a fine grid has hundreds
-  // of millions of mostly empty row items); the next grab is in flight while
-  // the current rows are walked
+  // rows from a device counter, `grab` (at most 32) consecutive rows per
+  // atomic (one atomic per row serialises on the counter when a fine grid has
+  // hundreds of millions of mostly empty row items); the next grab is in
+  // flight while the current rows are walked.  Lane q keeps the class of row
+  // base + q, and the grab's rows are appended to each list with one atomic.
+  grab = min(grab, 32);
   const unsigned long long n_rows = (unsigned long long)g.n_row_items;
   unsigned long long base = 0;
   if (lane == 0) base = atomicAdd(queue, (unsigned long long)grab);
@@ -506,6 +508,7 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
     unsigned long long nx = 0;
     if (lane == 0) nx = atomicAdd(queue, (unsigned long long)grab);
     const unsigned long long end = min(base + (unsigned long long)grab, n_rows);
+    int cls = -1;  // list of row base + lane: 0 light, 1 heavy, 3 very heavy
     for (unsigned long long it = base; it < end; it++) {
     const int64_t ri = (int64_t)it;
     const RowInfo x = decode_row(g, ri);
@@ -559,15 +562,21 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
       xr[4] = ((float)x.tj + 0.5f) / (float)g.gn;
       ub_out[ri] = (int32_t)(tot < INT32_MAX ? tot : INT32_MAX);
     }
-    if (lane == 0 && tot > 0) {
-      mine += (unsigned long long)tot;
-      if (tot <= light_ub && x.w < heavy_min_cols)
-        light_list[atomicAdd(&counters[0], 1)] = (int32_t)ri;
-      else if (tot <= kVeryHeavyUb)
-        heavy_list[atomicAdd(&counters[1], 1)] = (int32_t)ri;
-      else
-        vheavy_list[atomicAdd(&counters[3], 1)] = (int32_t)ri;
+    if (tot > 0) {
+      if (lane == 0) mine += (unsigned long long)tot;
+      if (lane == (int)(it - base)) cls = (tot <= light_ub && x.w < heavy_min_cols) ? 0 : (tot <= kVeryHeavyUb ? 1 : 3);
     }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      if (c == 2) continue;
+      const unsigned m = __ballot_sync(kFull, cls == c);
+      if (m == 0) continue;
+      int pos = 0;
+      if (lane == 0) pos = atomicAdd(&counters[c], __popc(m));
+      pos = __shfl_sync(kFull, pos, 0) + __popc(m & ((1u << lane) - 1u));
+      int32_t* list = c == 0 ? light_list : (c == 1 ? heavy_list : vheavy_list);
+      if (cls == c) list[pos] = (int32_t)(base + lane);
     }
     base = __shfl_sync(kFull, nx, 0);
   }
@@ -1371,11 +1380,12 @@ static int check_grids(const bclx_spgrid_t* a, const bclx_spgrid_t* b, const bcl
   return BCLX_OK;
 }
 
-// Rows a warp takes from a device counter at a time: about 32 grabs per
-// resident warp over the pass, at least 1 and at most `cap`.
-static int queue_grab(Context* ctx, int64_t rows, int warps_per_block, int blocks_per_sm, int cap) {
+// Rows a warp takes from a device counter at a time: about `per_warp` grabs
+// per resident warp over the pass, at least 1 and at most `cap`.
+static int queue_grab(Context* ctx, int64_t rows, int warps_per_block, int blocks_per_sm, int cap,
+                      int per_warp = 32) {
   const int64_t warps = (int64_t)ctx->num_sms * blocks_per_sm * warps_per_block;
-  const int64_t g = rows / (warps * 32);
+  const int64_t g = rows / (warps * per_warp);
   return (int)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
@@ -1548,7 +1558,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, heavy_min_cols, P->light_ub_max,
-        nullptr, nullptr, P->queue + 1, queue_grab(ctx, nri, 8, 16, 64));
+        nullptr, nullptr, P->queue + 1, queue_grab(ctx, nri, 8, 16, 32, 8));
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1996,7 +2006,7 @@ static int noalloc_product(Context* ctx, ScratchArena& ar, const bclx_csr_t* a, 
   BCLX_CK(cudaMemsetAsync(P.queue + 1, 0, sizeof(unsigned long long), ctx->stream));
   k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
       A, B, g, P.light_list, P.heavy_tmp, P.vheavy_list, P.counters, P.products_dev, 8192 + 1, kLightUb, nullptr, nullptr,
-      P.queue + 1, queue_grab(ctx, nri, 8, 16, 64));
+      P.queue + 1, queue_grab(ctx, nri, 8, 16, 32, 8));
   note_launch();
   BCLX_CK_LAUNCH();
   int32_t cnts[4];
@@ -2163,7 +2173,7 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, tuning(ctx, BCLX_TUNE_WIDE_LIGHT) ? INT_MAX : 8192 + 1,
         (int)tuning(ctx, BCLX_TUNE_LIGHT_UB), P->feat, P->ub,
-        P->queue + 1, queue_grab(ctx, nri, 8, 16, 64));
+        P->queue + 1, queue_grab(ctx, nri, 8, 16, 32, 8));
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -2456,7 +2466,7 @@ int bclx_spgemm_row_features(bclx_context_t c, const bclx_spgrid_t* a, const bcl
     cudaMemsetAsync(prod, 0, 2 * sizeof(unsigned long long), ctx->stream);
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         make_view(*a), make_view(*b), g, lists, lists + nri, lists + 2 * nri, cnt, prod, 8192 + 1, kLightUb, X, ub, prod + 1,
-        queue_grab(ctx, nri, 8, 16, 64));
+        queue_grab(ctx, nri, 8, 16, 32, 8));
     note_launch();
     if (cudaGetLastError() != cudaSuccess) rc = BCLX_ERR_CUDA;
   }
