@@ -35,8 +35,8 @@ CANDIDATES = {
 DEFAULT = (1, 4, 32)
 SPMM_CANDIDATES = {
     "spmm_rows": (0, 1, 2, 4),
-    "spmm_long_row": (512, 1024, 2048, 4096),
-    "spmm_long_blocks": (37, 74, 111),
+    "spmm_long_row": (0, 512, 1024, 2048),
+    "spmm_long_blocks": (0, 37, 74, 111),
     "spmm_schedule": (0, 1),
     "spmm_panel_major": (0, 1),
 }

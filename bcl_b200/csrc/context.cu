@@ -23,8 +23,8 @@ static int64_t tuning_default(const Context* ctx, int key) {
     case BCLX_TUNE_LEARN_TARGET: return 320;
     case BCLX_TUNE_BTABLE_MAX_BYTES: return env_or("BCLX_BTABLE_MAX_BYTES", int64_t(2) << 30);
     case BCLX_TUNE_SPMM_ROWS: return env_or("BCLX_SPMM_ROWS", 0);
-    case BCLX_TUNE_SPMM_LONG_ROW: return 1024;
-    case BCLX_TUNE_SPMM_LONG_BLOCKS: return env_or("BCLX_SPMM_LONG_BLOCKS", ctx->num_sms / 2);
+    case BCLX_TUNE_SPMM_LONG_ROW: return env_or("BCLX_SPMM_LONG_ROW", 0);
+    case BCLX_TUNE_SPMM_LONG_BLOCKS: return env_or("BCLX_SPMM_LONG_BLOCKS", 0);
     case BCLX_TUNE_SPMM_SCHEDULE: return env_or("BCLX_SPMM_SCHEDULE", 0);
     case BCLX_TUNE_ITEM_OUTPUTS: return env_or("BCLX_ITEM_OUTPUTS", 512);
     case BCLX_TUNE_WIDE_LIGHT: return env_or("BCLX_WIDE_LIGHT", 0);
@@ -39,8 +39,8 @@ static bool tuning_in_range(const Context* ctx, int key, int64_t v) {
     case BCLX_TUNE_LEARN_TARGET: return v >= 64 && v <= 448;
     case BCLX_TUNE_BTABLE_MAX_BYTES: return true;
     case BCLX_TUNE_SPMM_ROWS: return v == 0 || v == 1 || v == 2 || v == 4;
-    case BCLX_TUNE_SPMM_LONG_ROW: return v >= 64 && v <= INT32_MAX;
-    case BCLX_TUNE_SPMM_LONG_BLOCKS: return v >= 1 && v <= ctx->num_sms;
+    case BCLX_TUNE_SPMM_LONG_ROW: return v == 0 || (v >= 64 && v <= INT32_MAX);
+    case BCLX_TUNE_SPMM_LONG_BLOCKS: return v >= 0 && v <= ctx->num_sms;
     case BCLX_TUNE_SPMM_SCHEDULE: return v == 0 || v == 1;
     case BCLX_TUNE_ITEM_OUTPUTS: return v == 512 || v == 1024;
     case BCLX_TUNE_WIDE_LIGHT: return v == 0 || v == 1;

@@ -433,8 +433,8 @@ constexpr int kLongWarps = 4;
 constexpr int kLongBSlots = 3;  // chunks of B slices per warp: applied, in flight, being issued
 constexpr int kLongTSlots = 3;  // chunks of table entries per warp (with the B slices)
 constexpr int kLongASlots = 6;  // chunks of staged A entries per warp
-// A row is long from BCLX_TUNE_SPMM_LONG_ROW entries over all stages (1024 by
-// default).
+// A row is long from BCLX_TUNE_SPMM_LONG_ROW entries over all stages (512
+// for FP32, 1024 for BF16 by default).
 constexpr int64_t kSpmmLongMinRows = 65536;  // smaller products do not use the long-row path
 
 struct LongSmem {
@@ -659,10 +659,14 @@ __global__ void k_spmm_launch_delay(unsigned ns) {
   }
 }
 
-// Blocks of k_spmm_long (one per SM: its shared memory fills the SM): half
-// the SMs by default, the rest run k_spmm (BCLX_TUNE_SPMM_LONG_BLOCKS).
-static int spmm_long_blocks(const Context* ctx) {
-  const int b = (int)tuning(ctx, BCLX_TUNE_SPMM_LONG_BLOCKS);
+// Blocks of k_spmm_long (one per SM: its shared memory fills the SM); the
+// other SMs run k_spmm.  By default a quarter of the SMs per column panel of
+// a long row, at most half (R-MAT s21 x 256: FP32, two panels, 74 blocks;
+// BF16, one panel, 37 blocks, measured 2.39 against 2.75 ms with 74);
+// BCLX_TUNE_SPMM_LONG_BLOCKS sets the count.
+static int spmm_long_blocks(const Context* ctx, int npanels) {
+  int b = (int)tuning(ctx, BCLX_TUNE_SPMM_LONG_BLOCKS);
+  if (b <= 0) b = std::min(ctx->num_sms / 2, ctx->num_sms / 4 * npanels);
   return std::max(1, std::min(b, ctx->num_sms));
 }
 
@@ -711,7 +715,11 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   const int64_t cap = (int64_t)ctx->num_sms * 4;  // resident blocks: warps take items from a counter
   const int64_t arows = A.gm * A.tm;
   const bool long_path = align_ok && A.gn <= 32 && arows >= spmm_long_min_rows();
-  const int long_row = (int)tuning(ctx, BCLX_TUNE_SPMM_LONG_ROW);
+  // rows of at least long_row entries go to the long-row kernel: by default
+  // 512 for FP32 and 1024 for BF16 (R-MAT s21 x 256: FP32 4.00 against
+  // 4.21 ms with 1024; BF16 2.42 against 3.11 ms with 512)
+  int long_row = (int)tuning(ctx, BCLX_TUNE_SPMM_LONG_ROW);
+  if (long_row <= 0) long_row = sizeof(ST) == 4 ? 512 : 1024;
   const bool dependent = tuning(ctx, BCLX_TUNE_SPMM_SCHEDULE) == 1;
   // counters: [0] k_spmm items, [1] k_spmm_long items, [2] listed very long / other long rows (2 x int32)
   unsigned long long* ctr = nullptr;
@@ -737,7 +745,7 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
     if (!dependent) BCLX_CK(cudaEventRecord(ctx->fork2_ev, ctx->side));
     const size_t lsmem = sizeof(LongSmem) * kLongWarps;
     BCLX_CK(cudaFuncSetAttribute(k_spmm_long<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
-    k_spmm_long<ST><<<(unsigned)spmm_long_blocks(ctx), kLongWarps * 32, lsmem, ls>>>(A, B, C, list, cnt, npanels,
+    k_spmm_long<ST><<<(unsigned)spmm_long_blocks(ctx, npanels), kLongWarps * 32, lsmem, ls>>>(A, B, C, list, cnt, npanels,
                                                                                     align_ok, ctr + 1);
     note_launch();
     BCLX_CK_LAUNCH();

@@ -490,18 +490,79 @@ def bench_spgemm_e2e(args, A, stream, flops, dist, shard=False):
     torch.cuda.synchronize()
     t = dist.max(e0.elapsed_time(e1) / 1e3)
     rate = flops * args.steps / t if shard else job_rate(dist.world, flops, args.steps, t)
-    pipelined = None
-    out_host.clear()  # the pinned output buffers go back before the second form allocates its own
+    forms = []
+    out_host.clear()  # the pinned output buffers go back before the other forms allocate their own
+    if not shard and dist.world == 1 and d2h < (4 << 30):
+        forms.append(bench_spgemm_e2e_streamed(args, A, host, dev, stream, flops))
     if not shard and dist.world == 1 and d2h < (16 << 30):
-        pipelined = bench_spgemm_e2e_pipelined(args, A, host, dev, stream, flops)
+        forms.append(bench_spgemm_e2e_pipelined(args, A, host, dev, stream, flops))
     one_call = {"value": rate / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": t * 1e3 / args.steps, "api": "containers.spgemm, then the output arrays copied back"}
-    if pipelined and pipelined.get("value") and pipelined["value"] > one_call["value"]:
-        pipelined["other"] = one_call
-        return pipelined
-    if pipelined:
-        one_call["other"] = pipelined
-    return one_call
+    forms = [one_call] + [f for f in forms if f and f.get("value")]
+    forms.sort(key=lambda f: -f["value"])
+    best = dict(forms[0])
+    if len(forms) > 1:
+        best["other"] = forms[1:] if len(forms) > 2 else forms[1]
+    return best
+
+
+def bench_spgemm_e2e_streamed(args, A, host, dev, stream, flops):
+    """The end-to-end step as a stream of products: every step copies A's
+    tiles in from pinned host memory, runs containers.spgemm and copies C's
+    arrays out to pinned host memory, with each step's copy out on a second
+    stream while the next step's product runs (two pinned output sets, used
+    in turn).  Every step's copies are inside the timed region, which ends
+    when the last copy out has landed."""
+    import torch
+    from bcl_b200.containers import SPMatrix, spgemm
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    copy = torch.cuda.Stream()
+    hbuf = [{}, {}]
+    state = {"d2h": 0}
+
+    def one(s):
+        for k in host:
+            dev[k].copy_(host[k], non_blocking=True)
+        Ad = SPMatrix(A.m, A.n, A.tm, A.tn, A.dtype, A.device, dev["tile_row_ptr"], dev["tile_offset"],
+                      dev["col_ind"], dev["vals"])
+        C = spgemm(Ad, Ad)
+        nnz = C.nnz()
+        done = torch.cuda.Event()
+        done.record(stream)
+        copy.wait_event(done)
+        hb = hbuf[s % 2]
+        d2h = 0
+        with torch.cuda.stream(copy):
+            for k in ("tile_row_ptr", "tile_offset", "col_ind", "vals"):
+                t = getattr(C, k)
+                cnt = nnz if k in ("col_ind", "vals") else t.numel()
+                if k not in hb or hb[k].numel() < cnt:
+                    hb[k] = torch.empty(max(cnt, 1), dtype=t.dtype).pin_memory()
+                hb[k][:cnt].copy_(t.reshape(-1)[:cnt], non_blocking=True)
+                t.record_stream(copy)  # C's memory is not reused before its copy out
+                d2h += cnt * t.element_size()
+        state["d2h"] = d2h
+
+    try:
+        for s in range(max(1, args.warmup)):
+            one(s)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(args.steps):
+            one(s)
+        last = torch.cuda.Event()
+        last.record(copy)
+        stream.wait_event(last)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    except Exception as e:  # e.g. pinned host memory
+        return {"value": None, "error": repr(e)[:200]}
+    t = e0.elapsed_time(e1) / 1e3
+    return {"value": flops * args.steps / t / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": state["d2h"], "ms_per_step": t * 1e3 / args.steps,
+            "api": "containers.spgemm per step, each step's C copied out on a second stream while the next "
+                   "step's product runs"}
 
 
 def bench_spgemm_e2e_pipelined(args, A, host, dev, stream, flops, block_rows=2):
@@ -1009,8 +1070,94 @@ def bench_spmm_e2e(args, A, B, C, stream, flops, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     t = dist.max(e0.elapsed_time(e1) / 1e3)
+    one_call = {"value": job_rate(dist.world, flops, args.steps, t) / 1e9, "unit": "GFLOP/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3 / args.steps,
+                "api": "containers.spmm with every copy on the product's stream"}
+    streamed = bench_spmm_e2e_streamed(args, A, B, C, host, hb, hc, stream, flops, dist)
+    forms = sorted([f for f in (one_call, streamed) if f and f.get("value")], key=lambda f: -f["value"])
+    best = dict(forms[0])
+    if len(forms) > 1:
+        best["other"] = forms[1]
+    return best
+
+
+def bench_spmm_e2e_streamed(args, A, B, C, host, hb, hc, stream, flops, dist):
+    """The end-to-end SpMM as a stream of products over two sets of device
+    buffers used in turn: each step copies A's tiles and B in from pinned
+    host memory on one stream, zeroes C and runs containers.spmm on the
+    product's stream, and copies C out on a third, so that one step's copy
+    in, another's product and a third's copy out overlap (PCIe carries both
+    directions at once).  Every step's copies are inside the timed region,
+    which ends when the last copy out has landed."""
+    import torch
+    from bcl_b200.containers import DMatrix, SPMatrix, spmm
+    ok, err, t_local = True, "", 0.0
+    try:
+        sets = []
+        for i in range(2):
+            dev = {k: torch.empty_like(v, device="cuda") for k, v in host.items()}
+            Bi = B if i == 0 else DMatrix(B.m, B.n, B.tm, B.tn, torch.empty_like(B.tiles))
+            Ci = C if i == 0 else DMatrix(C.m, C.n, C.tm, C.tn, torch.empty_like(C.tiles))
+            sets.append((dev, Bi, Ci))
+        cin, cout = torch.cuda.Stream(), torch.cuda.Stream()
+        loaded = [torch.cuda.Event(), torch.cuda.Event()]
+        computed = [torch.cuda.Event(), torch.cuda.Event()]
+        copied = [torch.cuda.Event(), torch.cuda.Event()]
+        used = [False, False]
+
+        def one(s):
+            i = s % 2
+            dev, Bi, Ci = sets[i]
+            if used[i]:
+                cin.wait_event(computed[i])  # set i's inputs are no longer read
+            with torch.cuda.stream(cin):
+                for k in host:
+                    dev[k].copy_(host[k], non_blocking=True)
+                Bi.tiles.copy_(hb, non_blocking=True)
+            loaded[i].record(cin)
+            stream.wait_event(loaded[i])
+            if used[i]:
+                stream.wait_event(copied[i])  # set i's C has been copied out
+            Ci.tiles.zero_()
+            Ad = SPMatrix(A.m, A.n, A.tm, A.tn, A.dtype, A.device, dev["tile_row_ptr"], dev["tile_offset"],
+                          dev["col_ind"], dev["vals"])
+            spmm(Ad, Bi, Ci)
+            computed[i].record(stream)
+            cout.wait_event(computed[i])
+            with torch.cuda.stream(cout):
+                hc.copy_(Ci.tiles, non_blocking=True)
+            copied[i].record(cout)
+            used[i] = True
+
+        for s in range(max(1, args.warmup)):
+            one(s)
+        torch.cuda.synchronize()
+    except Exception as e:  # e.g. device memory for the second set
+        ok, err = False, repr(e)[:200]
+    # every rank takes the same collective steps, failed or not
+    dist.barrier()
+    if ok:
+        try:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for s in range(args.steps):
+                one(s)
+            last = torch.cuda.Event()
+            last.record(cout)
+            stream.wait_event(last)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_local = e0.elapsed_time(e1) / 1e3
+        except Exception as e:
+            ok, err = False, repr(e)[:200]
+    t = dist.max(t_local)
+    if dist.max(0.0 if ok else 1.0) > 0.0:
+        return {"value": None, "error": err or "failed on another rank"}
+    h2d = sum(v.numel() * v.element_size() for v in host.values()) + hb.numel() * hb.element_size()
     return {"value": job_rate(dist.world, flops, args.steps, t) / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3 / args.steps}
+            "d2h_bytes_per_step": hc.numel() * hc.element_size(), "ms_per_step": t * 1e3 / args.steps,
+            "api": "containers.spmm per step over two buffer sets; copies in, products and copies out of "
+                   "different steps overlap on three streams"}
 
 
 # ---- CPU baselines (the reference's own code) -------------------------------------------

@@ -149,8 +149,8 @@ typedef enum {
   BCLX_TUNE_LEARN_TARGET = 1,      /* learned product: outputs aimed at per heavy item (64..448; 320) */
   BCLX_TUNE_BTABLE_MAX_BYTES = 2,  /* SpGEMM: largest B-row table built (0..; 2 GiB, or BCLX_BTABLE_MAX_BYTES) */
   BCLX_TUNE_SPMM_ROWS = 3,         /* SpMM: rows per warp item (0 = by product size, 1, 2, 4) */
-  BCLX_TUNE_SPMM_LONG_ROW = 4,     /* SpMM: entries from which a row goes to the long-row kernel (64..; 1024) */
-  BCLX_TUNE_SPMM_LONG_BLOCKS = 5,  /* SpMM: blocks of the long-row kernel (1..SMs; half the SMs) */
+  BCLX_TUNE_SPMM_LONG_ROW = 4,     /* SpMM: entries from which a row goes to the long-row kernel (0 = 512 FP32 / 1024 BF16, 64..) */
+  BCLX_TUNE_SPMM_LONG_BLOCKS = 5,  /* SpMM: blocks of the long-row kernel (0 = a quarter of the SMs per panel up to half, 1..SMs) */
   BCLX_TUNE_SPMM_SCHEDULE = 6,     /* SpMM: 0 = long rows on the side stream, 1 = dependent launch (0 or 1; 0) */
   BCLX_TUNE_ITEM_OUTPUTS = 7,      /* SpGEMM: outputs per heavy-row work item (512 or 1024; 512) */
   BCLX_TUNE_WIDE_LIGHT = 8,        /* SpGEMM: 1 = rows of tiles wider than 8192 columns may be light (0 or 1; 0) */
