@@ -486,13 +486,22 @@ __device__ __forceinline__ void walk_columns_ranged(const SpGridView& A, const S
 // X[ri*5 + 0..4] = log2(1 + A-row nnz over all stages), log2(1 + products),
 // log2(1 + longest referenced B row), (i + 1/2)/grid_m, (j + 1/2)/grid_n,
 // and the row's product count (capped at 2^31-1) to ub_out[ri].
+// `live` (or null: every C tile): the n_live[0] C tiles with at least one
+// stage; only their rows are walked (the others have no products).
 template <bool FEATURES>
 __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restrict__ light_list,
                            int32_t* __restrict__ heavy_list, int32_t* __restrict__ vheavy_list,
                            int32_t* __restrict__ counters, unsigned long long* __restrict__ products,
                            int heavy_min_cols, int light_ub, float* __restrict__ X,
-                           int32_t* __restrict__ ub_out, unsigned long long* __restrict__ queue, int grab) {
+                           int32_t* __restrict__ ub_out, unsigned long long* __restrict__ queue, int grab,
+                           const int32_t* __restrict__ live = nullptr, const int32_t* __restrict__ n_live = nullptr) {
   const int lane = lane_id();
+  // row item of walk position `it`
+  auto row_of = [&](unsigned long long it) -> int64_t {
+    if (!live) return (int64_t)it;
+    const int64_t lt = (int64_t)(it / (unsigned long long)g.tm);
+    return (int64_t)__ldg(live + lt) * g.tm + (int64_t)(it - (unsigned long long)lt * g.tm);
+  };
   unsigned long long mine = 0;
   // rows from a device counter, `grab` (at most 32) consecutive rows per
   // atomic (one atomic per row serialises on the counter when a fine grid has
@@ -500,7 +509,8 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
   // flight while the current rows are walked.  Lane q keeps the class of row
   // base + q, and the grab's rows are appended to each list with one atomic.
   grab = min(grab, 32);
-  const unsigned long long n_rows = (unsigned long long)g.n_row_items;
+  const unsigned long long n_rows =
+      live ? (unsigned long long)__ldg(n_live) * (unsigned long long)g.tm : (unsigned long long)g.n_row_items;
   unsigned long long base = 0;
   if (lane == 0) base = atomicAdd(queue, (unsigned long long)grab);
   base = __shfl_sync(kFull, base, 0);
@@ -510,7 +520,7 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
     const unsigned long long end = min(base + (unsigned long long)grab, n_rows);
     int cls = -1;  // list of row base + lane: 0 light, 1 heavy, 3 very heavy
     for (unsigned long long it = base; it < end; it++) {
-    const int64_t ri = (int64_t)it;
+    const int64_t ri = row_of(it);
     const RowInfo x = decode_row(g, ri);
     int64_t tot = 0, annz = 0;
     int32_t bmax = 0;
@@ -576,7 +586,7 @@ __global__ void k_classify(SpGridView A, SpGridView B, Geom g, int32_t* __restri
       if (lane == 0) pos = atomicAdd(&counters[c], __popc(m));
       pos = __shfl_sync(kFull, pos, 0) + __popc(m & ((1u << lane) - 1u));
       int32_t* list = c == 0 ? light_list : (c == 1 ? heavy_list : vheavy_list);
-      if (cls == c) list[pos] = (int32_t)(base + lane);
+      if (cls == c) list[pos] = (int32_t)row_of(base + lane);
     }
     base = __shfl_sync(kFull, nx, 0);
   }
@@ -735,6 +745,7 @@ __global__ void __launch_bounds__(256)
     const int nfb = (x.w + kFineCols - 1) / kFineCols;
     const uint32_t* bm = heavy_bitmaps + h * hbm_words;
     const int words = (x.w + 31) >> 5;
+    int tot = 0, first_nz = INT_MAX;
     for (int b = lane; b < nfb; b += 32) {
       int c = 0;
 #pragma unroll
@@ -743,9 +754,20 @@ __global__ void __launch_bounds__(256)
         if (w < words) c += __popc(__ldg(bm + w));
       }
       cnt[b] = c;
+      tot += c;
+      if (c > 0) first_nz = min(first_nz, b);
     }
+    tot = warp_sum(tot);
+    first_nz = __reduce_min_sync(kFull, first_nz);
     __syncwarp();
-    if (lane == 0) {
+    if (tot <= vcap) {
+      // one item, from the first block with outputs to the row's end: what
+      // the block-by-block cut below gives for such a row
+      if (lane == 0) {
+        if (FILL && tot > 0) items[first[h]] = HeavyItem{(int32_t)h, (int16_t)first_nz, (int16_t)nfb, 0, tot};
+        if (!FILL) n_items[h] = tot > 0 ? 1 : 0;
+      }
+    } else if (lane == 0) {
       int nit = 0, cur = 0, start = 0, rel = 0;
       int64_t out = FILL ? first[h] : 0;
       for (int b = 0; b < nfb; b++) {
@@ -1482,6 +1504,23 @@ __global__ void k_stage_map(SpGridView A, SpGridView B, Geom g, int32_t* __restr
   }
 }
 
+// C tiles with at least one stage (scount[t] > 0) into live[], their number
+// to *n_live (one atomic per warp; the order is immaterial).
+__global__ void k_live_tiles(const int32_t* __restrict__ scount, int64_t nt, int32_t* __restrict__ live,
+                             int32_t* __restrict__ n_live) {
+  const int lane = lane_id();
+  const int64_t end = (nt + 31) & ~int64_t(31);  // whole warps run every iteration
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < end; t += (int64_t)gridDim.x * blockDim.x) {
+    const bool on = t < nt && scount[t] > 0;
+    const unsigned m = __ballot_sync(kFull, on);
+    if (m == 0) continue;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(n_live, __popc(m));
+    base = __shfl_sync(kFull, base, 0);
+    if (on) live[base + __popc(m & ((1u << lane) - 1u))] = (int32_t)t;
+  }
+}
+
 constexpr int64_t kStageMapMinGrid = 17;
 
 static int build_stage_map(Context* ctx, const SpGridView& A, const SpGridView& B, bclx_spgemm_plan_s* P, Geom& g) {
@@ -1554,16 +1593,26 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   const int heavy_min_cols = tuning(ctx, BCLX_TUNE_WIDE_LIGHT) ? INT_MAX : 8192 + 1;
   P->light_ub_max = (int)tuning(ctx, BCLX_TUNE_LIGHT_UB);
   P->vcap = (int)tuning(ctx, BCLX_TUNE_ITEM_OUTPUTS);
+  int32_t* live = nullptr;  // C tiles with stages (when the stage map says which)
   if (nri > 0) {
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
+    const int64_t nt = g.gm * g.gn;
+    if (g.scount) {
+      BCLX_TRY(scratch_alloc_n(ctx, &live, (size_t)nt + 1));
+      BCLX_CK(cudaMemsetAsync(live + nt, 0, sizeof(int32_t), ctx->stream));
+      k_live_tiles<<<grid_for(ctx, nt / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(g.scount, nt, live, live + nt);
+      note_launch();
+      BCLX_CK_LAUNCH();
+    }
     k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, heavy_min_cols, P->light_ub_max,
-        nullptr, nullptr, P->queue + 1, queue_grab(ctx, nri, 8, 16, 32, 8));
+        nullptr, nullptr, P->queue + 1, queue_grab(ctx, nri, 8, 16, 32, 8), live, live ? live + nt : nullptr);
     note_launch();
     BCLX_CK_LAUNCH();
   }
   BCLX_CK(cudaMemcpyAsync(ctx->pinned, P->counters, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   BCLX_CK(cudaMemcpyAsync(ctx->pinned + 2, P->products_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  if (live) scratch_free(ctx, live);
   BCLX_CK(cudaStreamSynchronize(ctx->stream));
   int32_t cnts[4];
   std::memcpy(cnts, ctx->pinned, sizeof(cnts));
