@@ -629,7 +629,7 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
     k_symbolic(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
                const int32_t* __restrict__ heavy_list, int n_light, int n_heavy, int n_vheavy,
                int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
-               unsigned long long* __restrict__ queue, int grab) {
+               int16_t* __restrict__ heavy_fb0, unsigned long long* __restrict__ queue, int grab) {
   __shared__ uint32_t bm_all[kWarpsSym][kMaxWords];
   uint32_t* bm = bm_all[threadIdx.x >> 5];
   const int lane = lane_id();
@@ -651,15 +651,20 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
     __syncwarp();
     walk_columns(A, B, g, x, 0, 1, [&](int32_t j) { atomicOr(&bm[j >> 5], 1u << (j & 31)); });
     __syncwarp();
-    int cnt = 0;
+    int cnt = 0, w0 = INT_MAX;
     uint32_t* out = heavy ? heavy_bitmaps + idx * hbm_words : nullptr;
     for (int w = lane; w < words; w += 32) {
       const uint32_t v = bm[w];
       if (heavy) out[w] = v;
       cnt += __popc(v);
+      if (v && w < w0) w0 = w;
     }
     cnt = warp_sum(cnt);
-    if (lane == 0) row_count[ri] = cnt;
+    if (heavy && heavy_fb0) w0 = __reduce_min_sync(kFull, w0);
+    if (lane == 0) {
+      row_count[ri] = cnt;
+      if (heavy && heavy_fb0) heavy_fb0[idx] = (int16_t)(cnt > 0 ? w0 / (kFineCols / 32) : 0);
+    }
     __syncwarp();
     }
     base = __shfl_sync(kFull, nx, 0);
@@ -669,24 +674,32 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
 // ... and one block per very heavy row, its warps sharing the bitmap.
 __global__ void __launch_bounds__(kWarpsSym * 32)
     k_symbolic_block(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ heavy_list, int n_vheavy,
-                     int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words) {
+                     int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
+                     int16_t* __restrict__ heavy_fb0) {
   __shared__ uint32_t bm[kMaxWords];
   __shared__ int red[kWarpsSym];
+  __shared__ int first_word;
   const int wid = threadIdx.x >> 5;
   for (int64_t h = blockIdx.x; h < n_vheavy; h += gridDim.x) {
     const int64_t ri = heavy_list[h];
     const RowInfo x = decode_row(g, ri);
     const int words = (x.w + 31) >> 5;
     for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
+    if (threadIdx.x == 0) first_word = INT_MAX;
     __syncthreads();
     walk_columns(A, B, g, x, wid, kWarpsSym, [&](int32_t j) { atomicOr(&bm[j >> 5], 1u << (j & 31)); });
     __syncthreads();
-    int cnt = 0;
+    int cnt = 0, w0 = INT_MAX;
     uint32_t* out = heavy_bitmaps + h * hbm_words;
     for (int w = threadIdx.x; w < words; w += blockDim.x) {
       const uint32_t v = bm[w];
       out[w] = v;
       cnt += __popc(v);
+      if (v && w < w0) w0 = w;
+    }
+    if (heavy_fb0) {
+      w0 = __reduce_min_sync(kFull, w0);
+      if ((threadIdx.x & 31) == 0 && w0 != INT_MAX) atomicMin(&first_word, w0);
     }
     cnt = warp_sum(cnt);
     if ((threadIdx.x & 31) == 0) red[wid] = cnt;
@@ -695,6 +708,7 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
       int t = 0;
       for (int q = 0; q < kWarpsSym; q++) t += red[q];
       row_count[ri] = t;
+      if (heavy_fb0) heavy_fb0[h] = (int16_t)(t > 0 ? first_word / (kFineCols / 32) : 0);
     }
     __syncthreads();
   }
@@ -733,7 +747,8 @@ template <bool FILL>
 __global__ void __launch_bounds__(256)
     k_cut_heavy(Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
                 const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, int32_t* __restrict__ n_items,
-                const int64_t* __restrict__ first, HeavyItem* __restrict__ items, int vcap) {
+                const int64_t* __restrict__ first, HeavyItem* __restrict__ items, int vcap,
+                const int32_t* __restrict__ row_count = nullptr, const int16_t* __restrict__ fb0 = nullptr) {
   __shared__ int32_t cnt_all[8][kMaxCols / kFineCols];
   int32_t* cnt = cnt_all[threadIdx.x >> 5];
   const int lane = lane_id();
@@ -741,8 +756,21 @@ __global__ void __launch_bounds__(256)
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   constexpr int kWordsPerBlock = kFineCols / 32;
   for (int64_t h = warp; h < n_heavy; h += nwarps) {
-    const RowInfo x = decode_row(g, heavy_list[h]);
+    const int64_t ri = heavy_list[h];
+    const RowInfo x = decode_row(g, ri);
     const int nfb = (x.w + kFineCols - 1) / kFineCols;
+    if (fb0 && row_count) {
+      // counted by the symbolic pass: a row whose outputs fit one item needs
+      // no look at its bitmap
+      const int tot = __ldg(row_count + ri);
+      if (tot <= vcap) {
+        if (lane == 0) {
+          if (FILL && tot > 0) items[first[h]] = HeavyItem{(int32_t)h, __ldg(fb0 + h), (int16_t)nfb, 0, tot};
+          if (!FILL) n_items[h] = tot > 0 ? 1 : 0;
+        }
+        continue;
+      }
+    }
     const uint32_t* bm = heavy_bitmaps + h * hbm_words;
     const int words = (x.w + 31) >> 5;
     int tot = 0, first_nz = INT_MAX;
@@ -1280,6 +1308,7 @@ struct bclx_spgemm_plan_s {
   int32_t* row_count = nullptr;
   int64_t* row_offset = nullptr;
   uint32_t* heavy_bitmaps = nullptr;
+  int16_t* heavy_fb0 = nullptr;  // first fine block with outputs of each heavy row (or null)
   int32_t* heavy_nitems = nullptr;
   int64_t* heavy_first = nullptr;
   HeavyItem* heavy_items = nullptr;
@@ -1360,9 +1389,10 @@ struct bclx_spgemm_plan_s {
     temp_val = redo_val = nullptr;
     void* ps[] = {queue, light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
                   heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset,
-                  smap_own, scount_own, rot_own};
+                  smap_own, scount_own, rot_own, heavy_fb0};
     for (void* p : ps) scratch_free(ctx, p);
     queue = nullptr;
+    heavy_fb0 = nullptr;
     smap_own = scount_own = rot_own = nullptr;
     light_list = heavy_list = vheavy_list = heavy_tmp = counters = row_count = heavy_nitems = tab = id_rp = id_ci = nullptr;
     products_dev = nullptr;
@@ -1432,7 +1462,7 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
       st = ctx->side;
     }
     k_symbolic_block<<<grid_for(ctx, P->n_vheavy, 1, 8), kWarpsSym * 32, 0, st>>>(
-        A, B, P->g, P->heavy_list, (int)P->n_vheavy, P->row_count, P->heavy_bitmaps, P->hbm_words);
+        A, B, P->g, P->heavy_list, (int)P->n_vheavy, P->row_count, P->heavy_bitmaps, P->hbm_words, P->heavy_fb0);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1442,7 +1472,7 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
     BCLX_CK(cudaMemsetAsync(P->queue, 0, sizeof(unsigned long long), ctx->stream));
     k_symbolic<<<grid_for(ctx, rows, kWarpsSym, 8), kWarpsSym * 32, 0, ctx->stream>>>(
         A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, (int)P->n_heavy, (int)P->n_vheavy,
-        P->row_count, P->heavy_bitmaps, P->hbm_words, P->queue, queue_grab(ctx, rows, kWarpsSym, 8, 8));
+        P->row_count, P->heavy_bitmaps, P->hbm_words, P->heavy_fb0, P->queue, queue_grab(ctx, rows, kWarpsSym, 8, 8));
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1629,6 +1659,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
                             cudaMemcpyDeviceToDevice, ctx->stream));
 
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_bitmaps, (size_t)P->n_heavy * P->hbm_words));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_fb0, (size_t)P->n_heavy));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_nitems, P->n_heavy));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_first, P->n_heavy + 1));
   BCLX_TRY(launch_symbolic(ctx, A, B, P, true));
@@ -1644,7 +1675,8 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   if (P->n_heavy > 0) {
     const unsigned blocks = grid_for(ctx, P->n_heavy, 8, 8);
     k_cut_heavy<false><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
-                                                        P->hbm_words, P->heavy_nitems, nullptr, nullptr, P->vcap);
+                                                        P->hbm_words, P->heavy_nitems, nullptr, nullptr, P->vcap,
+                                                        P->row_count, P->heavy_fb0);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1666,7 +1698,8 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_items, P->n_heavy_items));
     const unsigned blocks = grid_for(ctx, P->n_heavy, 8, 8);
     k_cut_heavy<true><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
-                                                       P->hbm_words, nullptr, P->heavy_first, P->heavy_items, P->vcap);
+                                                       P->hbm_words, nullptr, P->heavy_first, P->heavy_items, P->vcap,
+                                                       P->row_count, P->heavy_fb0);
     note_launch();
     BCLX_CK_LAUNCH();
   }
