@@ -519,8 +519,14 @@ def bench_spgemm_e2e_streamed(args, A, host, dev, stream, flops):
     copy = torch.cuda.Stream()
     hbuf = [{}, {}]
     state = {"d2h": 0}
+    copied = [torch.cuda.Event(), torch.cuda.Event()]
+    used = [False, False]
 
     def one(s):
+        if used[s % 2]:
+            # at most two steps' C in flight: step s - 2's copy out has landed
+            # (so its C's memory goes back to the pool before this product)
+            stream.wait_event(copied[s % 2])
         for k in host:
             dev[k].copy_(host[k], non_blocking=True)
         Ad = SPMatrix(A.m, A.n, A.tm, A.tn, A.dtype, A.device, dev["tile_row_ptr"], dev["tile_offset"],
@@ -541,6 +547,8 @@ def bench_spgemm_e2e_streamed(args, A, host, dev, stream, flops):
                 hb[k][:cnt].copy_(t.reshape(-1)[:cnt], non_blocking=True)
                 t.record_stream(copy)  # C's memory is not reused before its copy out
                 d2h += cnt * t.element_size()
+        copied[s % 2].record(copy)
+        used[s % 2] = True
         state["d2h"] = d2h
 
     try:
