@@ -1567,6 +1567,21 @@ static int build_stage_map(Context* ctx, const SpGridView& A, const SpGridView& 
   return BCLX_OK;
 }
 
+// With a stage map: the C tiles that have stages, into a new scratch array
+// (their number in its last slot, written by the device); *live stays null
+// without a map (every tile is walked).
+static int build_live_tiles(Context* ctx, const Geom& g, int32_t** live) {
+  *live = nullptr;
+  if (!g.scount) return BCLX_OK;
+  const int64_t nt = g.gm * g.gn;
+  BCLX_TRY(scratch_alloc_n(ctx, live, (size_t)nt + 1));
+  BCLX_CK(cudaMemsetAsync(*live + nt, 0, sizeof(int32_t), ctx->stream));
+  k_live_tiles<<<grid_for(ctx, nt / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(g.scount, nt, *live, *live + nt);
+  note_launch();
+  BCLX_CK_LAUNCH();
+  return BCLX_OK;
+}
+
 // B-row table (k_btable) when it fits the context's BCLX_TUNE_BTABLE_MAX_BYTES
 // (default 2 GiB); otherwise none and the walks find column-block ranges by
 // binary search.
@@ -1627,13 +1642,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
   if (nri > 0) {
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
     const int64_t nt = g.gm * g.gn;
-    if (g.scount) {
-      BCLX_TRY(scratch_alloc_n(ctx, &live, (size_t)nt + 1));
-      BCLX_CK(cudaMemsetAsync(live + nt, 0, sizeof(int32_t), ctx->stream));
-      k_live_tiles<<<grid_for(ctx, nt / 32 + 1, 8, 8), 256, 0, ctx->stream>>>(g.scount, nt, live, live + nt);
-      note_launch();
-      BCLX_CK_LAUNCH();
-    }
+    BCLX_TRY(build_live_tiles(ctx, g, &live));
     k_classify<false><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, heavy_min_cols, P->light_ub_max,
         nullptr, nullptr, P->queue + 1, queue_grab(ctx, nri, 8, 16, 32, 8), live, live ? live + nt : nullptr);
@@ -2250,14 +2259,18 @@ static int learned_impl(Context* ctx, const SpGridView& A, const SpGridView& B, 
   BCLX_CK(cudaMemsetAsync(P->counters, 0, 4 * sizeof(int32_t), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P->products_dev, 0, sizeof(unsigned long long), ctx->stream));
   BCLX_CK(cudaMemsetAsync(P->row_count, 0, sizeof(int32_t) * (nri > 0 ? nri : 1), ctx->stream));
+  int32_t* live = nullptr;  // C tiles with stages (rows of the others have no products)
   if (nri > 0) {
     BCLX_CK(cudaMemsetAsync(P->queue + 1, 0, sizeof(unsigned long long), ctx->stream));
+    BCLX_TRY(build_live_tiles(ctx, g, &live));
+    const int64_t nt = g.gm * g.gn;
     k_classify<true><<<grid_for(ctx, nri, 8, 16), 256, 0, ctx->stream>>>(
         A, B, g, P->light_list, P->heavy_tmp, P->vheavy_list, P->counters, P->products_dev, tuning(ctx, BCLX_TUNE_WIDE_LIGHT) ? INT_MAX : 8192 + 1,
         (int)tuning(ctx, BCLX_TUNE_LIGHT_UB), P->feat, P->ub,
-        P->queue + 1, queue_grab(ctx, nri, 8, 16, 32, 8));
+        P->queue + 1, queue_grab(ctx, nri, 8, 16, 32, 8), live, live ? live + nt : nullptr);
     note_launch();
     BCLX_CK_LAUNCH();
+    if (live) scratch_free(ctx, live);
   }
   int32_t cnts[4];
   int64_t prod = 0;
