@@ -629,7 +629,7 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
     k_symbolic(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ light_list,
                const int32_t* __restrict__ heavy_list, int n_light, int n_heavy, int n_vheavy,
                int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
-               int16_t* __restrict__ heavy_fb0, unsigned long long* __restrict__ queue, int grab) {
+               int16_t* __restrict__ heavy_span, unsigned long long* __restrict__ queue, int grab) {
   __shared__ uint32_t bm_all[kWarpsSym][kMaxWords];
   uint32_t* bm = bm_all[threadIdx.x >> 5];
   const int lane = lane_id();
@@ -651,19 +651,28 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
     __syncwarp();
     walk_columns(A, B, g, x, 0, 1, [&](int32_t j) { atomicOr(&bm[j >> 5], 1u << (j & 31)); });
     __syncwarp();
-    int cnt = 0, w0 = INT_MAX;
+    int cnt = 0, w0 = INT_MAX, w1 = -1;
     uint32_t* out = heavy ? heavy_bitmaps + idx * hbm_words : nullptr;
     for (int w = lane; w < words; w += 32) {
       const uint32_t v = bm[w];
       if (heavy) out[w] = v;
       cnt += __popc(v);
-      if (v && w < w0) w0 = w;
+      if (v) {
+        w0 = min(w0, w);
+        w1 = max(w1, w);
+      }
     }
     cnt = warp_sum(cnt);
-    if (heavy && heavy_fb0) w0 = __reduce_min_sync(kFull, w0);
+    if (heavy && heavy_span) {
+      w0 = __reduce_min_sync(kFull, w0);
+      w1 = __reduce_max_sync(kFull, w1);
+    }
     if (lane == 0) {
       row_count[ri] = cnt;
-      if (heavy && heavy_fb0) heavy_fb0[idx] = (int16_t)(cnt > 0 ? w0 / (kFineCols / 32) : 0);
+      if (heavy && heavy_span) {
+        heavy_span[2 * idx] = (int16_t)(cnt > 0 ? w0 / (kFineCols / 32) : 0);
+        heavy_span[2 * idx + 1] = (int16_t)(cnt > 0 ? w1 / (kFineCols / 32) + 1 : 0);
+      }
     }
     __syncwarp();
     }
@@ -675,31 +684,41 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
 __global__ void __launch_bounds__(kWarpsSym * 32)
     k_symbolic_block(SpGridView A, SpGridView B, Geom g, const int32_t* __restrict__ heavy_list, int n_vheavy,
                      int32_t* __restrict__ row_count, uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words,
-                     int16_t* __restrict__ heavy_fb0) {
+                     int16_t* __restrict__ heavy_span) {
   __shared__ uint32_t bm[kMaxWords];
   __shared__ int red[kWarpsSym];
-  __shared__ int first_word;
+  __shared__ int first_word, last_word;
   const int wid = threadIdx.x >> 5;
   for (int64_t h = blockIdx.x; h < n_vheavy; h += gridDim.x) {
     const int64_t ri = heavy_list[h];
     const RowInfo x = decode_row(g, ri);
     const int words = (x.w + 31) >> 5;
     for (int w = threadIdx.x; w < words; w += blockDim.x) bm[w] = 0u;
-    if (threadIdx.x == 0) first_word = INT_MAX;
+    if (threadIdx.x == 0) {
+      first_word = INT_MAX;
+      last_word = -1;
+    }
     __syncthreads();
     walk_columns(A, B, g, x, wid, kWarpsSym, [&](int32_t j) { atomicOr(&bm[j >> 5], 1u << (j & 31)); });
     __syncthreads();
-    int cnt = 0, w0 = INT_MAX;
+    int cnt = 0, w0 = INT_MAX, w1 = -1;
     uint32_t* out = heavy_bitmaps + h * hbm_words;
     for (int w = threadIdx.x; w < words; w += blockDim.x) {
       const uint32_t v = bm[w];
       out[w] = v;
       cnt += __popc(v);
-      if (v && w < w0) w0 = w;
+      if (v) {
+        w0 = min(w0, w);
+        w1 = max(w1, w);
+      }
     }
-    if (heavy_fb0) {
+    if (heavy_span) {
       w0 = __reduce_min_sync(kFull, w0);
-      if ((threadIdx.x & 31) == 0 && w0 != INT_MAX) atomicMin(&first_word, w0);
+      w1 = __reduce_max_sync(kFull, w1);
+      if ((threadIdx.x & 31) == 0 && w0 != INT_MAX) {
+        atomicMin(&first_word, w0);
+        atomicMax(&last_word, w1);
+      }
     }
     cnt = warp_sum(cnt);
     if ((threadIdx.x & 31) == 0) red[wid] = cnt;
@@ -708,7 +727,10 @@ __global__ void __launch_bounds__(kWarpsSym * 32)
       int t = 0;
       for (int q = 0; q < kWarpsSym; q++) t += red[q];
       row_count[ri] = t;
-      if (heavy_fb0) heavy_fb0[h] = (int16_t)(t > 0 ? first_word / (kFineCols / 32) : 0);
+      if (heavy_span) {
+        heavy_span[2 * h] = (int16_t)(t > 0 ? first_word / (kFineCols / 32) : 0);
+        heavy_span[2 * h + 1] = (int16_t)(t > 0 ? last_word / (kFineCols / 32) + 1 : 0);
+      }
     }
     __syncthreads();
   }
@@ -748,7 +770,7 @@ __global__ void __launch_bounds__(256)
     k_cut_heavy(Geom g, const int32_t* __restrict__ heavy_list, int n_heavy,
                 const uint32_t* __restrict__ heavy_bitmaps, int64_t hbm_words, int32_t* __restrict__ n_items,
                 const int64_t* __restrict__ first, HeavyItem* __restrict__ items, int vcap,
-                const int32_t* __restrict__ row_count = nullptr, const int16_t* __restrict__ fb0 = nullptr) {
+                const int32_t* __restrict__ row_count = nullptr, const int16_t* __restrict__ span = nullptr) {
   __shared__ int32_t cnt_all[8][kMaxCols / kFineCols];
   int32_t* cnt = cnt_all[threadIdx.x >> 5];
   const int lane = lane_id();
@@ -759,13 +781,15 @@ __global__ void __launch_bounds__(256)
     const int64_t ri = heavy_list[h];
     const RowInfo x = decode_row(g, ri);
     const int nfb = (x.w + kFineCols - 1) / kFineCols;
-    if (fb0 && row_count) {
+    if (span && row_count) {
       // counted by the symbolic pass: a row whose outputs fit one item needs
-      // no look at its bitmap
+      // no look at its bitmap; the item spans its first to its last block
+      // with outputs
       const int tot = __ldg(row_count + ri);
       if (tot <= vcap) {
         if (lane == 0) {
-          if (FILL && tot > 0) items[first[h]] = HeavyItem{(int32_t)h, __ldg(fb0 + h), (int16_t)nfb, 0, tot};
+          if (FILL && tot > 0)
+            items[first[h]] = HeavyItem{(int32_t)h, __ldg(span + 2 * h), __ldg(span + 2 * h + 1), 0, tot};
           if (!FILL) n_items[h] = tot > 0 ? 1 : 0;
         }
         continue;
@@ -773,7 +797,7 @@ __global__ void __launch_bounds__(256)
     }
     const uint32_t* bm = heavy_bitmaps + h * hbm_words;
     const int words = (x.w + 31) >> 5;
-    int tot = 0, first_nz = INT_MAX;
+    int tot = 0, first_nz = INT_MAX, last_nz = -1;
     for (int b = lane; b < nfb; b += 32) {
       int c = 0;
 #pragma unroll
@@ -783,23 +807,29 @@ __global__ void __launch_bounds__(256)
       }
       cnt[b] = c;
       tot += c;
-      if (c > 0) first_nz = min(first_nz, b);
+      if (c > 0) {
+        first_nz = min(first_nz, b);
+        last_nz = max(last_nz, b);
+      }
     }
     tot = warp_sum(tot);
     first_nz = __reduce_min_sync(kFull, first_nz);
+    last_nz = __reduce_max_sync(kFull, last_nz);
     __syncwarp();
     if (tot <= vcap) {
-      // one item, from the first block with outputs to the row's end: what
-      // the block-by-block cut below gives for such a row
+      // one item, from the first to the last block with outputs: what the
+      // block-by-block cut below gives for such a row
       if (lane == 0) {
-        if (FILL && tot > 0) items[first[h]] = HeavyItem{(int32_t)h, (int16_t)first_nz, (int16_t)nfb, 0, tot};
+        if (FILL && tot > 0)
+          items[first[h]] = HeavyItem{(int32_t)h, (int16_t)first_nz, (int16_t)(last_nz + 1), 0, tot};
         if (!FILL) n_items[h] = tot > 0 ? 1 : 0;
       }
     } else if (lane == 0) {
-      int nit = 0, cur = 0, start = 0, rel = 0;
+      int nit = 0, cur = 0, start = 0, rel = 0, last = -1;
       int64_t out = FILL ? first[h] : 0;
       for (int b = 0; b < nfb; b++) {
         const int c = cnt[b];
+        if (c > 0) last = b;
         if (cur > 0 && cur + c > vcap) {
           if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)b, rel, cur};
           nit++;
@@ -810,8 +840,8 @@ __global__ void __launch_bounds__(256)
         if (cur == 0 && c == 0) start = b + 1;
         cur += c;
       }
-      if (cur > 0) {
-        if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)nfb, rel, cur};
+      if (cur > 0) {  // the last item ends after the row's last block with outputs
+        if (FILL) items[out++] = HeavyItem{(int32_t)h, (int16_t)start, (int16_t)(last + 1), rel, cur};
         nit++;
       }
       if (!FILL) n_items[h] = nit;
@@ -1308,7 +1338,7 @@ struct bclx_spgemm_plan_s {
   int32_t* row_count = nullptr;
   int64_t* row_offset = nullptr;
   uint32_t* heavy_bitmaps = nullptr;
-  int16_t* heavy_fb0 = nullptr;  // first fine block with outputs of each heavy row (or null)
+  int16_t* heavy_span = nullptr;  // per heavy row: first fine block with outputs, one past the last (or null)
   int32_t* heavy_nitems = nullptr;
   int64_t* heavy_first = nullptr;
   HeavyItem* heavy_items = nullptr;
@@ -1389,10 +1419,10 @@ struct bclx_spgemm_plan_s {
     temp_val = redo_val = nullptr;
     void* ps[] = {queue, light_list, heavy_list, vheavy_list, heavy_tmp, counters, products_dev, row_count, row_offset, heavy_bitmaps,
                   heavy_nitems, heavy_first, heavy_items, tab, id_rp, id_ci, id_v, id_desc, acc_tile_offset,
-                  smap_own, scount_own, rot_own, heavy_fb0};
+                  smap_own, scount_own, rot_own, heavy_span};
     for (void* p : ps) scratch_free(ctx, p);
     queue = nullptr;
-    heavy_fb0 = nullptr;
+    heavy_span = nullptr;
     smap_own = scount_own = rot_own = nullptr;
     light_list = heavy_list = vheavy_list = heavy_tmp = counters = row_count = heavy_nitems = tab = id_rp = id_ci = nullptr;
     products_dev = nullptr;
@@ -1462,7 +1492,7 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
       st = ctx->side;
     }
     k_symbolic_block<<<grid_for(ctx, P->n_vheavy, 1, 8), kWarpsSym * 32, 0, st>>>(
-        A, B, P->g, P->heavy_list, (int)P->n_vheavy, P->row_count, P->heavy_bitmaps, P->hbm_words, P->heavy_fb0);
+        A, B, P->g, P->heavy_list, (int)P->n_vheavy, P->row_count, P->heavy_bitmaps, P->hbm_words, P->heavy_span);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1472,7 +1502,7 @@ static int launch_symbolic(Context* ctx, const SpGridView& A, const SpGridView& 
     BCLX_CK(cudaMemsetAsync(P->queue, 0, sizeof(unsigned long long), ctx->stream));
     k_symbolic<<<grid_for(ctx, rows, kWarpsSym, 8), kWarpsSym * 32, 0, ctx->stream>>>(
         A, B, P->g, P->light_list, P->heavy_list, (int)P->n_light, (int)P->n_heavy, (int)P->n_vheavy,
-        P->row_count, P->heavy_bitmaps, P->hbm_words, P->heavy_fb0, P->queue, queue_grab(ctx, rows, kWarpsSym, 8, 8));
+        P->row_count, P->heavy_bitmaps, P->hbm_words, P->heavy_span, P->queue, queue_grab(ctx, rows, kWarpsSym, 8, 8));
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1584,7 +1614,9 @@ static int build_live_tiles(Context* ctx, const Geom& g, int32_t** live) {
 
 // B-row table (k_btable) when it fits the context's BCLX_TUNE_BTABLE_MAX_BYTES
 // (default 2 GiB); otherwise none and the walks find column-block ranges by
-// binary search.
+// binary search.  (A larger table pays where memory allows: R-MAT s20 on
+// 64x64 tiles, 17.4 GB, 638 against 679 ms per product; but the table is
+// sized before the product's bitmaps and C are, so the default stays small.)
 static int64_t btable_cap(const Context* ctx) { return tuning(ctx, BCLX_TUNE_BTABLE_MAX_BYTES); }
 
 // With `side`, the table is allocated in stream order on the main stream and
@@ -1668,7 +1700,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
                             cudaMemcpyDeviceToDevice, ctx->stream));
 
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_bitmaps, (size_t)P->n_heavy * P->hbm_words));
-  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_fb0, (size_t)P->n_heavy));
+  BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_span, 2 * (size_t)P->n_heavy));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_nitems, P->n_heavy));
   BCLX_TRY(scratch_alloc_n(ctx, &P->heavy_first, P->n_heavy + 1));
   BCLX_TRY(launch_symbolic(ctx, A, B, P, true));
@@ -1685,7 +1717,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     const unsigned blocks = grid_for(ctx, P->n_heavy, 8, 8);
     k_cut_heavy<false><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
                                                         P->hbm_words, P->heavy_nitems, nullptr, nullptr, P->vcap,
-                                                        P->row_count, P->heavy_fb0);
+                                                        P->row_count, P->heavy_span);
     note_launch();
     BCLX_CK_LAUNCH();
   }
@@ -1708,7 +1740,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     const unsigned blocks = grid_for(ctx, P->n_heavy, 8, 8);
     k_cut_heavy<true><<<blocks, 256, 0, ctx->stream>>>(g, P->heavy_list, (int)P->n_heavy, P->heavy_bitmaps,
                                                        P->hbm_words, nullptr, P->heavy_first, P->heavy_items, P->vcap,
-                                                       P->row_count, P->heavy_fb0);
+                                                       P->row_count, P->heavy_span);
     note_launch();
     BCLX_CK_LAUNCH();
   }
