@@ -46,7 +46,8 @@ struct Context {
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
-  int64_t* pinned = nullptr;  // host readback slots
+  int64_t* pinned = nullptr;      // host readback slots (page-locked, mapped)
+  int64_t* pinned_dev = nullptr;  // the same slots as the device addresses them
   // A second stream for planning work that overlaps the main stream (created
   // on first use), with events to fork from and join back to the main stream.
   cudaStream_t side = nullptr;

@@ -248,9 +248,11 @@ int bclx_context_create(int device, bclx_context_t* out) {
     uint64_t thr = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
-  if (cudaMallocHost(&ctx->pinned, 8 * sizeof(int64_t)) != cudaSuccess) {
+  if (cudaHostAlloc(&ctx->pinned, 8 * sizeof(int64_t), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(&ctx->pinned_dev, ctx->pinned, 0) != cudaSuccess) {
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
     delete ctx;
-    set_last_error("cudaMallocHost failed");
+    set_last_error("cudaHostAlloc (mapped readback slots) failed");
     return BCLX_ERR_NO_MEMORY;
   }
   *out = reinterpret_cast<bclx_context_t>(ctx);

@@ -43,7 +43,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace bclx {
@@ -475,6 +477,45 @@ __device__ __forceinline__ void walk_columns_ranged(const SpGridView& A, const S
       }
     }
   }
+}
+
+// ---- host reads ----------------------------------------------------------------------
+//
+// The planning passes read a few sizes back to the host.  A one-warp kernel
+// stores them into the context's mapped page-locked slots instead of a
+// device-to-host copy, which would queue behind any large copy the caller
+// has running in the same direction (a previous product's output on its way
+// to the host).
+
+struct ReadBack {
+  const void* src[4];
+  int32_t bytes[4];  // at most 8 each
+  int32_t slot[4];   // 8-byte destination slot
+  int32_t n;
+};
+
+__global__ void k_read_back(ReadBack r, int64_t* __restrict__ dst) {
+  const int t = threadIdx.x;
+  for (int i = 0; i < r.n; i++)
+    if (t < r.bytes[i])
+      reinterpret_cast<volatile unsigned char*>(dst + r.slot[i])[t] = reinterpret_cast<const unsigned char*>(r.src[i])[t];
+}
+
+// Store up to four values (each at most 8 bytes) into ctx->pinned[slot] on
+// the context's stream; the host reads them after synchronizing the stream.
+static int read_back(Context* ctx, std::initializer_list<std::tuple<const void*, int, int>> items) {
+  ReadBack r{};
+  for (const auto& it : items) {
+    if (r.n == 4 || std::get<1>(it) > 8) return BCLX_ERR_INVALID;
+    r.src[r.n] = std::get<0>(it);
+    r.bytes[r.n] = std::get<1>(it);
+    r.slot[r.n] = std::get<2>(it);
+    r.n++;
+  }
+  k_read_back<<<1, 32, 0, ctx->stream>>>(r, ctx->pinned_dev);
+  note_launch();
+  BCLX_CK_LAUNCH();
+  return BCLX_OK;
 }
 
 // ---- planning --------------------------------------------------------------------
@@ -1681,8 +1722,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     note_launch();
     BCLX_CK_LAUNCH();
   }
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned, P->counters, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 2, P->products_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_TRY(read_back(ctx, {{P->counters, 8, 0}, {P->counters + 2, 8, 1}, {P->products_dev, 8, 2}}));
   if (live) scratch_free(ctx, live);
   BCLX_CK(cudaStreamSynchronize(ctx->stream));
   int32_t cnts[4];
@@ -1722,10 +1762,7 @@ static int symbolic_impl(Context* ctx, const SpGridView& A, const SpGridView& B,
     BCLX_CK_LAUNCH();
   }
   BCLX_TRY(exclusive_scan_i32(ctx, P->heavy_nitems, P->heavy_first, P->n_heavy));
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned, P->row_offset + nri, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 1, P->heavy_first + P->n_heavy, sizeof(int64_t), cudaMemcpyDeviceToHost,
-                          ctx->stream));
-  BCLX_CK(cudaMemcpyAsync(ctx->pinned + 2, P->counters + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  BCLX_TRY(read_back(ctx, {{P->row_offset + nri, 8, 0}, {P->heavy_first + P->n_heavy, 8, 1}, {P->counters + 2, 4, 2}}));
   BCLX_CK(cudaStreamSynchronize(ctx->stream));
   P->nnz = ctx->pinned[0];
   P->n_heavy_items = ctx->pinned[1];

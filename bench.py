@@ -532,7 +532,9 @@ def bench_spgemm_e2e_streamed(args, A, host, dev, stream, flops):
         Ad = SPMatrix(A.m, A.n, A.tm, A.tn, A.dtype, A.device, dev["tile_row_ptr"], dev["tile_offset"],
                       dev["col_ind"], dev["vals"])
         C = spgemm(Ad, Ad)
-        nnz = C.nnz()
+        # nnz from the output array's length: C.nnz() would read tile_offset
+        # back, a copy queued behind the previous step's copy out
+        nnz = C.col_ind.numel() if C.vals.numel() > 1 else C.nnz()
         done = torch.cuda.Event()
         done.record(stream)
         copy.wait_event(done)
