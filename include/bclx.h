@@ -64,7 +64,8 @@ typedef enum {
   BCLX_ERR_CUDA = 3,            /* a CUDA runtime call failed (see bclx_last_error) */
   BCLX_ERR_NO_MEMORY = 4,       /* device allocation failed */
   BCLX_ERR_INDEX_OVERFLOW = 5,  /* a tile's nnz does not fit the int32 index type */
-  BCLX_ERR_DEVICE_TIMEOUT = 6,  /* a bounded device-side wait gave up */
+  BCLX_ERR_DEVICE_TIMEOUT = 6,  /* reserved for a bounded device-side wait that gives up; no kernel of
+                                   this library waits on a flag set by another kernel, so none returns it */
   BCLX_ERR_NO_DEVICE = 7        /* no usable sm_100 device */
 } bclx_status_t;
 
