@@ -1199,14 +1199,20 @@ def run_reference_ranks(jobs, timeout=3000, threads=1):
     procs = [subprocess.Popen([O.REF_BIN] + [str(x) for x in j], stdout=subprocess.PIPE, stderr=subprocess.PIPE,
                               text=True, env=env) for j in jobs]
     out = []
-    for p in procs:
-        so, se = p.communicate(timeout=timeout)
-        if p.returncode != 0:
-            raise RuntimeError(f"bcl_ref exited {p.returncode}: {se[-300:]}")
-        lines = [ln for ln in so.splitlines() if ln.strip().startswith("{")]
-        if not lines:
-            raise RuntimeError(f"bcl_ref printed no result: {so[-300:]!r}")
-        out.append(json.loads(lines[-1]))
+    try:
+        for p in procs:
+            so, se = p.communicate(timeout=timeout)
+            if p.returncode != 0:
+                raise RuntimeError(f"bcl_ref exited {p.returncode}: {se[-300:]}")
+            lines = [ln for ln in so.splitlines() if ln.strip().startswith("{")]
+            if not lines:
+                raise RuntimeError(f"bcl_ref printed no result: {so[-300:]!r}")
+            out.append(json.loads(lines[-1]))
+    finally:  # none of these processes outlives a failure of another
+        for p in procs:
+            if p.poll() is None:
+                p.kill()
+                p.wait()
     return out
 
 
