@@ -716,9 +716,33 @@ def spgemm_sub(a: SPMatrix, b: SPMatrix, tile_rows, tile_cols, form: str = "fuse
     tile_rows, tile_cols = list(tile_rows), list(tile_cols)
     if any(q <= p for p, q in zip(tile_rows, tile_rows[1:])) or any(q <= p for p, q in zip(tile_cols, tile_cols[1:])):
         raise ValueError("tile rows and columns must be increasing")
-    h = context(a.device).use_current_stream()
     ag, adesc = _sub_spgrid(a, tile_rows, range(a.gn))
     bg, bdesc = _sub_spgrid(b, range(b.gm), tile_cols)
+    c = _sub_product(a, b, ag, bg, tile_rows, tile_cols)
+    del adesc, bdesc  # (the numeric pass is ordered on the stream before any reuse)
+    return c
+
+
+def spgemm_compact(a: SPMatrix, b: SPMatrix, tile_rows, tile_cols):
+    """The C tiles (tile_rows[x], tile_cols[y]) of a product whose operands
+    are held as compact grids: `a` holds exactly A's tile rows `tile_rows`
+    (its tile (x, k) is global tile (tile_rows[x], k)) and `b` exactly B's
+    tile columns `tile_cols` (as a process of a distributed product holds
+    them after fetching them from their owners, bcl_b200.distributed).  Every
+    tile is bit-identical to that tile of the whole product."""
+    _check_grids(a, b)
+    tile_rows, tile_cols = list(tile_rows), list(tile_cols)
+    if a.gm != len(tile_rows) or b.gn != len(tile_cols):
+        raise RuntimeError("BCL::gemm: compact operand grids do not match the tile lists")
+    if any(q <= p for p, q in zip(tile_rows, tile_rows[1:])) or any(q <= p for p, q in zip(tile_cols, tile_cols[1:])):
+        raise ValueError("tile rows and columns must be increasing")
+    return _sub_product(a, b, a.spgrid(), b.spgrid(), tile_rows, tile_cols)
+
+
+def _sub_product(a: SPMatrix, b: SPMatrix, ag, bg, tile_rows, tile_cols):
+    """bclx_spgemm_symbolic_sub + numeric on the grid views ag (A's rows
+    tile_rows) and bg (B's columns tile_cols)."""
+    h = context(a.device).use_current_stream()
     td = a.tile_row_ptr.device
     gm, gn = len(tile_rows), len(tile_cols)
     trp = torch.empty((gm * gn, a.tm + 1), dtype=torch.int32, device=td)
@@ -737,7 +761,6 @@ def spgemm_sub(a: SPMatrix, b: SPMatrix, tile_rows, tile_cols, form: str = "fuse
     out.col_ind, out.vals = ci.data_ptr(), v.data_ptr()
     call("bclx_spgemm_numeric", h, pl.h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(out), 0, 0)
     pl.close()
-    del adesc, bdesc  # (the numeric pass is ordered on the stream before any reuse)
     return SPMatrix(ag.m, bg.n, a.tm, b.tn, a.dtype, a.device, trp, toff, ci, v)
 
 
