@@ -197,8 +197,12 @@ def spgemm_owned(a_rows: Dict, b_cols: Dict, I: List[int], J: List[int], a_shape
     GPU: A's rows I and B's columns J packed into compact grids, the product
     through bclx_spgemm_symbolic_sub with the global tile indices (so every
     tile keeps the stage order k = (k_ + i + j) mod G of its global
-    position).  Returns the C sub-grid (an SPMatrix in I x J order)."""
+    position).  Returns the C sub-grid (an SPMatrix in I x J order), or None
+    for a process that owns no C tile (more processes than tile rows or
+    columns)."""
     from .containers import spgemm_compact
+    if not I or not J:
+        return None
     dev = torch.cuda.current_device() if device is None else device
     m, kdim = a_shape
     _, n = b_shape

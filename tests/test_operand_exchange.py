@@ -22,11 +22,13 @@ def _free_port():
     return port
 
 
-def _operands(value_type):
+def _operands(value_type, tiles=(100, 70, 90)):
+    """Two 512 x 512 R-MAT matrices; the default tiles are ragged at the
+    edge in every dimension."""
     from bcl_b200 import gen
     a = gen.rmat(9, seed=31, value_type=value_type)
     b = gen.rmat(9, seed=32, value_type=value_type)
-    return a, b, 100, 70, 90  # ragged edge tiles in every dimension
+    return (a, b) + tuple(tiles)
 
 
 def _from_tiles(tiles, rows, cols, tr, tc, m, n, dtype):
@@ -72,7 +74,7 @@ def _owned_part(rp, ci, cv, rows, cols, tm, tn, m, n):
             np.concatenate(vs) if vs else np.zeros(0, cv.dtype))
 
 
-def _exchange_rank(rank, world, pgrid, value_type, port, out):
+def _exchange_rank(rank, world, pgrid, value_type, tiles, port, out):
     import torch.distributed as tdist
     from bcl_b200.containers import assemble_tiles
     from bcl_b200.distributed import ProcessGroups, exchange_operands, host_tile, owned_input_tiles
@@ -81,7 +83,7 @@ def _exchange_rank(rank, world, pgrid, value_type, port, out):
                       LOCAL_RANK=str(rank))
     tdist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        a, b, tm, tk, tn = _operands(value_type)
+        a, b, tm, tk, tn = _operands(value_type, tiles)
         pm, pn = pgrid
         groups = ProcessGroups(world, pm, pn)
         a_own = owned_input_tiles(a, tm, tk, rank, pm, pn)
@@ -105,15 +107,19 @@ def _exchange_rank(rank, world, pgrid, value_type, port, out):
         # this process's C tiles from the received operands only
         ar = _from_tiles(a_rows, I, range(gk), tm, tk, a.m, a.n, a.vals.dtype)
         bc = _from_tiles(b_cols, range(gk), J, tk, tn, b.m, b.n, b.vals.dtype)
-        rp, ci, cv = O.gemm_tiled(ar, bc, tm, tk, tn, mode=value_type)
-        part = _owned_part(rp, ci, cv, I, J, tm, tn, a.m, b.n)
+        if I and J:
+            rp, ci, cv = O.gemm_tiled(ar, bc, tm, tk, tn, mode=value_type)
+            part = _owned_part(rp, ci, cv, I, J, tm, tn, a.m, b.n)
+        else:  # no C tile here; the process still served its tiles to the others
+            part = None
         gathered = [None] * world if rank == 0 else None
         tdist.gather_object((part, ok, fetched), gathered, dst=0)
         if rank == 0:
-            whole = assemble_tiles(a.m, b.n, tm, tn, [g[0] for g in gathered])
+            whole = assemble_tiles(a.m, b.n, tm, tn, [g[0] for g in gathered if g[0] is not None])
             wrp, wci, wcv = O.gemm_tiled(a, b, tm, tk, tn, mode=value_type)
             out["ok"] = all(g[1] for g in gathered)
             out["fetched"] = [g[2] for g in gathered]
+            out["idle"] = sum(g[0] is None for g in gathered)
             out["same"] = (np.array_equal(whole.row_ptr.astype(np.int64), wrp) and np.array_equal(whole.col_ind, wci)
                            and np.array_equal(whole.vals.view(np.uint32), wcv.view(np.uint32)))
             out["nnz"] = int(wrp[-1])
@@ -121,17 +127,29 @@ def _exchange_rank(rank, world, pgrid, value_type, port, out):
         tdist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,pgrid,value_type", [(2, (1, 2), "f32"), (4, (2, 2), "f32"), (3, (3, 1), "i32"),
-                                                    (4, (2, 2), "i32")])
-def test_exchange_serves_the_whole_product(world, pgrid, value_type):
+def _run(world, pgrid, value_type, tiles):
     port = _free_port()
     with mp.Manager() as m:
         out = m.dict()
-        mp.spawn(_exchange_rank, args=(world, pgrid, value_type, port, out), nprocs=world, join=True)
-        res = dict(out)
+        mp.spawn(_exchange_rank, args=(world, pgrid, value_type, tiles, port, out), nprocs=world, join=True)
+        return dict(out)
+
+
+@pytest.mark.parametrize("world,pgrid,value_type", [(2, (1, 2), "f32"), (4, (2, 2), "f32"), (3, (3, 1), "i32"),
+                                                    (4, (2, 2), "i32")])
+def test_exchange_serves_the_whole_product(world, pgrid, value_type):
+    res = _run(world, pgrid, value_type, (100, 70, 90))
     assert res["ok"], "a received tile differs from its owner's"
     assert all(f > 0 for f in res["fetched"]), "every process needs tiles it does not own"
-    assert res["same"] and res["nnz"] > 0
+    assert res["same"] and res["nnz"] > 0 and res["idle"] == 0
+
+
+def test_exchange_with_processes_that_own_no_c_tile():
+    """One tile row and one tile column of C on a 2 x 2 process grid: three
+    processes own no C tile but hold operand tiles (k is cut in 8) and must
+    still serve them; rank 0 computes the whole product."""
+    res = _run(4, (2, 2), "f32", (512, 70, 512))
+    assert res["ok"] and res["same"] and res["idle"] == 3
 
 
 def test_pack_tiles_matches_the_grid_layout():
