@@ -131,3 +131,67 @@ def test_owned_product_from_fetched_operands(world, pgrid, tiles, value_type):
     whole = assemble_tiles(a.m, b.n, tm, tn, parts)
     rp, ci, cv = O.gemm_tiled(a, b, tm, tk, tn, mode=value_type)
     assert_csr_identical(whole, rp, ci, cv)
+
+
+def _nccl_exchange_one_rank(port, q):
+    """One NCCL rank on cuda:0: its tiles pass through exchange_operands as
+    device tensors (NCCL broadcasts of the counts, index and value buffers)
+    and spgemm_owned multiplies them in place."""
+    import os
+    from datetime import timedelta
+    import torch
+    import torch.distributed as tdist
+    from bcl_b200.containers import assemble_tiles
+    from bcl_b200.distributed import ProcessGroups, exchange_operands, owned_input_tiles, spgemm_owned
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    try:
+        torch.cuda.set_device(0)
+        tdist.init_process_group("nccl", rank=0, world_size=1, timeout=timedelta(seconds=60))
+        a = gen.rmat(11, seed=77)
+        tm, tk, tn = 300, 200, 250
+        dev = torch.device("cuda", 0)
+        groups = ProcessGroups(1, 1, 1)
+        a_own = owned_input_tiles(a, tm, tk, 0, 1, 1, device=dev)
+        b_own = owned_input_tiles(a, tk, tn, 0, 1, 1, device=dev)
+        a_rows, b_cols, I, J = exchange_operands(a_own, (a.m, a.n), b_own, (a.m, a.n), tm, tk, tn, 0,
+                                                 groups, device=dev)
+        on_device = all(t[0].is_cuda and t[1].is_cuda and t[2].is_cuda for t in list(a_rows.values()) +
+                        list(b_cols.values()))
+        C = spgemm_owned(a_rows, b_cols, I, J, (a.m, a.n), (a.m, a.n), tm, tk, tn, device=0)
+        n = C.nnz()
+        part = (I, J, C.tile_row_ptr.cpu().numpy(), C.tile_offset.cpu().numpy(), C.col_ind[:n].cpu().numpy(),
+                C.vals[:n].cpu().numpy())
+        whole = assemble_tiles(a.m, a.n, tm, tn, [part])
+        rp, ci, cv = O.gemm_tiled(a, a, tm, tk, tn)
+        same = (np.array_equal(whole.row_ptr.astype(np.int64), rp) and np.array_equal(whole.col_ind, ci)
+                and np.array_equal(whole.vals.view(np.uint32), cv.view(np.uint32)))
+        q.put((on_device, same))
+    except Exception as e:  # reported to the parent
+        q.put(repr(e))
+    finally:
+        if tdist.is_initialized():
+            tdist.destroy_process_group()
+
+
+def test_exchange_over_nccl_one_rank():
+    """The device path of the operand exchange over NCCL on one GPU (one
+    rank: the owner's broadcasts of its own tiles; the receiving side is
+    covered by the gloo ranks on CPU), then the owned product from the
+    device tiles, bit-identical to the whole product."""
+    import multiprocessing
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = multiprocessing.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_exchange_one_rank, args=(port, q))
+    p.start()
+    p.join(240)
+    if p.is_alive():
+        p.kill()
+        p.join()
+        pytest.fail("the one-rank NCCL exchange did not finish in 240 s")
+    res = q.get(timeout=5)
+    assert res == (True, True), res
