@@ -98,6 +98,7 @@ SIGNATURES = {
     "bclx_spmm_tile": [vp, i64, i64, i64, i64, vp, vp, vp, vp, vp, i64, i64, i32],
     "bclx_spmm_grid": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid)],
     "bclx_spmm_grid_rowwise": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid)],
+    "bclx_spmm_grid_sub": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), ctypes.POINTER(DGrid), vp, vp],
     "bclx_dmatrix_sum": [vp, ctypes.POINTER(DGrid), vp],
     "bclx_spmatrix_binary_op": [vp, ctypes.POINTER(SpGrid), ctypes.POINTER(DGrid), i32],
     "bclx_csr_to_tiles": [vp, ctypes.POINTER(CSRDesc), ctypes.POINTER(SpGridOut)],

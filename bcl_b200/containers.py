@@ -1035,6 +1035,73 @@ def spmm(a: SPMatrix, b: DMatrix, c: DMatrix, tuning=None) -> None:
         call("bclx_spmm_grid", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(cg))
 
 
+def _sub_dgrid(x: DMatrix, rows, cols):
+    """Tile rows `rows` x tile columns `cols` of x as a grid view: a gathered
+    tile-pointer array (the tiles themselves are not copied)."""
+    td = x.ptrs.device
+    r = torch.as_tensor(list(rows), dtype=torch.int64, device=td)
+    c = torch.as_tensor(list(cols), dtype=torch.int64, device=td)
+    ptrs = x.ptrs[(r[:, None] * x.gn + c[None, :]).reshape(-1)].contiguous()
+    m = sum(min(x.tm, x.m - i * x.tm) for i in rows)
+    n = sum(min(x.tn, x.n - j * x.tn) for j in cols)
+    return DGrid(m, n, x.tm, x.tn, len(rows), len(cols), ptrs.data_ptr(), x.bclx_dtype, 0), ptrs
+
+
+def _check_spmm(a: SPMatrix, b: DMatrix, c: DMatrix):
+    if a.n != b.m or a.m != c.m or b.n != c.n:
+        raise RuntimeError("BCL::gemm: shape mismatch")
+    if a.dtype != np.float32:
+        raise TypeError("SpMM needs FP32 sparse values")
+
+
+def _increasing(tile_rows, tile_cols):
+    tile_rows, tile_cols = list(tile_rows), list(tile_cols)
+    if any(q <= p for p, q in zip(tile_rows, tile_rows[1:])) or any(q <= p for p, q in zip(tile_cols, tile_cols[1:])):
+        raise ValueError("tile rows and columns must be increasing")
+    return tile_rows, tile_cols
+
+
+def _spmm_grid_sub(device, ag, bg, cg, tile_rows, tile_cols):
+    h = context(device).use_current_stream()
+    rows_arr = (ctypes.c_int64 * max(len(tile_rows), 1))(*tile_rows)
+    cols_arr = (ctypes.c_int64 * max(len(tile_cols), 1))(*tile_cols)
+    call("bclx_spmm_grid_sub", h, ctypes.byref(ag), ctypes.byref(bg), ctypes.byref(cg), rows_arr, cols_arr)
+
+
+def spmm_sub(a: SPMatrix, b: DMatrix, c: DMatrix, tile_rows, tile_cols) -> None:
+    """C += A * B for the C tiles (i, j), i in tile_rows, j in tile_cols
+    (increasing global tile indices), in place in c's tiles, each over all k
+    in the rotated order of its global position: what one process of the
+    reference's stationary-C loop computes (spgemm.hpp:153-179 under
+    c.tile_rank), in one launch (bclx_spmm_grid_sub); bit-identical to those
+    tiles of spmm(a, b, c)."""
+    _check_spmm(a, b, c)
+    tile_rows, tile_cols = _increasing(tile_rows, tile_cols)
+    if not tile_rows or not tile_cols:
+        return
+    ag, adesc = _sub_spgrid(a, tile_rows, range(a.gn))
+    bg, bptr = _sub_dgrid(b, range(b.gm), tile_cols)
+    cg, cptr = _sub_dgrid(c, tile_rows, tile_cols)
+    _spmm_grid_sub(a.device, ag, bg, cg, tile_rows, tile_cols)
+    del adesc, bptr, cptr  # (the launches are ordered on the stream before any reuse)
+
+
+def spmm_compact(a: SPMatrix, b: DMatrix, c: DMatrix, tile_rows, tile_cols) -> None:
+    """C += A * B on operands held as compact grids: `a` holds exactly A's
+    tile rows tile_rows (its tile (x, k) is global tile (tile_rows[x], k)),
+    `b` B's tile columns tile_cols and `c` the C tiles tile_rows x
+    tile_cols (as a process of a distributed product holds them after
+    fetching its operands, bcl_b200.distributed).  Every C tile is
+    bit-identical to that tile of the whole product."""
+    _check_spmm(a, b, c)
+    tile_rows, tile_cols = _increasing(tile_rows, tile_cols)
+    if a.gm != len(tile_rows) or c.gm != len(tile_rows) or c.gn != len(tile_cols) or b.gn != len(tile_cols):
+        raise RuntimeError("BCL::gemm: compact operand grids do not match the tile lists")
+    if not tile_rows or not tile_cols:
+        return
+    _spmm_grid_sub(a.device, a.spgrid(), b.dgrid(), c.dgrid(), tile_rows, tile_cols)
+
+
 def rowwise_gemm(a: SPMatrix, b: DMatrix, c: DMatrix) -> None:
     """C += A * B with C in one tile column, every C tile row taking the k
     tiles in ascending order (rowwise_gemm, experimental_gemm.hpp:83-123)."""

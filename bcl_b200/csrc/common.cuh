@@ -117,6 +117,12 @@ struct DGridView {
   // G (spgemm.hpp:162-175), 1 = ascending k (the row-wise variants,
   // experimental_gemm.hpp:83-214).  Read from the B view.
   int32_t natural_order;
+  // Sub-grid stage maps (bclx_spmm_grid_sub), read from the B view: the
+  // global tile row of each C grid row and the global tile column of each C
+  // grid column, both mod G, so that the rotation is that of the tile's
+  // global position; null when the grids are the whole product.
+  const int32_t* rot_i;
+  const int32_t* rot_j;
 
   __device__ __forceinline__ void* tile(int64_t i, int64_t j) const {
     return tiles ? tiles[i * gn + j] : single;

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <vector>
 
 namespace bclx {
 
@@ -147,13 +148,14 @@ struct StageLane {
   const ST* bt;
 };
 
-template <typename ST>
+template <typename ST, bool SUB>
 __device__ __forceinline__ StageLane<ST> stage_lane(const SpGridView& A, const DGridView& B, int64_t ti, int64_t tj,
                                                     int64_t r, int64_t kk, bool valid) {
   StageLane<ST> s{0, nullptr, nullptr, nullptr};
   const int64_t gk = A.gn;
   if (valid && kk < gk) {
-    const int64_t k = B.natural_order ? kk : (kk + ti + tj) % gk;
+    const int64_t rot = SUB ? (int64_t)__ldg(B.rot_i + ti) + __ldg(B.rot_j + tj) : ti + tj;
+    const int64_t k = B.natural_order ? kk : (kk + rot) % gk;
     const bclx_csr_t At = A.tile(ti, k);
     const int32_t as = __ldg(At.row_ptr + r);
     s.alen = __ldg(At.row_ptr + r + 1) - as;
@@ -191,7 +193,7 @@ __device__ __forceinline__ bool tiles_aligned(const DGridView& B, const DGridVie
 // test for inside the unrolled loop).  `skip` (or null): rows flagged there
 // are left to another kernel.  `vec`: every B and C row slice of this tile
 // pair is 16-byte aligned; otherwise element-wise access.
-template <typename ST, bool GROUP, int UNROLL = kSpmmUnroll>
+template <typename ST, bool GROUP, bool SUB, int UNROLL = kSpmmUnroll>
 __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& B, const DGridView& C, int64_t ti,
                                           int64_t tj, int64_t r0, int R, int c0, int W, bool vec,
                                           const uint8_t* __restrict__ skip) {
@@ -244,7 +246,7 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
     const int64_t kk = GROUP ? lane - ql * gk : g0 + lane;
     bool valid = ql < nrows;
     if (valid && skip) valid = skip[ti * C.tm + r0 + ql] == 0;
-    const StageLane<ST> sl = stage_lane<ST>(A, B, ti, tj, r0 + ql, kk, valid);
+    const StageLane<ST> sl = stage_lane<ST, SUB>(A, B, ti, tj, r0 + ql, kk, valid);
     const int32_t aincl = warp_inclusive_scan(sl.alen);
     const int32_t atot = __shfl_sync(kFull, aincl, 31);
     if (atot == 0) continue;
@@ -376,7 +378,7 @@ __device__ __forceinline__ void spmm_rows(const SpGridView& A, const DGridView& 
 // flight while the current item runs), so warps that draw short rows take
 // more of them: the cost of a (row group, panel) item varies by orders of
 // magnitude on power-law matrices.
-template <typename ST, bool GROUP>
+template <typename ST, bool GROUP, bool SUB>
 __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     k_spmm(SpGridView A, DGridView B, DGridView C, int64_t n_items, int npanels, int R, int64_t ngroups,
            int row_align_ok, int panel_major, const uint8_t* __restrict__ long_flag,
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 4)
     if (r0 < C.rows_of(ti) && c0 < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
       // rows flagged long are k_spmm_long's (it takes the aligned ones)
-      spmm_rows<ST, GROUP>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr);
+      spmm_rows<ST, GROUP, SUB>(A, B, C, ti, tj, r0, R, c0, W, vec, vec ? long_flag : nullptr);
     }
     it = __shfl_sync(kFull, nx, 0);
   }
@@ -479,7 +481,7 @@ __global__ void k_spmm_find_long(SpGridView A, int long_row, int very_long_row, 
 //   * chunk c applied: the multiply-adds in entry order from shared memory.
 // One commit group per chunk step holds A(c+6) and B(c+2); B(c) is in the
 // group two steps back.  The stages are at most 32 (one lane each).
-template <typename ST>
+template <typename ST, bool SUB>
 __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, const DGridView& B,
                                               const DGridView& C, int64_t ti, int64_t tj, int64_t r, int c0, int W) {
   using V = Vec<ST>;
@@ -490,7 +492,7 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
   const bool own = col < W;
   float acc[VN];
   if (own) V::load_c(crow + col, acc);
-  const StageLane<ST> sl = stage_lane<ST>(A, B, ti, tj, r, lane, true);
+  const StageLane<ST> sl = stage_lane<ST, SUB>(A, B, ti, tj, r, lane, true);
   const int32_t aincl = warp_inclusive_scan(sl.alen);
   const int32_t atot = __shfl_sync(kFull, aincl, 31);
   const int32_t aexcl = aincl - sl.alen;
@@ -606,7 +608,7 @@ __device__ __forceinline__ void spmm_long_row(LongSmem& S, const SpGridView& A, 
 // Items (listed row, C tile column, panel), a row's items consecutive, taken
 // from a device counter in list order.  Every block, once placed, lets a
 // programmatic dependent (k_spmm under the dependent-launch schedule) launch.
-template <typename ST>
+template <typename ST, bool SUB>
 __global__ void __launch_bounds__(kLongWarps * 32)
     k_spmm_long(SpGridView A, DGridView B, DGridView C, const int64_t* __restrict__ list,
                 const int32_t* __restrict__ count, int npanels, int row_align_ok,
@@ -636,7 +638,7 @@ __global__ void __launch_bounds__(kLongWarps * 32)
     const int W = (int)C.cols_of(tj);
     if (panel * PW < W) {
       const bool vec = row_align_ok && (W % Vec<ST>::N) == 0 && tiles_aligned(B, C, ti, tj);
-      if (vec) spmm_long_row<ST>(S, A, B, C, ti, tj, r, panel * PW, W);  // otherwise k_spmm did it element-wise
+      if (vec) spmm_long_row<ST, SUB>(S, A, B, C, ti, tj, r, panel * PW, W);  // otherwise k_spmm did it element-wise
     }
     it = __shfl_sync(kFull, nx, 0);
   }
@@ -703,7 +705,7 @@ static int spmm_rows_per_item(const Context* ctx, const DGridView& C, int64_t gk
 // and one cp.async.bulk copy per 512-byte B slice, completing on an
 // mbarrier, in place of the per-lane copies: 6.8 ms for k_spmm_long alone
 // against 1.9.
-template <typename ST>
+template <typename ST, bool SUB>
 static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, const DGridView& C, int align_ok) {
   constexpr int VN = Vec<ST>::N;
   const int npanels = (int)ceil_div(C.tn, 32 * VN);
@@ -744,8 +746,8 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
     BCLX_CK_LAUNCH();
     if (!dependent) BCLX_CK(cudaEventRecord(ctx->fork2_ev, ctx->side));
     const size_t lsmem = sizeof(LongSmem) * kLongWarps;
-    BCLX_CK(cudaFuncSetAttribute(k_spmm_long<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
-    k_spmm_long<ST><<<(unsigned)spmm_long_blocks(ctx, npanels), kLongWarps * 32, lsmem, ls>>>(A, B, C, list, cnt, npanels,
+    BCLX_CK(cudaFuncSetAttribute(k_spmm_long<ST, SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem));
+    k_spmm_long<ST, SUB><<<(unsigned)spmm_long_blocks(ctx, npanels), kLongWarps * 32, lsmem, ls>>>(A, B, C, list, cnt, npanels,
                                                                                     align_ok, ctr + 1);
     note_launch();
     BCLX_CK_LAUNCH();
@@ -771,10 +773,10 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
   const uint8_t* lflag = flag;
   const int pmajor = (int)tuning(ctx, BCLX_TUNE_SPMM_PANEL_MAJOR);
   if (R > 1)
-    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true>, A, B, C, n_items, npanels, R, ngroups, align_ok, pmajor, lflag,
+    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, true, SUB>, A, B, C, n_items, npanels, R, ngroups, align_ok, pmajor, lflag,
                                ctr));
   else
-    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, false>, A, B, C, n_items, npanels, 1, ngroups, align_ok, pmajor, lflag,
+    BCLX_CK(cudaLaunchKernelEx(&cfg, k_spmm<ST, false, SUB>, A, B, C, n_items, npanels, 1, ngroups, align_ok, pmajor, lflag,
                                ctr));
   note_launch();
   BCLX_CK_LAUNCH();
@@ -790,8 +792,12 @@ static int launch_spmm(Context* ctx, const SpGridView& A, const DGridView& B, co
 static int run_spmm(Context* ctx, const SpGridView& A, const DGridView& B, const DGridView& C, int dtype) {
   const int es = dtype == BCLX_F32 ? 4 : 2;
   const int align_ok = ((B.ld * es) % 16 == 0) && ((C.ld * es) % 16 == 0);
-  if (dtype == BCLX_F32) return launch_spmm<float>(ctx, A, B, C, align_ok);
-  return launch_spmm<__nv_bfloat16>(ctx, A, B, C, align_ok);
+  if (B.rot_i) {  // a sub-grid (bclx_spmm_grid_sub): stage maps
+    if (dtype == BCLX_F32) return launch_spmm<float, true>(ctx, A, B, C, align_ok);
+    return launch_spmm<__nv_bfloat16, true>(ctx, A, B, C, align_ok);
+  }
+  if (dtype == BCLX_F32) return launch_spmm<float, false>(ctx, A, B, C, align_ok);
+  return launch_spmm<__nv_bfloat16, false>(ctx, A, B, C, align_ok);
 }
 
 }  // namespace bclx
@@ -829,7 +835,8 @@ int bclx_spmm_tile(bclx_context_t c, int64_t m, int64_t n, int64_t k, int64_t nn
 }
 
 static int spmm_grid_impl(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg,
-                          int natural_order) {
+                          int natural_order, const int64_t* tile_rows = nullptr,
+                          const int64_t* tile_cols = nullptr) {
   Context* ctx = reinterpret_cast<Context*>(c);
   if (!ctx || !a || !b || !cg || !a->tiles || !b->tiles || !cg->tiles) return BCLX_ERR_INVALID;
   if (a->dtype != BCLX_F32) return BCLX_ERR_DTYPE;
@@ -853,7 +860,26 @@ static int spmm_grid_impl(bclx_context_t c, const bclx_spgrid_t* a, const bclx_d
   DGridView C{};
   C.tiles = cg->tiles; C.m = cg->m; C.n = cg->n; C.tm = cg->tile_m; C.tn = cg->tile_n; C.gm = cg->grid_m;
   C.gn = cg->grid_n; C.ld = cg->tile_n;
-  return run_spmm(ctx, A, B, C, b->dtype);
+  if (!tile_rows || a->grid_n == 0 || cg->grid_m == 0 || cg->grid_n == 0) return run_spmm(ctx, A, B, C, b->dtype);
+  // sub-grid: the stage maps, on the device for the launch
+  std::vector<int32_t> maps((size_t)(cg->grid_m + cg->grid_n));
+  for (int64_t i = 0; i < cg->grid_m; i++) maps[(size_t)i] = (int32_t)(tile_rows[i] % a->grid_n);
+  for (int64_t j = 0; j < cg->grid_n; j++) maps[(size_t)(cg->grid_m + j)] = (int32_t)(tile_cols[j] % a->grid_n);
+  int32_t* dmaps = nullptr;
+  BCLX_TRY(scratch_alloc_n(ctx, &dmaps, maps.size()));
+  cudaError_t e = cudaMemcpyAsync(dmaps, maps.data(), sizeof(int32_t) * maps.size(), cudaMemcpyHostToDevice,
+                                  ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // the host vector goes out of scope
+  if (e != cudaSuccess) {
+    scratch_free(ctx, dmaps);
+    set_last_error(std::string("stage maps: ") + cudaGetErrorString(e));
+    return BCLX_ERR_CUDA;
+  }
+  B.rot_i = dmaps;
+  B.rot_j = dmaps + cg->grid_m;
+  const int rc = run_spmm(ctx, A, B, C, b->dtype);
+  scratch_free(ctx, dmaps);  // stream-ordered: after the launches (the side stream is joined)
+  return rc;
 }
 
 int bclx_spmm_grid(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg) {
@@ -862,6 +888,19 @@ int bclx_spmm_grid(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t*
 
 int bclx_spmm_grid_rowwise(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg) {
   return spmm_grid_impl(c, a, b, cg, 1);
+}
+
+int bclx_spmm_grid_sub(bclx_context_t c, const bclx_spgrid_t* a, const bclx_dgrid_t* b, const bclx_dgrid_t* cg,
+                       const int64_t* tile_rows, const int64_t* tile_cols) {
+  if (!cg || !tile_rows || !tile_cols) return BCLX_ERR_INVALID;
+  // global tile indices increasing (so only the last may be a ragged edge tile)
+  for (int64_t i = 0; i < cg->grid_m; i++)
+    if (tile_rows[i] < 0 || tile_rows[i] >= INT32_MAX || (i > 0 && tile_rows[i] <= tile_rows[i - 1]))
+      return BCLX_ERR_INVALID;
+  for (int64_t j = 0; j < cg->grid_n; j++)
+    if (tile_cols[j] < 0 || tile_cols[j] >= INT32_MAX || (j > 0 && tile_cols[j] <= tile_cols[j - 1]))
+      return BCLX_ERR_INVALID;
+  return spmm_grid_impl(c, a, b, cg, 0, tile_rows, tile_cols);
 }
 
 }  // extern "C"

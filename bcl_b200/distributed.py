@@ -10,11 +10,14 @@ I x J with I = {i : i % pm = r} and J = {j : j % pn = c}; it needs the A
 tiles (i, k), i in I, whose owners (r, k % pn) are in its process row, and
 the B tiles (k, j), j in J, whose owners (k % pm, c) are in its process
 column.  So one exchange serves the whole product: every owner broadcasts
-its tiles once within its process row (A) and its process column (B), packed
-into three buffers (per-tile entry counts, then the int32 row pointers and
-column indices, then the values).  Over NCCL the buffers are device tensors
-and land in local HBM, where the sub-grid product reads them
-(`spgemm_owned`); over gloo they are host tensors.
+its tiles once within its process row (A) and its process column (B), sparse
+tiles packed into three buffers (per-tile entry counts, then the int32 row
+pointers and column indices, then the values), dense tiles into one.  Over
+NCCL the buffers are device tensors and land in local HBM, where the
+sub-grid products read them (`spgemm_owned`, `spmm_owned`); over gloo they
+are host tensors.  The sparse x dense product (spgemm.hpp:153-179; its GPU
+driver cuda/algorithms/spmm.hpp:20-115) places dense tiles the same way
+(DMatrix.hpp:75-90), so the same exchange serves it with B dense.
 """
 from __future__ import annotations
 
@@ -132,23 +135,97 @@ def exchange_operands(a_own: Dict, a_shape: Tuple[int, int], b_own: Dict, b_shap
     j in J, I and J this process's C tile rows and columns.  Every process of
     the grid calls it (the broadcasts are collective within process rows and
     columns); a process that owns no tile still takes part."""
+    I, J, gk = _owned_lines(a_shape, b_shape, tm, tk, tn, rank, groups)
+    a_rows = _exchange_a_rows(a_own, a_shape[0], tm, gk, I, rank, groups, device, val_dtype)
     pm, pn = groups.pm, groups.pn
-    r, c = divmod(rank, pn)
-    m, kdim = a_shape
-    _, n = b_shape
-    gm, gk, gn = _ceil_div(m, tm), _ceil_div(kdim, tk), _ceil_div(n, tn)
-    I = [i for i in range(gm) if i % pm == r]
-    J = [j for j in range(gn) if j % pn == c]
-    a_rows: Dict = {}
-    for cc in range(pn):  # A along the process row, owner by owner
-        keys = [(i, k) for i in I for k in range(gk) if k % pn == cc]
-        a_rows.update(_broadcast_tiles(keys, lambda key: min(tm, m - key[0] * tm), a_own, r * pn + cc, rank,
-                                       groups.rows[r], device, val_dtype))
+    c = rank % pn
+    kdim = a_shape[1]
     b_cols: Dict = {}
-    for rr in range(pm):  # B along the process column
+    for rr in range(pm):  # B along the process column, owner by owner
         keys = [(k, j) for k in range(gk) if k % pm == rr for j in J]
         b_cols.update(_broadcast_tiles(keys, lambda key: min(tk, kdim - key[0] * tk), b_own, rr * pn + c, rank,
                                        groups.cols[c], device, val_dtype))
+    return a_rows, b_cols, I, J
+
+
+def _owned_lines(a_shape, b_shape, tm: int, tk: int, tn: int, rank: int, groups: ProcessGroups):
+    """This process's C tile rows I and columns J, and the number of k tiles."""
+    r, c = divmod(rank, groups.pn)
+    m, kdim = a_shape
+    n = b_shape[1]
+    I = [i for i in range(_ceil_div(m, tm)) if i % groups.pm == r]
+    J = [j for j in range(_ceil_div(n, tn)) if j % groups.pn == c]
+    return I, J, _ceil_div(kdim, tk)
+
+
+def _exchange_a_rows(a_own: Dict, m: int, tm: int, gk: int, I: List[int], rank: int, groups: ProcessGroups, device,
+                     val_dtype) -> Dict:
+    """A's tiles (i, k), i in I, every k, along the process row: process
+    (r, cc) broadcasts the tiles with k % pn == cc that the row needs."""
+    pn = groups.pn
+    r = rank // pn
+    a_rows: Dict = {}
+    for cc in range(pn):
+        keys = [(i, k) for i in I for k in range(gk) if k % pn == cc]
+        a_rows.update(_broadcast_tiles(keys, lambda key: min(tm, m - key[0] * tm), a_own, r * pn + cc, rank,
+                                       groups.rows[r], device, val_dtype))
+    return a_rows
+
+
+def owned_dense_tiles(arr, tm: int, tn: int, rank: int, pm: int, pn: int, dtype=torch.float32,
+                      device="cpu") -> Dict[Tuple[int, int], torch.Tensor]:
+    """The tiles of a dense m x n matrix that process `rank` holds in the
+    reference's layout (DMatrix.hpp:75-90: tile (i, j) on process
+    (j % pn) + (i % pm) * pn), each tm x tn row-major and zero-padded at the
+    edges as a DMatrix tile is."""
+    full = torch.as_tensor(arr)
+    m, n = full.shape
+    out = {}
+    for i in range(_ceil_div(m, tm)):
+        for j in range(_ceil_div(n, tn)):
+            if tile_owner(i, j, pm, pn) == rank:
+                t = torch.zeros((tm, tn), dtype=dtype, device=device)
+                blk = full[i * tm:(i + 1) * tm, j * tn:(j + 1) * tn]
+                t[:blk.shape[0], :blk.shape[1]] = blk.to(device=device, dtype=dtype)
+                out[(i, j)] = t
+    return out
+
+
+def _broadcast_dense(keys: List[Tuple[int, int]], owned: Dict, src: int, me: int, group, shape, dtype,
+                     device) -> Dict[Tuple[int, int], torch.Tensor]:
+    """Dense tiles `keys` from process `src` to every member of `group`, in
+    one buffer."""
+    import torch.distributed as tdist
+    if not keys:
+        return {}
+    if me == src:
+        buf = torch.stack([owned[k] for k in keys]).contiguous()
+    else:
+        buf = torch.empty((len(keys),) + tuple(shape), dtype=dtype, device=device)
+    tdist.broadcast(buf, src=src, group=group)
+    if me == src:
+        return {k: owned[k] for k in keys}
+    return {k: buf[x] for x, k in enumerate(keys)}
+
+
+def exchange_spmm_operands(a_own: Dict, a_shape: Tuple[int, int], b_own: Dict, b_shape: Tuple[int, int],
+                           tm: int, tk: int, tn: int, rank: int, groups: ProcessGroups, device="cpu",
+                           b_dtype=torch.float32):
+    """The operands of this process's C tiles for the sparse x dense product
+    (spgemm.hpp:153-179; the GPU driver's broadcasts,
+    cuda/algorithms/spmm.hpp:20-115): the sparse A tiles of its C tile rows
+    along its process row, and the dense B tiles (tk x tn, padded) of its C
+    tile columns along its process column.  The C tiles I x J are this
+    process's own (the same layout) and do not move.  Returns (a_rows,
+    b_cols, I, J); every process of the grid calls it."""
+    I, J, gk = _owned_lines(a_shape, b_shape, tm, tk, tn, rank, groups)
+    a_rows = _exchange_a_rows(a_own, a_shape[0], tm, gk, I, rank, groups, device, torch.float32)
+    pm, pn = groups.pm, groups.pn
+    c = rank % pn
+    b_cols: Dict = {}
+    for rr in range(pm):  # dense B along the process column
+        keys = [(k, j) for k in range(gk) if k % pm == rr for j in J]
+        b_cols.update(_broadcast_dense(keys, b_own, rr * pn + c, rank, groups.cols[c], (tk, tn), b_dtype, device))
     return a_rows, b_cols, I, J
 
 
@@ -189,6 +266,35 @@ def pack_grid(tiles: Dict, rows: List[int], cols: List[int], tm: int, tn: int, m
     mm = sum(min(tm, m - i * tm) for i in rows)
     nn = sum(min(tn, n - j * tn) for j in cols)
     return SPMatrix(mm, nn, tm, tn, dtype, device, trp, toff, ci, v)
+
+
+def spmm_owned(a_rows: Dict, b_cols: Dict, c_tiles: Dict, I: List[int], J: List[int], a_shape, b_shape, tm: int,
+               tk: int, tn: int, device: Optional[int] = None):
+    """C += A * B for this process's C tiles I x J on the GPU, from the
+    fetched operand tiles: A's rows I packed as a compact sparse grid, B's
+    columns J and the C tiles (c_tiles[(i, j)], tm x tn) stacked as compact
+    dense grids, one launch through bclx_spmm_grid_sub with the global tile
+    indices.  Returns the C tiles ({(i, j): tm x tn tensor on the device},
+    bit-identical to those tiles of the whole product), or {} for a process
+    that owns no C tile."""
+    from .containers import DMatrix, spmm_compact
+    if not I or not J:
+        return {}
+    dev = torch.cuda.current_device() if device is None else device
+    td = torch.device("cuda", dev)
+    m, kdim = a_shape
+    _, n = b_shape
+    gk = _ceil_div(kdim, tk)
+    A = pack_grid(a_rows, I, list(range(gk)), tm, tk, m, kdim, np.float32, dev)
+    kk = list(range(gk))
+    bt = torch.stack([b_cols[(k, j)].to(td) for k in kk for j in J]).contiguous()
+    ct = torch.stack([c_tiles[(i, j)].to(td) for i in I for j in J]).contiguous()
+    nn = sum(min(tn, n - j * tn) for j in J)
+    mm = sum(min(tm, m - i * tm) for i in I)
+    B = DMatrix(kdim, nn, tk, tn, bt)
+    C = DMatrix(mm, nn, tm, tn, ct)
+    spmm_compact(A, B, C, I, J)
+    return {(i, j): C.tiles[x * len(J) + y] for x, i in enumerate(I) for y, j in enumerate(J)}
 
 
 def spgemm_owned(a_rows: Dict, b_cols: Dict, I: List[int], J: List[int], a_shape, b_shape, tm: int, tk: int,

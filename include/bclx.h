@@ -18,6 +18,8 @@
  *                                     colind, ldb, ldc), spgemm.hpp:140-149 (80-96)
  *   bclx_spmm_grid                    BCL::gemm(SPMatrix, DMatrix, DMatrix&)
  *                                     spgemm.hpp:153-179
+ *   bclx_spmm_grid_sub                one process's C tiles of that product
+ *                                     (the same loop under c.tile_rank)
  *   bclx_csr_to_tiles                 SPMatrix(fname, blocking) slicing,
  *                                     SPMatrix.hpp:194-271
  *   bclx_tiles_to_csr                 SPMatrix::get, SPMatrix.hpp:516-546
@@ -348,6 +350,21 @@ BCLX_API int bclx_spmm_tile(bclx_context_t ctx, int64_t m, int64_t n, int64_t k,
  * b->dtype == c->dtype selects FP32 or BF16 storage. */
 BCLX_API int bclx_spmm_grid(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_dgrid_t* b,
                    const bclx_dgrid_t* c);
+/* The C tiles (tile_rows[x], tile_cols[y]) of a larger product C += A * B,
+ * in one launch: what one process of the reference's stationary-C loop
+ * computes (spgemm.hpp:153-179 with c.tile_rank({i, j}) == rank; the GPU
+ * driver cuda/algorithms/spmm.hpp:20-115).  `c` is the grid of those tiles
+ * (grid_m = number of tile_rows, grid_n = number of tile_cols), `a` holds
+ * A's tile rows tile_rows over every k, `b` B's tile columns tile_cols over
+ * every k (grids of gathered tile pointers or compact copies).  Each C tile
+ * takes the k tiles in the rotated order of its global position,
+ * k = (k_ + tile_rows[x] + tile_cols[y]) mod G, so it is bit-identical to
+ * that tile of bclx_spmm_grid on the whole grids.  tile_rows / tile_cols:
+ * host arrays of global tile indices, increasing (only the last can be a
+ * ragged edge tile), else BCLX_ERR_INVALID.  Copies the two index maps to
+ * the device (synchronizes the context's stream once). */
+BCLX_API int bclx_spmm_grid_sub(bclx_context_t ctx, const bclx_spgrid_t* a, const bclx_dgrid_t* b,
+                                const bclx_dgrid_t* c, const int64_t* tile_rows, const int64_t* tile_cols);
 /* The row-wise variants rowwise_gemm / cached_rowwise_gemm /
  * batched_rowwise_gemm (bcl/containers/algorithms/experimental_gemm.hpp:
  * 83-214): C += A * B with C in one tile column (c->grid_n == 1, else

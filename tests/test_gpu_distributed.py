@@ -195,3 +195,91 @@ def test_exchange_over_nccl_one_rank():
         pytest.fail("the one-rank NCCL exchange did not finish in 240 s")
     res = q.get(timeout=5)
     assert res == (True, True), res
+
+
+def _dense_grids(a, b, c0, tiles, dtype):
+    import torch
+    from bcl_b200.containers import BlockCustom, DMatrix, SPMatrix
+    tm, tk, tn = tiles
+    A = SPMatrix.from_csr(a, BlockCustom((tm, tk)))
+    if dtype == "f32":
+        B = DMatrix.from_array(torch.from_numpy(b), BlockCustom((tk, tn)))
+        C = DMatrix.from_array(torch.from_numpy(c0), BlockCustom((tm, tn)))
+    else:
+        as_bf16 = lambda x: torch.from_numpy(x.view(np.int16)).view(torch.bfloat16)
+        B = DMatrix.from_array(as_bf16(b), BlockCustom((tk, tn)), dtype=torch.bfloat16)
+        C = DMatrix.from_array(as_bf16(c0), BlockCustom((tm, tn)), dtype=torch.bfloat16)
+    return A, B, C
+
+
+def _dense_out(C, dtype):
+    import torch
+    out = C.get_matrix().cpu()
+    return out.numpy() if dtype == "f32" else out.view(torch.int16).numpy().view(np.uint16)
+
+
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+@pytest.mark.parametrize("case", ["rmat_2x2", "rmat_3x1_ragged", "long_rows_4x1"])
+def test_spmm_sub_grids_cover_the_whole_product(monkeypatch, dtype, case):
+    """Every process's C tiles of the sparse x dense product computed in turn
+    on one GPU (bclx_spmm_grid_sub: one launch per process, each C tile in
+    the rotated stage order of its global position), in place in the whole
+    C: the result is the whole product bit for bit (FP32 against the oracle,
+    BF16 storage against the oracle's BF16 restatement).  Covers ragged
+    tiles, 12 tiles along k, and rows long enough for the long-row kernel."""
+    from bcl_b200.containers import owned_tiles, spmm_sub
+    from test_gpu_spmm import heavy_rows_matrix
+    if case == "rmat_2x2":
+        a, tiles, pgrid, n = gen.rmat(13, seed=81), (4096, 4096, 128), (2, 2), 256
+    elif case == "rmat_3x1_ragged":
+        a, tiles, pgrid, n = gen.rmat(13, seed=82), (1000, 700, 64), (3, 1), 200
+    else:
+        monkeypatch.setenv("BCLX_SPMM_LONG_MIN_ROWS", "0")
+        a, tiles, pgrid, n = heavy_rows_matrix(), (4096, 4096, 256), (4, 1), 256
+    b = gen.dense(a.n, n, seed=83, dist="normal")
+    c0 = gen.dense(a.m, n, seed=84)
+    if dtype == "bf16":
+        b, c0 = O.to_bf16(b), O.to_bf16(c0)
+    A, B, C = _dense_grids(a, b, c0, tiles, dtype)
+    pm, pn = pgrid
+    for p in range(pm * pn):
+        rows, cols = owned_tiles(C.gm, C.gn, p, pm, pn)
+        spmm_sub(A, B, C, rows, cols)
+    got = _dense_out(C, dtype)
+    if dtype == "f32":
+        want = O.spmm_tiled(a, b, c0, *tiles)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    else:
+        assert np.array_equal(got, O.spmm_tiled_bf16(a, b, c0, *tiles))
+
+
+def test_spmm_owned_from_fetched_operands():
+    """Each process's C tiles from its received operands (A's tile rows I as
+    a compact sparse grid, B's tile columns J and its own C tiles as compact
+    dense grids; bcl_b200.distributed.spmm_owned), 2 x 2 processes, ragged
+    tiles: the tiles assemble to the whole product bit for bit."""
+    import torch
+    from bcl_b200.distributed import host_tile, owned_dense_tiles, spmm_owned
+    a = gen.rmat(13, seed=85)
+    n = 200
+    b = gen.dense(a.n, n, seed=86, dist="normal")
+    c0 = gen.dense(a.m, n, seed=87)
+    tm, tk, tn = 1000, 700, 64
+    gm, gk, gn = -(-a.m // tm), -(-a.n // tk), -(-n // tn)
+    pm, pn = 2, 2
+    whole = np.array(c0, copy=True)
+    for p in range(pm * pn):
+        r, c = divmod(p, pn)
+        I = [i for i in range(gm) if i % pm == r]
+        J = [j for j in range(gn) if j % pn == c]
+        a_rows = {(i, k): tuple(torch.from_numpy(x) for x in host_tile(a, tm, tk, i, k)) for i in I for k in range(gk)}
+        b_all = owned_dense_tiles(b, tk, tn, 0, 1, 1)
+        b_cols = {(k, j): b_all[(k, j)] for k in range(gk) for j in J}
+        c_tiles = owned_dense_tiles(c0, tm, tn, p, pm, pn)
+        out = spmm_owned(a_rows, b_cols, c_tiles, I, J, (a.m, a.n), (a.n, n), tm, tk, tn, device=0)
+        assert set(out) == set(c_tiles)
+        for (i, j), t in out.items():
+            blk = whole[i * tm:(i + 1) * tm, j * tn:(j + 1) * tn]
+            blk[...] = t.cpu().numpy()[:blk.shape[0], :blk.shape[1]]
+    want = O.spmm_tiled(a, b, c0, tm, tk, tn)
+    assert np.array_equal(whole.view(np.uint32), want.view(np.uint32))

@@ -187,3 +187,78 @@ def test_owned_input_tiles_partition_the_matrix():
             assert key not in seen and tile_owner(*key, pm, pn) == p
             seen[key] = int(t[1].numel())
     assert len(seen) == (-(-a.m // tm)) * (-(-a.n // tk)) and sum(seen.values()) == a.nnz
+
+
+def _spmm_exchange_rank(rank, world, pgrid, port, out):
+    """The sparse x dense product with distributed operands: A sparse and B,
+    C dense, every tile on its owner; A along process rows, dense B along
+    process columns; each process's C tiles from what it received (oracle)."""
+    import torch.distributed as tdist
+    from bcl_b200 import gen
+    from bcl_b200.distributed import (ProcessGroups, exchange_spmm_operands, host_tile, owned_dense_tiles,
+                                      owned_input_tiles)
+    from oracle import oracle as O
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
+                      LOCAL_RANK=str(rank))
+    tdist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        a = gen.rmat(9, seed=33)
+        n = 200
+        b = gen.dense(a.n, n, seed=34)
+        c0 = gen.dense(a.m, n, seed=35)
+        tm, tk, tn = 100, 70, 64  # ragged in every dimension
+        pm, pn = pgrid
+        groups = ProcessGroups(world, pm, pn)
+        a_own = owned_input_tiles(a, tm, tk, rank, pm, pn)
+        b_own = owned_dense_tiles(b, tk, tn, rank, pm, pn)
+        c_own = owned_dense_tiles(c0, tm, tn, rank, pm, pn)
+        a_rows, b_cols, I, J = exchange_spmm_operands(a_own, (a.m, a.n), b_own, (b.shape[0], n), tm, tk, tn, rank,
+                                                      groups)
+        gk = -(-a.n // tk)
+        ok = set(c_own) == {(i, j) for i in I for j in J}  # C tiles stay with their owner
+        ok &= set(b_cols) == {(k, j) for k in range(gk) for j in J}
+        for (k, j), t in b_cols.items():
+            want = np.zeros((tk, tn), np.float32)
+            blk = b[k * tk:(k + 1) * tk, j * tn:(j + 1) * tn]
+            want[:blk.shape[0], :blk.shape[1]] = blk
+            ok &= np.array_equal(t.numpy().view(np.uint32), want.view(np.uint32))
+        for (i, k), t in a_rows.items():
+            ref = host_tile(a, tm, tk, i, k)
+            ok &= all(np.array_equal(x.numpy().view(np.uint32) if x.dtype != torch.int32 else x.numpy(),
+                                     y.view(np.uint32) if y.dtype != np.int32 else y) for x, y in zip(t, ref))
+        # C tiles I x J from the received operands only: A's rows I, B's columns J
+        ar = _from_tiles(a_rows, I, range(gk), tm, tk, a.m, a.n, np.float32)
+        bc = np.zeros_like(b)
+        for (k, j), t in b_cols.items():
+            blk = bc[k * tk:(k + 1) * tk, j * tn:(j + 1) * tn]
+            blk[...] = t.numpy()[:blk.shape[0], :blk.shape[1]]
+        tiles = {}
+        if I and J:
+            cc = O.spmm_tiled(ar, bc, c0, tm, tk, tn)
+            tiles = {(i, j): cc[i * tm:(i + 1) * tm, j * tn:(j + 1) * tn].copy() for i in I for j in J}
+        gathered = [None] * world if rank == 0 else None
+        tdist.gather_object((tiles, ok), gathered, dst=0)
+        if rank == 0:
+            whole = np.array(c0, copy=True)
+            seen = 0
+            for part, _ in gathered:
+                for (i, j), blk in part.items():
+                    whole[i * tm:(i + 1) * tm, j * tn:(j + 1) * tn] = blk
+                    seen += 1
+            want = O.spmm_tiled(a, b, c0, tm, tk, tn)
+            out["ok"] = all(g[1] for g in gathered)
+            out["tiles"] = seen
+            out["same"] = np.array_equal(whole.view(np.uint32), want.view(np.uint32))
+    finally:
+        tdist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,pgrid", [(2, (1, 2)), (4, (2, 2)), (3, (3, 1))])
+def test_spmm_exchange_serves_the_whole_product(world, pgrid):
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_spmm_exchange_rank, args=(world, pgrid, port, out), nprocs=world, join=True)
+        res = dict(out)
+    assert res["ok"], "a received tile differs from its owner's, or C tiles moved"
+    assert res["tiles"] == 6 * 4 and res["same"]
