@@ -62,14 +62,19 @@ def owned_input_tiles(mat, tm: int, tn: int, rank: int, pm: int, pn: int, device
     """The tiles of `mat` that process `rank` holds when the matrix is
     distributed as the reference distributes it (what SPMatrix(fname,
     blocking) keeps on each process)."""
+    from .containers import split_tiles
     gm, gn = _ceil_div(mat.m, tm), _ceil_div(mat.n, tn)
+    trp, toff, ci, v = split_tiles(mat, tm, tn)  # every tile at once, packed in grid order
     out = {}
     for i in range(gm):
         for j in range(gn):
             if tile_owner(i, j, pm, pn) == rank:
-                rp, ci, v = host_tile(mat, tm, tn, i, j)
-                out[(i, j)] = (torch.from_numpy(rp).to(device), torch.from_numpy(ci).to(device),
-                               torch.from_numpy(v).to(device))
+                t = i * gn + j
+                rows = min(tm, mat.m - i * tm)
+                lo, hi = int(toff[t]), int(toff[t + 1])
+                out[(i, j)] = (torch.from_numpy(np.ascontiguousarray(trp[t, :rows + 1])).to(device),
+                               torch.from_numpy(np.ascontiguousarray(ci[lo:hi])).to(device),
+                               torch.from_numpy(np.ascontiguousarray(v[lo:hi])).to(device))
     return out
 
 
