@@ -1,5 +1,7 @@
-"""ctypes front end of the C restatement in oracle.c, and a runner for the
-reference's own CPU binary (_ref/bcl_ref).
+"""ctypes front end of the C restatement in oracle.c, and runners for the
+reference's own CPU binaries (_ref/bcl_ref: one rank; _ref/bcl_ref_mp: the
+reference's distributed BCL::gemm on several ranks over the shared-memory
+MPI subset in ref_stubs_mp/).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
 and by bench.py's CPU-baseline and reference legs, always as the checker or
@@ -13,12 +15,14 @@ import json
 import os
 import subprocess
 import tempfile
+import time
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "bcl_ref")
+REF_MP_BIN = os.path.join(HERE, "_ref", "bcl_ref_mp")
 
 _lib = None
 
@@ -280,6 +284,93 @@ def ref_spmm(a, b, tm, tk, tn, warmup=0, reps=1, want_output=True, workdir=None)
         gen.write_binary(fa, a)
         gen.write_dense(fb, b)
         res = run_ref(["spmm", fa, fb, tm, tk, tn, fc if want_output else "-", warmup, reps])
+        c = gen.read_dense(fc) if want_output else None
+    return c, res
+
+
+def ref_mp_available() -> bool:
+    return os.path.exists(REF_MP_BIN)
+
+
+def _shared_dir():
+    """A tmpfs directory for the ranks' shared windows when there is one."""
+    return "/dev/shm" if os.path.isdir("/dev/shm") and os.access("/dev/shm", os.W_OK) else None
+
+
+def run_ref_mp(args, nranks, timeout=3600, threads=1):
+    """Run _ref/bcl_ref_mp as `nranks` ranks (one process each, `threads`
+    OpenMP threads each) on ``args`` and return rank 0's JSON line.  The
+    ranks share a fresh directory for their windows; when one rank fails or
+    the time runs out, the others are stopped."""
+    with tempfile.TemporaryDirectory(dir=_shared_dir(), prefix="bclx_ranks_") as d:
+        procs, logs = [], []
+        try:
+            for r in range(nranks):
+                env = dict(os.environ, BCLX_STUB_RANK=str(r), BCLX_STUB_SIZE=str(nranks), BCLX_STUB_DIR=d,
+                           BCLX_STUB_TIMEOUT=str(int(min(timeout, 900))), OMP_NUM_THREADS=str(threads))
+                out = open(os.path.join(d, f"out{r}"), "w+")
+                err = open(os.path.join(d, f"err{r}"), "w+")
+                logs.append((out, err))
+                procs.append(subprocess.Popen([REF_MP_BIN] + [str(x) for x in args], stdout=out, stderr=err,
+                                              env=env))
+            deadline = time.time() + timeout
+            while True:
+                states = [p.poll() for p in procs]
+                if all(s == 0 for s in states) or any(s not in (None, 0) for s in states):
+                    break
+                if time.time() > deadline:
+                    raise RuntimeError(f"bcl_ref_mp: {nranks} ranks did not finish in {timeout} s")
+                time.sleep(0.005)
+            for r, (p, (out, err)) in enumerate(zip(procs, logs)):
+                if p.returncode not in (None, 0):
+                    err.seek(0)
+                    raise RuntimeError(f"bcl_ref_mp rank {r} exited {p.returncode}: {err.read()[-400:]}")
+            out = logs[0][0]
+            out.seek(0)
+            for line in out.read().splitlines()[::-1]:
+                if line.strip().startswith("{"):
+                    return json.loads(line)
+            raise RuntimeError("bcl_ref_mp printed no result")
+        finally:  # no rank outlives the call
+            for p in procs:
+                if p.poll() is None:
+                    p.kill()
+                    p.wait()
+            for out, err in logs:
+                out.close()
+                err.close()
+
+
+def ref_spgemm_mp(a, b, tm, tk, tn, pgrid, mode="f32", warmup=0, reps=1, want_output=True, workdir=None,
+                  threads=1):
+    """The reference's distributed BCL::gemm(SPMatrix, SPMatrix, SPMatrix&)
+    with A, B and C on a pm x pn process grid (pm * pn ranks); returns
+    (result CSR gathered by rank 0, or None; rank 0's timing line)."""
+    from bcl_b200 import gen
+
+    pm, pn = pgrid
+    with tempfile.TemporaryDirectory(dir=workdir) as d:
+        fa, fb, fc = (os.path.join(d, x + ".binary") for x in "abc")
+        gen.write_binary(fa, a)
+        gen.write_binary(fb, b)
+        res = run_ref_mp(["spgemm", fa, fb, tm, tk, tn, pm, pn, mode, fc if want_output else "-", warmup, reps],
+                         pm * pn, threads=threads)
+        c = gen.read_binary(fc, np.float32 if mode == "f32" else np.int32) if want_output else None
+    return c, res
+
+
+def ref_spmm_mp(a, b, tm, tk, tn, pgrid, warmup=0, reps=1, want_output=True, workdir=None, threads=1):
+    """The reference's distributed BCL::gemm(SPMatrix, DMatrix, DMatrix&),
+    C = 0 first, on a pm x pn process grid."""
+    from bcl_b200 import gen
+
+    pm, pn = pgrid
+    with tempfile.TemporaryDirectory(dir=workdir) as d:
+        fa, fb, fc = os.path.join(d, "a.binary"), os.path.join(d, "b.dense"), os.path.join(d, "c.dense")
+        gen.write_binary(fa, a)
+        gen.write_dense(fb, b)
+        res = run_ref_mp(["spmm", fa, fb, tm, tk, tn, pm, pn, fc if want_output else "-", warmup, reps], pm * pn,
+                         threads=threads)
         c = gen.read_dense(fc) if want_output else None
     return c, res
 
