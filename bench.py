@@ -1233,17 +1233,28 @@ def split_rows(s, parts):
     return out
 
 
-def best_layout(run, rows):
+def best_layout(run, rows, run_ranks=None):
     """Time `run(parts, threads)` as one process with every host thread and
-    as one single-threaded process per core (rows dealt round-robin); return
-    (seconds per rep, processes) of the faster."""
+    as one single-threaded process per core (rows dealt round-robin), and
+    `run_ranks(pm, pn)`, the reference's own distributed BCL::gemm with one
+    rank per core on a pm x pn process grid (when its binary is built);
+    return (seconds per rep, layout) of the fastest, the layout being
+    ("threads", n), ("rows", processes) or ("ranks", pm, pn)."""
+    from oracle import oracle as O
     cores = reference_ranks()
-    best = (run(1, cores), 1)
+    best = (run(1, cores), ("threads", cores))
     procs = min(cores, rows)
     if procs > 1:
         t = run(procs, 1)
         if t < best[0]:
-            best = (t, procs)
+            best = (t, ("rows", procs))
+    if run_ranks is not None and cores > 1 and O.ref_mp_available():
+        pm = int(cores ** 0.5)
+        while cores % pm:
+            pm -= 1
+        t = run_ranks(pm, cores // pm)
+        if t < best[0]:
+            best = (t, ("ranks", pm, cores // pm))
     return best
 
 
@@ -1272,23 +1283,37 @@ def reference_spgemm_sample(a, G, stride, warmup, reps):
             res = run_reference_ranks(jobs, threads=threads)
         return max(statistics.mean(r["times_s"]) for r in res)
 
-    t, procs = best_layout(run, s.m)
-    return products, t, s.m, procs
+    def run_ranks(pm, pn):
+        from oracle import oracle as O
+        with tempfile.TemporaryDirectory() as d:
+            fa, fb = os.path.join(d, "s.binary"), os.path.join(d, "a.binary")
+            gen.write_binary(fa, s)
+            gen.write_binary(fb, a)
+            res = O.run_ref_mp(["spgemm", fa, fb, -(-s.m // G), ts, ts, pm, pn, mode, "-", warmup, reps], pm * pn)
+        return statistics.mean(res["times_s"])
+
+    t, layout = best_layout(run, s.m, run_ranks)
+    return products, t, s.m, layout
 
 
-def layout_note(procs):
-    cores = reference_ranks()
-    return (f"one process, {cores} OpenMP threads (only the accumulate is threaded)" if procs == 1 else
-            f"the rows dealt to {procs} processes run at once (one per core, 1 thread each), time of the slowest")
+def layout_note(layout):
+    if layout[0] == "threads":
+        return f"one process, {layout[1]} OpenMP threads (only the accumulate is threaded)"
+    if layout[0] == "rows":
+        return (f"the rows dealt to {layout[1]} processes run at once (one per core, 1 thread each), time of the "
+                f"slowest")
+    pm, pn = layout[1], layout[2]
+    return (f"the reference's distributed BCL::gemm on {pm * pn} ranks ({pm}x{pn} process grid, one per core, "
+            f"1 thread each), barrier to barrier")
 
 
 def cpu_baseline_spgemm(a, G, stride=16):
-    products, t, rows, procs = reference_spgemm_sample(a, G, stride, 0, 1)
+    products, t, rows, layout = reference_spgemm_sample(a, G, stride, 0, 1)
     return {"value": 2.0 * products / t / 1e9, "unit": "GFLOP/s", "cores": reference_ranks(),
             "kind": "reference",
             "sample": f"every {stride}th row of A ({rows} rows, {products} products) times A, {G}x{G} tile grid, "
-                      f"reference BCL::gemm built from its headers; the faster of one process per core and one "
-                      f"multi-threaded process: {layout_note(procs)}",
+                      f"reference BCL::gemm built from its headers; the fastest of one multi-threaded process, "
+                      f"one process per core and the distributed gemm on one rank per core: {layout_note(layout)}",
             "seconds": t}
 
 
@@ -1322,18 +1347,27 @@ def reference_spmm_sample(a, b, wl, stride, warmup, reps):
             res = run_reference_ranks(jobs, threads=threads)
         return max(statistics.mean(r["times_s"]) for r in res)
 
-    t, procs = best_layout(run, s.m)
-    return 2.0 * s.nnz * wl["N"], t, s.m, procs
+    def run_ranks(pm, pn):
+        from oracle import oracle as O
+        with tempfile.TemporaryDirectory() as d:
+            fa, fb = os.path.join(d, "s.binary"), os.path.join(d, "b.dense")
+            gen.write_binary(fa, s)
+            gen.write_dense(fb, b)
+            res = O.run_ref_mp(["spmm", fa, fb, -(-s.m // G), ts, wl["N"], pm, pn, "-", warmup, reps], pm * pn)
+        return statistics.mean(res["times_s"])
+
+    t, layout = best_layout(run, s.m, run_ranks)
+    return 2.0 * s.nnz * wl["N"], t, s.m, layout
 
 
 def cpu_baseline_spmm(a, b, wl):
     stride = spmm_cpu_sample(a, b, wl)
-    flops, t, rows, procs = reference_spmm_sample(a, b, wl, stride, 0, 1 if stride > 1 else 3)
+    flops, t, rows, layout = reference_spmm_sample(a, b, wl, stride, 0, 1 if stride > 1 else 3)
     return {"value": flops / t / 1e9, "unit": "GFLOP/s", "cores": reference_ranks(), "kind": "reference",
             "sample": (f"every {stride}th row of A ({rows} rows)" if stride > 1 else "the whole product") +
                       f" times B ({a.n}x{wl['N']}), reference BCL::gemm(SPMatrix, DMatrix) built from its "
-                      f"headers; the faster of one process per core and one process (its SpMM loop is serial): "
-                      f"{layout_note(procs)}", "seconds": t}
+                      f"headers; the fastest of one process, one process per core and the distributed gemm on "
+                      f"one rank per core (its SpMM loop is serial): {layout_note(layout)}", "seconds": t}
 
 
 def run_reference(args, dist):
@@ -1351,10 +1385,10 @@ def run_reference(args, dist):
             return {"impl": "reference", "unavailable": "the reference SpMM has no BF16 storage (FP32 only)"}
         a, b = spmm_inputs(wl, args.seed)
         stride = spmm_cpu_sample(a, b, wl)
-        flops, t, rows, procs = reference_spmm_sample(a, b, wl, stride, args.warmup, args.steps)
+        flops, t, rows, layout = reference_spmm_sample(a, b, wl, stride, args.warmup, args.steps)
         value = flops / t / 1e9
         sample = ((f"every {stride}th row of A ({rows} rows)" if stride > 1 else "the whole product") +
-                  f" times B; {layout_note(procs)}")
+                  f" times B; {layout_note(layout)}")
         return {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
@@ -1367,17 +1401,17 @@ def run_reference(args, dist):
     a = spgemm_matrix(wl, args.seed)
     G = wl["grid"]
     stride = 128 if a.m <= 65536 else 2048
-    products, t, rows, procs = reference_spgemm_sample(a, G, stride, args.warmup, args.steps)
+    products, t, rows, layout = reference_spgemm_sample(a, G, stride, args.warmup, args.steps)
     value = 2.0 * products / t / 1e9
     return {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": wl["value_type"], "data": "synthetic (seeded R-MAT)",
             "config": {"workload": wl["desc"], "tile_grid": f"{G}x{G}",
                        "sample": f"every {stride}th row of A ({rows} rows, {products} products) times A; "
-                                 f"{layout_note(procs)}"},
+                                 f"{layout_note(layout)}"},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": reference_ranks(), "kind": "reference",
-                             "sample": f"every {stride}th row of A times A, {G}x{G} tiles; {layout_note(procs)}, "
+                             "sample": f"every {stride}th row of A times A, {G}x{G} tiles; {layout_note(layout)}, "
                                        f"{args.steps} reps"},
             "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "gpu_launches": 0}
