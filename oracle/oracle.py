@@ -297,11 +297,12 @@ def _shared_dir():
     return "/dev/shm" if os.path.isdir("/dev/shm") and os.access("/dev/shm", os.W_OK) else None
 
 
-def run_ref_mp(args, nranks, timeout=3600, threads=1):
-    """Run _ref/bcl_ref_mp as `nranks` ranks (one process each, `threads`
-    OpenMP threads each) on ``args`` and return rank 0's JSON line.  The
-    ranks share a fresh directory for their windows; when one rank fails or
-    the time runs out, the others are stopped."""
+def run_ref_mp(args, nranks, timeout=3600, threads=1, binary=None):
+    """Run _ref/bcl_ref_mp (or another program built over ref_stubs_mp/) as
+    `nranks` ranks (one process each, `threads` OpenMP threads each) on
+    ``args`` and return rank 0's JSON line.  The ranks share a fresh
+    directory for their windows; when one rank fails or the time runs out,
+    the others are stopped."""
     with tempfile.TemporaryDirectory(dir=_shared_dir(), prefix="bclx_ranks_") as d:
         procs, logs = [], []
         try:
@@ -311,8 +312,8 @@ def run_ref_mp(args, nranks, timeout=3600, threads=1):
                 out = open(os.path.join(d, f"out{r}"), "w+")
                 err = open(os.path.join(d, f"err{r}"), "w+")
                 logs.append((out, err))
-                procs.append(subprocess.Popen([REF_MP_BIN] + [str(x) for x in args], stdout=out, stderr=err,
-                                              env=env))
+                procs.append(subprocess.Popen([binary or REF_MP_BIN] + [str(x) for x in args], stdout=out,
+                                              stderr=err, env=env))
             deadline = time.time() + timeout
             while True:
                 states = [p.poll() for p in procs]

@@ -2,8 +2,8 @@
  * Multi-process MPI subset over shared memory, written for this project as
  * TEST INFRASTRUCTURE.
  *
- * It lets the reference's header-only MPI backend (bcl/backends/mpi/*.hpp)
- * run as several ranks on one host without an MPI installation, so that the
+ * It lets the reference's header-only MPI backend (the bcl/backends/mpi
+ * headers) run as several ranks on one host without an MPI installation, so that the
  * reference's own distributed BCL::gemm (bcl/containers/algorithms/
  * spgemm.hpp:153-242: block-cyclic tiles, remote tile fetches, barriers,
  * pointer broadcasts) runs as written.  The ranks are separate processes

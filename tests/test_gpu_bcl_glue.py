@@ -43,3 +43,27 @@ def test_reference_containers_through_the_glue(tmp_path, value_type, tiles, n):
     res = json.loads(line[-1])
     assert out.returncode == 0, res
     assert res["spgemm_identical"] and res["spmm_identical"] and res["nnz"] > 0
+
+
+GLUE_MP = os.path.join(ROOT, "oracle", "_ref", "bcl_glue_check_mp")
+
+
+@pytest.mark.parametrize("pgrid,value_type,tiles,n", [((1, 2), "f32", (300, 700, 260), 40),
+                                                      ((2, 2), "f32", (256, 256, 256), 64),
+                                                      ((2, 1), "i32", (512, 333, 600), 0)])
+def test_reference_containers_through_the_glue_on_ranks(tmp_path, pgrid, value_type, tiles, n):
+    """The reference's containers distributed over a process grid, each rank
+    a process on this GPU (over the shared-memory MPI subset): every rank
+    fetches its operand tiles through get_tile and computes its own C tiles
+    in one sub-grid call; rank 0 compares every tile with the reference's
+    distributed BCL::gemm, bit for bit."""
+    from oracle import oracle as O
+    if not os.path.exists(GLUE_MP):
+        pytest.skip("bcl_glue_check_mp not built (needs the reference tree at build time)")
+    a = gen.rmat(11, seed=92, value_type=value_type)
+    fa = str(tmp_path / "a.binary")
+    gen.write_binary(fa, a)
+    pm, pn = pgrid
+    res = O.run_ref_mp([fa, *tiles, value_type, n, pm, pn], pm * pn, timeout=300, binary=GLUE_MP)
+    assert res["ranks"] == pm * pn
+    assert res["spgemm_identical"] and res["spmm_identical"] and res["nnz"] > 0
