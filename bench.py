@@ -1252,8 +1252,12 @@ def best_layout(run, rows, run_ranks=None):
         pm = int(cores ** 0.5)
         while cores % pm:
             pm -= 1
-        t = run_ranks(pm, cores // pm)
-        if t < best[0]:
+        try:
+            t = run_ranks(pm, cores // pm)
+        except (RuntimeError, OSError, subprocess.SubprocessError) as e:  # an extra layout: the others stand
+            print(f"reference on {cores} ranks skipped: {e}", file=sys.stderr)
+            t = None
+        if t is not None and t < best[0]:
             best = (t, ("ranks", pm, cores // pm))
     return best
 
