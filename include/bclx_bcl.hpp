@@ -55,7 +55,9 @@ inline void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// One bclx context per process (device 0, legacy default stream).
+// One bclx context per process on the legacy default stream: rank r uses
+// GPU r mod (number of GPUs), so the ranks of one node spread over its GPUs
+// (one rank: GPU 0).
 inline bclx_context_t context() {
   struct Holder {
     bclx_context_t h = nullptr;
@@ -64,7 +66,12 @@ inline bclx_context_t context() {
     }
   };
   static Holder holder;
-  if (!holder.h) check(bclx_context_create(0, &holder.h), "bclx_context_create");
+  if (!holder.h) {
+    int ndev = 0;
+    check_cuda(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    const int dev = ndev > 0 ? (int)(BCL::rank() % (uint64_t)ndev) : 0;
+    check(bclx_context_create(dev, &holder.h), "bclx_context_create");
+  }
   return holder.h;
 }
 
