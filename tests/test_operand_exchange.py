@@ -262,3 +262,39 @@ def test_spmm_exchange_serves_the_whole_product(world, pgrid):
         res = dict(out)
     assert res["ok"], "a received tile differs from its owner's, or C tiles moved"
     assert res["tiles"] == 6 * 4 and res["same"]
+
+
+def _rank_leaves(rank, world, port, out):
+    """Rank 1 leaves before the exchange (between steps, nothing in
+    flight); rank 0 must get an error from its next collective, within the
+    process group's timeout, instead of waiting for ever."""
+    from datetime import timedelta
+    import time
+    import torch.distributed as tdist
+    from bcl_b200.distributed import ProcessGroups, exchange_operands, owned_input_tiles
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
+                      LOCAL_RANK=str(rank))
+    tdist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=10))
+    groups = ProcessGroups(world, 1, world)
+    a, b, tm, tk, tn = _operands("f32")
+    if rank == 1:
+        out["left"] = True
+        return  # leaves without destroying the group: its peers see it gone
+    t0 = time.time()
+    try:
+        exchange_operands(owned_input_tiles(a, tm, tk, rank, 1, world), (a.m, a.n),
+                          owned_input_tiles(b, tk, tn, rank, 1, world), (b.m, b.n), tm, tk, tn, rank, groups)
+        out["error"] = None
+    except RuntimeError as e:
+        out["error"] = type(e).__name__
+    out["seconds"] = time.time() - t0
+
+
+def test_exchange_fails_fast_when_a_rank_leaves():
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_rank_leaves, args=(2, port, out), nprocs=2, join=True)
+        res = dict(out)
+    assert res["left"] and res["error"] is not None
+    assert res["seconds"] < 60
